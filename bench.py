@@ -1,0 +1,436 @@
+"""Benchmark: registrations/s (+ p50/p99 latency) of the CLAIRE GN-Krylov path.
+
+Workload (default): 128^3 periodic grid, FP32, H2 regularisation beta=1e-3,
+nt=8, tricubic SL, GN + PCG (inverse-regularisation preconditioner) +
+Armijo, gradient tolerance 1e-2, at most `--maxit` GN iterations.  Inputs
+are the seeded synthetic ellipsoid template and random smooth velocity
+(claire_b200.synthetic), mR = transport(mT, v).  A step solves one batch of
+`--batch` registrations to the stopping test.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1): every rank solves its own batch
+(independent problems, no collective on the data path: weak scaling); the
+timed region is bracketed by a barrier + synchronize, timed with CUDA events,
+and the max over ranks is reported.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "registrations/s at 128^3 (H2 beta=1e-3, nt=8, gradient reduced 1e-2 or maxit)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--nt", type=int, default=8)
+    ap.add_argument("--norm", default="h2")
+    ap.add_argument("--beta", type=float, default=1e-3)
+    ap.add_argument("--maxit", type=int, default=10)
+    ap.add_argument("--opttol", type=float, default=1e-2)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--no-plain", action="store_true", help="skip the single-problem comparison leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gather_list(vals, world):
+    if world == 1:
+        return list(vals)
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, list(vals))
+    return [v for part in out for v in part]
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, nm in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def make_opt(cb, a):
+    return cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", a.norm, "-beta", repr(a.beta),
+                      "-maxit", str(a.maxit), "-opttol", repr(a.opttol)])
+
+
+def run_ours(a, rank, world, local):
+    import torch
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = a.batch
+    # seeded inputs: problem index = rank*B + b
+    probs = [synthetic.ellipsoid_problem(a.n, a.nt, 1, rank * B + b, dev) for b in range(B)]
+    host = [(p[0].cpu().pin_memory(), p[1].cpu().pin_memory()) for p in probs]
+    n = a.n ** 3
+    stream = torch.cuda.Stream(device=dev)
+    opt = make_opt(cb, a)
+    ci = cb.CLAIREInterface(opt, nbatch=B)
+    ci.set_stream(stream)
+    zero_v = torch.zeros((3, a.n, a.n, a.n), device=dev)
+
+    def load_device():
+        for b, (mR, mT, _) in enumerate(probs):
+            ci.set_images(mR, mT, b)
+            ci.SetInitialGuess(zero_v, b)
+
+    # --- device-resident throughput ---------------------------------------------
+    for _ in range(a.warmup):
+        load_device()
+        ci.Run()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = cb.kernel_launches()
+    step_ms = []
+    with Clocks(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(a.steps):
+            load_device()
+            es = torch.cuda.Event(enable_timing=True)
+            ee = torch.cuda.Event(enable_timing=True)
+            es.record(stream)
+            ci.Run()
+            ee.record(stream)
+            step_ms.append((es, ee))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = cb.kernel_launches() - launches0
+    barrier(world)
+    total_ms = ev0.elapsed_time(ev1)
+    total_ms = max_over_ranks(total_ms, world)
+    lat = [s.elapsed_time(e) for s, e in step_ms]   # every problem of a batch completes with its batch
+    lat_all = gather_list([x for x in lat for _ in range(B)], world)
+    stats = [ci.stats(b) for b in range(B)]
+
+    # --- e2e: host buffers, H2D + D2H inside the timed region ---------------------
+    vout = torch.empty((3, a.n, a.n, a.n), dtype=torch.float32).pin_memory()
+    h2d = 2 * n * 4 * B
+    d2h = 3 * n * 4 * B
+
+    def e2e_step():
+        for b, (mRh, mTh) in enumerate(host):
+            with torch.cuda.stream(stream):
+                mRd = mRh.to(dev, non_blocking=True)
+                mTd = mTh.to(dev, non_blocking=True)
+            stream.synchronize()
+            ci.set_images(mRd, mTd, b)
+            ci.SetInitialGuess(zero_v, b)
+        ci.Run()
+        for b in range(B):
+            v = ci.GetSolution(b)   # device -> host (pageable NumPy buffer)
+            vout.copy_(torch.from_numpy(v))
+
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+
+    # --- plain single-problem path (B = 1, same problems one at a time) ----------
+    plain = None
+    if not a.no_plain:
+        ci1 = cb.CLAIREInterface(opt, nbatch=1)
+        ci1.set_stream(stream)
+        ci1.set_images(probs[0][0], probs[0][1])
+        ci1.SetInitialGuess(zero_v)
+        ci1.Run()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for b in range(B):
+            ci1.set_images(probs[b][0], probs[b][1])
+            ci1.SetInitialGuess(zero_v)
+            ci1.Run()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(p0.elapsed_time(p1), world)
+        plain = world * B / (plain_ms / 1e3)
+        ci1.close()
+
+    roof = roofline(cb, a, probs[0], dev, stream) if rank == 0 else None
+    ci.close()
+    return dict(total_ms=total_ms, lat=lat_all, stats=stats, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
+                launches=launches, clocks=clk.summary(), plain=plain, roof=roof)
+
+
+def roofline(cb, a, prob, dev, stream):
+    """Time the SL gather (m^{j+1} = m^j(X)) at the workload's size with CUDA events.
+
+    Algorithmic bytes per launch: field 4n + displacement 12n + output 4n = 20n.
+    """
+    import torch
+    mR, mT, v = prob
+    n = a.n ** 3
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    sl = cb.SemiLagrangian(a.nt)
+    with torch.cuda.stream(stream):
+        disp = sl.ComputeTrajectory(v, "state")
+        bufs = [mT.clone() for _ in range(8)]
+        outs = [torch.empty_like(mT) for _ in range(8)]
+        for i in range(5):
+            sl.Interpolate(bufs[i % 8], disp, out=outs[i % 8])
+        torch.cuda.synchronize()
+        reps = 40
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(reps):
+            sl.Interpolate(bufs[i % 8], disp, out=outs[i % 8])
+        t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / reps
+    bytes_ = 20 * n
+    achieved = bytes_ / (ms / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "interp_traffic.json")))
+        traffic = prof.get(str(a.n))
+    except Exception:
+        pass
+    return {"kernel": "k_interp (tricubic SL gather, 1 field)", "bound": "hbm", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes": bytes_, "avg_launch_us": round(ms * 1e3, 2), "peak_source": peak_src}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle port, numpy, host cores)
+# ---------------------------------------------------------------------------
+def cpu_op_times(n, reps=1):
+    """Seconds for one tricubic gather of a scalar field and one 3D real FFT
+    (r2c or c2r) at n^3 with the oracle port (NumPy FP64, one core)."""
+    from oracle import claire_ref as R
+    rng = np.random.default_rng(0)
+    shape = (n, n, n)
+    f = rng.standard_normal(shape)
+    disp = rng.uniform(-2, 2, size=(3,) + shape)
+    q = R.index_grid(shape) + disp
+    t = time.perf_counter()
+    for _ in range(reps):
+        st = R.Stencil(q, shape)
+        st.apply(f)
+    t_gather = (time.perf_counter() - t) / reps
+    t = time.perf_counter()
+    for _ in range(reps):
+        fh = np.fft.rfftn(f)
+        np.fft.irfftn(fh, s=shape)
+    t_fft = (time.perf_counter() - t) / (2 * reps)
+    return t_gather, t_fft
+
+
+def cpu_seconds_per_registration(stats, nt, t_gather, t_fft):
+    """Compose the reference's per-call operation counts (SURVEY call stacks):
+    objective: 3 (trajectory) + nt gathers, 6 FFTs (H2 functional);
+    gradient: 3 + 1 + nt gathers, 4(nt+1) + 4 + 6 FFTs;
+    Hessian matvec: 5nt + 4 gathers, 12nt + 14 FFTs; preconditioner: 6 FFTs."""
+    t_obj = (3 + nt) * t_gather + 6 * t_fft
+    t_grad = (4 + nt) * t_gather + (4 * (nt + 1) + 10) * t_fft
+    t_mv = (5 * nt + 4) * t_gather + (12 * nt + 14) * t_fft
+    t_pc = 6 * t_fft
+    return (stats["obj_evals"] * t_obj + stats["grad_evals"] * t_grad + stats["hess_matvecs"] * t_mv
+            + stats["pc_matvecs"] * t_pc)
+
+
+def default_stats(a):
+    """Operation counts of one registration of the workload (measured on the GPU
+    path; used by the reference arm to size its sample)."""
+    path = os.path.join(ROOT, "profiles", "workload_counts.json")
+    try:
+        return json.load(open(path))[f"{a.n}_{a.nt}_{a.norm}_{a.maxit}"]
+    except Exception:
+        return {"obj_evals": 20, "grad_evals": 11, "hess_matvecs": 100, "pc_matvecs": 110}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    t_gather, t_fft = cpu_op_times(a.n)
+    st = default_stats(a)
+    steps = []
+    for _ in range(max(1, a.steps)):
+        tg, tf = (t_gather, t_fft) if not steps else cpu_op_times(a.n)
+        steps.append(cpu_seconds_per_registration(st, a.nt, tg, tf))
+    sec = float(np.median(steps))
+    val = 1.0 / sec
+    cores = 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "registrations/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"single registration {a.n}^3 {a.norm} beta={a.beta} nt={a.nt} maxit={a.maxit}",
+                   "n": a.n, "nt": a.nt, "regnorm": a.norm, "beta": a.beta},
+        "cpu_baseline": {"value": val, "unit": "registrations/s", "cores": cores, "kind": "port",
+                         "sample": f"oracle NumPy FP64: one tricubic gather + one r2c/c2r at {a.n}^3 per step, "
+                                   "composed with the reference's per-call operation counts of one registration"},
+        "e2e": {"value": val, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    rank, world, local = dist_init(a)
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+    r = run_ours(a, rank, world, local)
+    if rank != 0:
+        return
+    B = a.batch
+    regs = world * B * a.steps
+    value = regs / (r["total_ms"] / 1e3)
+    lat = sorted(r["lat"])
+    p50 = float(np.percentile(lat, 50))
+    p99 = float(np.percentile(lat, 99))
+    st0 = r["stats"][0]
+    cpu = None
+    if not a.no_cpu:
+        t_gather, t_fft = cpu_op_times(a.n)
+        mean_stats = {k: float(np.mean([s[k] for s in r["stats"]])) for k in
+                      ("obj_evals", "grad_evals", "hess_matvecs", "pc_matvecs")}
+        sec = cpu_seconds_per_registration(mean_stats, a.nt, t_gather, t_fft)
+        cpu = {"value": 1.0 / sec, "unit": "registrations/s", "cores": 1, "kind": "port",
+               "sample": f"oracle NumPy FP64: one tricubic gather ({t_gather:.2f} s) and one 3D real FFT "
+                         f"({t_fft:.3f} s) at {a.n}^3, composed with this run's per-registration operation "
+                         "counts and the reference's per-call gather/FFT counts"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": r["total_ms"] / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"batched registrations {a.n}^3 {a.norm} beta={a.beta} nt={a.nt} "
+                               f"maxit={a.maxit} opttol={a.opttol}, {B} per GPU per step",
+                   "n": a.n, "nt": a.nt, "regnorm": a.norm, "beta": a.beta, "batch_per_gpu": B,
+                   "parallelism": f"independent problems, {world} GPU(s)",
+                   "l2": "inputs larger than L2 (per-problem working set ~0.9 GB)",
+                   "latency_ms": {"p50": p50, "p99": p99},
+                   "plain_single_problem_value": r["plain"],
+                   "gn_iterations": st0["gn_iterations"], "pcg_iterations": st0["pcg_iterations"],
+                   "rel_mismatch": st0["rel_mismatch"], "grad_reduction": st0["gnorm"] / st0["gnorm0"]},
+        "e2e": {"value": regs / (r["e2e_ms"] / 1e3), "unit": "registrations/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "roofline": r["roof"],
+        "cpu_baseline": cpu,
+        "clocks": r["clocks"],
+        "gpu_launches": r["launches"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

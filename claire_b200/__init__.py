@@ -1,0 +1,509 @@
+"""claire_b200: B200-native CLAIRE Gauss-Newton-Krylov registration path.
+
+The compute path is ``libclaire_b200.so`` (CUDA for sm_100a plus the C++ GN
+driver); this module is a thin ctypes mirror of its C ABI
+(``include/claire_b200.h``) that keeps the reference's names:
+
+* ``RegOpt``            -- reg::RegOpt (include/RegOpt.hpp:475-635)
+* ``CLAIREInterface``   -- reg::CLAIREInterface (include/CLAIREInterface.hpp:42-90)
+* ``SemiLagrangian``    -- ComputeTrajectory / Interpolate (include/SemiLagrangian.hpp:43-58)
+* ``Regularization``    -- EvaluateFunctional / EvaluateGradient / HessianMatVec /
+                           ApplyInverse (include/Regularization.hpp:46-50)
+* ``DistanceMeasureSL2``-- EvaluateFunctional (include/DistanceMeasure.hpp:44-50)
+* spectral helpers standing in for AccFFT's accfft_grad_t / accfft_divergence_t.
+
+Operator functions take torch CUDA tensors (float32, contiguous) and run on
+the current torch stream.  There is no CPU fallback: importing without the
+built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+__all__ = [
+    "lib", "RegOpt", "CLAIREInterface", "SemiLagrangian", "Regularization", "DistanceMeasureSL2",
+    "Preconditioner", "fft_grad", "fft_div", "leray", "smooth", "kernel_launches", "ClaireError",
+    "NORMS", "MODELS",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+# CLAIRE_B200_LIB selects another build of the library (A/B comparisons).
+LIB_PATH = os.environ.get("CLAIRE_B200_LIB") or os.path.join(_HERE, "libclaire_b200.so")
+
+NORMS = {"l2": 0, "h1": 1, "h1s": 2, "h2": 3, "h2s": 4, "h3": 5, "h3s": 6}
+MODELS = {"compressible": 0, "stokes": 1, "relaxedstokes": 2}
+REG_KIND = {"gradient": 0, "inverse": 1, "sqrtinverse": 2}
+ERRORS = {-1: "invalid argument", -2: "allocation failed", -3: "CUDA error", -4: "numerical error (NaN)",
+          -5: "call out of order", -6: "unsupported grid size"}
+
+
+class ClaireError(RuntimeError):
+    """Raised for a negative status code from the C ABI."""
+
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        msg = f"{where}: {ERRORS.get(code, 'error')} ({code})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int * 3), ("nt", ctypes.c_int), ("regnorm", ctypes.c_int), ("model", ctypes.c_int),
+        ("beta", ctypes.c_double * 3), ("maxit", ctypes.c_int), ("opttol", ctypes.c_double),
+        ("gatol", ctypes.c_double), ("krylovmaxit", ctypes.c_int), ("krylovtol", ctypes.c_double * 3),
+        ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
+        ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("gn_iterations", ctypes.c_int), ("pcg_iterations", ctypes.c_int), ("obj_evals", ctypes.c_int),
+        ("grad_evals", ctypes.c_int), ("hess_matvecs", ctypes.c_int), ("pc_matvecs", ctypes.c_int),
+        ("pde_solves", ctypes.c_int), ("converged_reason", ctypes.c_int), ("J", ctypes.c_double),
+        ("J0", ctypes.c_double), ("D", ctypes.c_double), ("D0", ctypes.c_double), ("R", ctypes.c_double),
+        ("gnorm", ctypes.c_double), ("gnorm0", ctypes.c_double), ("rel_mismatch", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"claire_b200: {LIB_PATH} is not built; run `python -m claire_b200.build` "
+            "(there is no CPU fallback)")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_IA = ctypes.POINTER(ctypes.c_int)
+_DA = ctypes.POINTER(ctypes.c_double)
+_signatures = {
+    "claire_b200_default_opts": (_I, [ctypes.POINTER(Opts)]),
+    "claire_b200_parse_args": (_I, [ctypes.POINTER(Opts), _I, ctypes.POINTER(ctypes.c_char_p)]),
+    "claire_b200_create": (_I, [ctypes.POINTER(Opts), _I, ctypes.POINTER(_P)]),
+    "claire_b200_destroy": (_I, [_P]),
+    "claire_b200_last_error": (ctypes.c_char_p, [_P]),
+    "claire_b200_footprint_bytes": (ctypes.c_longlong, [_P]),
+    "claire_b200_estimate_bytes": (ctypes.c_longlong, [ctypes.POINTER(Opts), _I]),
+    "claire_b200_set_problem_opts": (_I, [_P, _I, ctypes.POINTER(Opts)]),
+    "claire_b200_set_images": (_I, [_P, _I, _P, _P, _I]),
+    "claire_b200_set_velocity": (_I, [_P, _I, _P, _I]),
+    "claire_b200_get_velocity": (_I, [_P, _I, _P, _I]),
+    "claire_b200_run": (_I, [_P]),
+    "claire_b200_run_masked": (_I, [_P, _IA]),
+    "claire_b200_get_final_state": (_I, [_P, _I, _P, _I]),
+    "claire_b200_forward": (_I, [_P, _I, _P, _P, _I]),
+    "claire_b200_get_stats": (_I, [_P, _I, ctypes.POINTER(Stats)]),
+    "claire_b200_objective": (_I, [_P, _I, _P, _DA, _DA, _DA]),
+    "claire_b200_gradient": (_I, [_P, _I, _P, _P]),
+    "claire_b200_hessian_matvec": (_I, [_P, _I, _P, _P, _P]),
+    "claire_b200_precond": (_I, [_P, _I, _P, _P]),
+    "claire_b200_get_adjoint": (_I, [_P, _I, _P, _P]),
+    "claire_b200_synchronize": (_I, [_P]),
+    "claire_b200_set_stream": (_I, [_P, _P]),
+    "claire_b200_trajectory": (_I, [_P, _P, _IA, _I, _I, _P]),
+    "claire_b200_interp3": (_I, [_P, _P, _P, _IA, _I, _P]),
+    "claire_b200_fft_grad": (_I, [_P, _P, _IA, _P]),
+    "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
+    "claire_b200_reg_apply": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
+    "claire_b200_reg_functional": (_I, [_P, _DA, _IA, _I, _DA, _P]),
+    "claire_b200_leray": (_I, [_P, _IA, _I, _DA, _P]),
+    "claire_b200_smooth": (_I, [_P, _P, _IA, _DA, _P]),
+    "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),
+    "claire_b200_kernel_launches": (ctypes.c_longlong, []),
+}
+for _name, (_res, _args) in _signatures.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def _check(code: int, where: str, ctx=None):
+    if code != 0:
+        detail = ""
+        if ctx is not None:
+            raw = lib.claire_b200_last_error(ctx)
+            detail = raw.decode() if raw else ""
+        raise ClaireError(code, where, detail)
+
+
+def kernel_launches() -> int:
+    """CUDA kernel launches issued by the library since it was loaded."""
+    return int(lib.claire_b200_kernel_launches())
+
+
+# ---------------------------------------------------------------------------
+# tensor helpers (torch is only the device-memory / stream plumbing)
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch  # noqa: WPS433 (imported lazily: the ABI itself does not need torch)
+    return torch
+
+
+def _dev_ptr(t, shape_hint: str = ""):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"expected a CUDA tensor {shape_hint}")
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise TypeError(f"expected a contiguous float32 CUDA tensor {shape_hint}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    torch = _torch()
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _nx(shape) -> ctypes.Array:
+    return (ctypes.c_int * 3)(*[int(s) for s in shape])
+
+
+# ---------------------------------------------------------------------------
+# reg::RegOpt
+# ---------------------------------------------------------------------------
+
+class RegOpt:
+    """Hot-path subset of reg::RegOpt; ``RegOpt(["-nx", "64", ...])`` parses CLAIRE flags."""
+
+    def __init__(self, argv: Optional[Sequence[str]] = None, **kw):
+        self.opts = Opts()
+        _check(lib.claire_b200_default_opts(ctypes.byref(self.opts)), "RegOpt")
+        if argv:
+            arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+            _check(lib.claire_b200_parse_args(ctypes.byref(self.opts), len(argv), arr), "RegOpt.ParseArguments")
+        for k, v in kw.items():
+            self.set(k, v)
+
+    def set(self, key, value):
+        o = self.opts
+        if key == "nx":
+            vals = [value] * 3 if isinstance(value, int) else list(value)
+            for i in range(3):
+                o.nx[i] = int(vals[i])
+        elif key == "regnorm":
+            o.regnorm = NORMS[value] if isinstance(value, str) else int(value)
+            o.model = MODELS["compressible"]
+        elif key == "model":
+            o.model = MODELS[value] if isinstance(value, str) else int(value)
+        elif key == "beta":
+            vals = [value] if isinstance(value, (int, float)) else list(value)
+            for i, b in enumerate(vals):
+                o.beta[i] = float(b)
+        elif key == "krylovtol":
+            o.krylovtol[0] = float(value)
+        elif hasattr(o, key):
+            setattr(o, key, type(getattr(o, key))(value))
+        else:
+            raise KeyError(key)
+        return self
+
+    @property
+    def nx(self):
+        return tuple(self.opts.nx)
+
+    @property
+    def nt(self):
+        return int(self.opts.nt)
+
+    def estimate_bytes(self, nbatch: int = 1) -> int:
+        return int(lib.claire_b200_estimate_bytes(ctypes.byref(self.opts), nbatch))
+
+
+# ---------------------------------------------------------------------------
+# reg::CLAIREInterface (batched: nbatch independent problems of one size)
+# ---------------------------------------------------------------------------
+
+class CLAIREInterface:
+    """Drop-in for reg::CLAIREInterface; images and velocities are NumPy arrays
+    (host) or torch CUDA tensors (device, copied on set)."""
+
+    def __init__(self, opt: RegOpt, nbatch: int = 1):
+        self.opt = opt
+        self.nbatch = nbatch
+        self._ctx = ctypes.c_void_p()
+        _check(lib.claire_b200_create(ctypes.byref(opt.opts), nbatch, ctypes.byref(self._ctx)), "CLAIREInterface")
+        self.shape = opt.nx
+
+    def close(self):
+        if self._ctx:
+            lib.claire_b200_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- data -----------------------------------------------------------------
+    def _src(self, arr, count):
+        torch = _torch()
+        if isinstance(arr, torch.Tensor):
+            if arr.is_cuda:
+                t = arr.detach().to(torch.float32).contiguous()
+                if t.numel() != count:
+                    raise ValueError("size mismatch")
+                return ctypes.c_void_p(t.data_ptr()), 1, t
+            arr = arr.numpy()
+        import numpy as np
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        if a.size != count:
+            raise ValueError(f"size mismatch: {a.size} != {count}")
+        return a.ctypes.data_as(ctypes.c_void_p), 0, a
+
+    def _n(self):
+        n1, n2, n3 = self.shape
+        return n1 * n2 * n3
+
+    def set_problem_opts(self, b: int, opt: RegOpt):
+        _check(lib.claire_b200_set_problem_opts(self._ctx, b, ctypes.byref(opt.opts)), "set_problem_opts", self._ctx)
+
+    def SetReferenceImage(self, mR, b: int = 0):
+        self._mR = (b, mR)
+        if getattr(self, "_mT", None) is not None and self._mT[0] == b:
+            self._set_images(b)
+
+    def SetTemplateImage(self, mT, b: int = 0):
+        self._mT = (b, mT)
+        if getattr(self, "_mR", None) is not None and self._mR[0] == b:
+            self._set_images(b)
+
+    def set_images(self, mR, mT, b: int = 0):
+        pr, devr, keep_r = self._src(mR, self._n())
+        pt, devt, keep_t = self._src(mT, self._n())
+        if devr != devt:
+            raise ValueError("mR and mT must both be host arrays or both CUDA tensors")
+        _check(lib.claire_b200_set_images(self._ctx, b, pr, pt, devr), "SetImages", self._ctx)
+
+    def _set_images(self, b):
+        self.set_images(self._mR[1], self._mT[1], b)
+        self._mR = self._mT = None
+
+    def SetInitialGuess(self, v, b: int = 0):
+        p, dev, keep = self._src(v, 3 * self._n())
+        _check(lib.claire_b200_set_velocity(self._ctx, b, p, dev), "SetInitialGuess", self._ctx)
+
+    def GetSolution(self, b: int = 0, out=None):
+        import numpy as np
+        if out is None:
+            out = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+            _check(lib.claire_b200_get_velocity(self._ctx, b, out.ctypes.data_as(ctypes.c_void_p), 0), "GetSolution",
+                   self._ctx)
+            return out
+        _check(lib.claire_b200_get_velocity(self._ctx, b, _dev_ptr(out), 1), "GetSolution", self._ctx)
+        return out
+
+    def GetFinalState(self, b: int = 0, out=None):
+        import numpy as np
+        if out is None:
+            out = np.empty(tuple(self.shape), dtype=np.float32)
+            _check(lib.claire_b200_get_final_state(self._ctx, b, out.ctypes.data_as(ctypes.c_void_p), 0),
+                   "GetFinalState", self._ctx)
+            return out
+        _check(lib.claire_b200_get_final_state(self._ctx, b, _dev_ptr(out), 1), "GetFinalState", self._ctx)
+        return out
+
+    def Run(self, mask: Optional[Sequence[int]] = None):
+        if mask is None:
+            _check(lib.claire_b200_run(self._ctx), "Run", self._ctx)
+        else:
+            arr = (ctypes.c_int * self.nbatch)(*[int(x) for x in mask])
+            _check(lib.claire_b200_run_masked(self._ctx, arr), "Run", self._ctx)
+
+    def SolveForwardProblem(self, m0, b: int = 0):
+        import numpy as np
+        p, dev, keep = self._src(m0, self._n())
+        if dev:
+            torch = _torch()
+            out = torch.empty_like(keep)
+            _check(lib.claire_b200_forward(self._ctx, b, p, _dev_ptr(out), 1), "SolveForwardProblem", self._ctx)
+            return out
+        out = np.empty(tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_forward(self._ctx, b, p, out.ctypes.data_as(ctypes.c_void_p), 0),
+               "SolveForwardProblem", self._ctx)
+        return out
+
+    def stats(self, b: int = 0) -> dict:
+        st = Stats()
+        _check(lib.claire_b200_get_stats(self._ctx, b, ctypes.byref(st)), "stats", self._ctx)
+        return st.as_dict()
+
+    def footprint_bytes(self) -> int:
+        return int(lib.claire_b200_footprint_bytes(self._ctx))
+
+    def set_stream(self, stream=None):
+        """Issue the context's work on a torch.cuda.Stream (None: its own stream)."""
+        handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else ctypes.c_void_p()
+        _check(lib.claire_b200_set_stream(self._ctx, handle), "set_stream", self._ctx)
+
+    def synchronize(self):
+        _check(lib.claire_b200_synchronize(self._ctx), "synchronize", self._ctx)
+
+    # --- OptimizationProblem seams (host NumPy arrays) -------------------------
+    def EvaluateObjective(self, v, b: int = 0):
+        p, _, keep = self._src(v, 3 * self._n())
+        J, D, R = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib.claire_b200_objective(self._ctx, b, p, ctypes.byref(J), ctypes.byref(D), ctypes.byref(R)),
+               "EvaluateObjective", self._ctx)
+        return J.value, D.value, R.value
+
+    def EvaluateGradient(self, v, b: int = 0):
+        import numpy as np
+        p, _, keep = self._src(v, 3 * self._n())
+        g = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_gradient(self._ctx, b, p, g.ctypes.data_as(ctypes.c_void_p)), "EvaluateGradient",
+               self._ctx)
+        return g
+
+    def HessianMatVec(self, v, vt, b: int = 0):
+        import numpy as np
+        p, _, keep = self._src(v, 3 * self._n())
+        pt, _, keep_t = self._src(vt, 3 * self._n())
+        h = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_hessian_matvec(self._ctx, b, p, pt, h.ctypes.data_as(ctypes.c_void_p)),
+               "HessianMatVec", self._ctx)
+        return h
+
+    def ApplyInvRegularizationOperator(self, x, b: int = 0):
+        import numpy as np
+        p, _, keep = self._src(x, 3 * self._n())
+        out = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_precond(self._ctx, b, p, out.ctypes.data_as(ctypes.c_void_p)), "Precond", self._ctx)
+        return out
+
+    def GetAdjoint(self, b: int = 0):
+        import numpy as np
+        lam = np.empty(tuple(self.shape), dtype=np.float32)
+        bf = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_get_adjoint(self._ctx, b, lam.ctypes.data_as(ctypes.c_void_p),
+                                           bf.ctypes.data_as(ctypes.c_void_p)), "GetAdjoint", self._ctx)
+        return lam, bf
+
+
+# ---------------------------------------------------------------------------
+# inner operator seams on torch CUDA tensors
+# ---------------------------------------------------------------------------
+
+class SemiLagrangian:
+    """ComputeTrajectory / Interpolate on device tensors (src/SemiLagrangian.cpp)."""
+
+    def __init__(self, nt: int):
+        self.nt = nt
+
+    def ComputeTrajectory(self, v, flag: str = "state", out=None):
+        torch = _torch()
+        shape = v.shape[1:]
+        if out is None:
+            out = torch.empty_like(v)
+        f = {"state": 0, "adjoint": 1}[flag]
+        _check(lib.claire_b200_trajectory(_dev_ptr(v), _dev_ptr(out), _nx(shape), self.nt, f, _stream()),
+               "ComputeTrajectory")
+        return out
+
+    @staticmethod
+    def Interpolate(f, disp, out=None):
+        torch = _torch()
+        dof = 3 if f.dim() == 4 else 1
+        shape = f.shape[-3:]
+        if out is None:
+            out = torch.empty_like(f)
+        _check(lib.claire_b200_interp3(_dev_ptr(f), _dev_ptr(disp), _dev_ptr(out), _nx(shape), dof, _stream()),
+               "Interpolate")
+        return out
+
+
+class Regularization:
+    """Spectral regularisation operators on device tensors (src/Regularization*.cpp)."""
+
+    def __init__(self, norm: str = "h1s", beta0: float = 1e-2, beta1: float = 1e-4):
+        self.norm = norm
+        self.beta = (ctypes.c_double * 2)(beta0, beta1)
+
+    def _apply(self, v, kind, out=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty_like(v)
+        _check(lib.claire_b200_reg_apply(_dev_ptr(v), _dev_ptr(out), _nx(v.shape[1:]), NORMS[self.norm], self.beta,
+                                         REG_KIND[kind], _stream()), "Regularization")
+        return out
+
+    def EvaluateGradient(self, v, out=None):
+        return self._apply(v, "gradient", out)
+
+    HessianMatVec = EvaluateGradient
+
+    def ApplyInverse(self, v, applysqrt: bool = False, out=None):
+        return self._apply(v, "sqrtinverse" if applysqrt else "inverse", out)
+
+    def EvaluateFunctional(self, v) -> float:
+        R = ctypes.c_double()
+        _check(lib.claire_b200_reg_functional(_dev_ptr(v), ctypes.byref(R), _nx(v.shape[1:]), NORMS[self.norm],
+                                              self.beta, _stream()), "EvaluateFunctional")
+        return R.value
+
+
+class Preconditioner(Regularization):
+    """INVREG preconditioner: P x = (beta A)^-1 x (src/Preconditioner.cpp:549-580)."""
+
+    def MatVec(self, x, out=None):
+        return self.ApplyInverse(x, False, out)
+
+
+class DistanceMeasureSL2:
+    @staticmethod
+    def EvaluateFunctional(mR, m1) -> float:
+        D = ctypes.c_double()
+        _check(lib.claire_b200_distance(_dev_ptr(mR), _dev_ptr(m1), _nx(mR.shape), ctypes.byref(D), _stream()),
+               "DistanceMeasureSL2")
+        return D.value
+
+
+def fft_grad(f, out=None):
+    torch = _torch()
+    if out is None:
+        out = torch.empty((3,) + tuple(f.shape), device=f.device, dtype=torch.float32)
+    _check(lib.claire_b200_fft_grad(_dev_ptr(f), _dev_ptr(out), _nx(f.shape), _stream()), "fft_grad")
+    return out
+
+
+def fft_div(v, out=None):
+    torch = _torch()
+    if out is None:
+        out = torch.empty(tuple(v.shape[1:]), device=v.device, dtype=torch.float32)
+    _check(lib.claire_b200_fft_div(_dev_ptr(v), _dev_ptr(out), _nx(v.shape[1:]), _stream()), "fft_div")
+    return out
+
+
+def leray(b, model: str = "stokes", beta=(1e-2, 1e-4, 1e-4)):
+    """In place: b += projection addend (CLAIREStokes / CLAIREDivReg ::ApplyProjection)."""
+    arr = (ctypes.c_double * 3)(*beta)
+    _check(lib.claire_b200_leray(_dev_ptr(b), _nx(b.shape[1:]), MODELS[model], arr, _stream()), "leray")
+    return b
+
+
+def smooth(f, sigma=(1.0, 1.0, 1.0), out=None):
+    torch = _torch()
+    if out is None:
+        out = torch.empty_like(f)
+    arr = (ctypes.c_double * 3)(*sigma)
+    _check(lib.claire_b200_smooth(_dev_ptr(f), _dev_ptr(out), _nx(f.shape), arr, _stream()), "smooth")
+    return out

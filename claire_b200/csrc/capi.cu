@@ -1,0 +1,580 @@
+// extern "C" boundary of libclaire_b200.so (declared in include/claire_b200.h).
+//
+// The context functions mirror reg::CLAIREInterface / reg::RegOpt
+// (include/CLAIREInterface.hpp:42-90, include/RegOpt.hpp:475-635); the
+// operator functions mirror the inner seams SemiLagrangian, Regularization,
+// DistanceMeasureSL2 and the AccFFT spectral calls so each piece can be
+// swapped and tested on its own.  No exception crosses the ABI.
+#include <atomic>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/claire_b200.h"
+#include "reduce.cuh"
+#include "sl.cuh"
+#include "solver.cuh"
+#include "spectral.cuh"
+
+namespace cb {
+static std::atomic<long long> g_launches{0};
+void note_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launches() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace cb
+
+using namespace cb;
+
+struct claire_b200_ctx {
+  Solver solver;
+  std::string last_error;
+};
+
+static int cuda_status(int e) { return e == 0 ? CB_OK : (e < 0 ? e : CB_ERR_CUDA); }
+
+extern "C" {
+
+int claire_b200_default_opts(claire_b200_opts* o) {
+  if (!o) return CB_ERR_ARG;
+  std::memset(o, 0, sizeof(*o));
+  o->nx[0] = o->nx[1] = o->nx[2] = 32;
+  o->nt = 4;
+  o->regnorm = CB_NORM_H1SN;
+  // RegOpt::Initialize defaults to RELAXEDSTOKES when -regnorm is absent
+  // (src/RegOpt.cpp:1066); every -regnorm choice selects COMPRESSIBLE.
+  o->model = CB_MODEL_RELAXEDSTOKES;
+  o->beta[0] = 1e-2;
+  o->beta[1] = 1e-4;
+  o->beta[2] = 1e-4;
+  o->maxit = 50;
+  o->opttol = 5e-2;
+  o->gatol = 1e-6;
+  o->krylovmaxit = 50;
+  o->krylovtol[0] = 1e-12;
+  o->krylovtol[1] = 1e-16;
+  o->krylovtol[2] = 1e6;
+  o->krylovfseq = CB_FSEQ_SUPERLINEAR;
+  o->precond = 1;
+  o->iporder = 3;
+  o->verbosity = 0;
+  o->bf16_images = 0;
+  return CB_OK;
+}
+
+int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* argv) {
+  if (!o || (argc > 0 && !argv)) return CB_ERR_ARG;
+  for (int i = 0; i < argc; ++i) {
+    const char* a = argv[i];
+    auto next = [&](const char** val) -> int {
+      if (i + 1 >= argc) return CB_ERR_ARG;
+      *val = argv[++i];
+      return CB_OK;
+    };
+    const char* val = nullptr;
+    if (!std::strcmp(a, "-nx")) {
+      if (next(&val)) return CB_ERR_ARG;
+      int v[3] = {0, 0, 0};
+      int cnt = std::sscanf(val, "%dx%dx%d", &v[0], &v[1], &v[2]);
+      if (cnt == 1) v[1] = v[2] = v[0];
+      else if (cnt != 3) return CB_ERR_ARG;
+      for (int k = 0; k < 3; ++k) o->nx[k] = v[k];
+    } else if (!std::strcmp(a, "-nt")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->nt = std::atoi(val);
+    } else if (!std::strcmp(a, "-regnorm")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->model = CB_MODEL_COMPRESSIBLE;
+      if (!std::strcmp(val, "h1s")) o->regnorm = CB_NORM_H1SN;
+      else if (!std::strcmp(val, "h2s")) o->regnorm = CB_NORM_H2SN;
+      else if (!std::strcmp(val, "h3s")) o->regnorm = CB_NORM_H3SN;
+      else if (!std::strcmp(val, "h1")) o->regnorm = CB_NORM_H1;
+      else if (!std::strcmp(val, "h2")) o->regnorm = CB_NORM_H2;
+      else if (!std::strcmp(val, "h3")) o->regnorm = CB_NORM_H3;
+      else if (!std::strcmp(val, "l2")) o->regnorm = CB_NORM_L2;
+      else if (!std::strcmp(val, "h1s-div")) { o->regnorm = CB_NORM_H1SN; o->model = CB_MODEL_RELAXEDSTOKES; }
+      else if (!std::strcmp(val, "h1s-stokes")) { o->regnorm = CB_NORM_H1SN; o->model = CB_MODEL_STOKES; }
+      else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-beta")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->beta[0] = std::atof(val);
+    } else if (!std::strcmp(a, "-beta-div")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->beta[2] = std::atof(val);
+    } else if (!std::strcmp(a, "-maxit")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->maxit = std::atoi(val);
+    } else if (!std::strcmp(a, "-opttol")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->opttol = std::atof(val);
+    } else if (!std::strcmp(a, "-gabs")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->gatol = std::atof(val);
+    } else if (!std::strcmp(a, "-krylovmaxit")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->krylovmaxit = std::atoi(val);
+    } else if (!std::strcmp(a, "-krylovtol")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->krylovtol[0] = std::atof(val);
+    } else if (!std::strcmp(a, "-krylovfseq")) {
+      if (next(&val)) return CB_ERR_ARG;
+      if (!std::strcmp(val, "none")) o->krylovfseq = CB_FSEQ_NONE;
+      else if (!std::strcmp(val, "quadratic")) o->krylovfseq = CB_FSEQ_QUADRATIC;
+      else if (!std::strcmp(val, "suplinear")) o->krylovfseq = CB_FSEQ_SUPERLINEAR;
+      else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-precond")) {
+      if (next(&val)) return CB_ERR_ARG;
+      if (!std::strcmp(val, "none")) o->precond = 0;
+      else if (!std::strcmp(val, "invreg")) o->precond = 1;
+      else return CB_ERR_UNSUPPORTED;  // 2level: not on this path
+    } else if (!std::strcmp(a, "-iporder")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->iporder = std::atoi(val);
+      if (o->iporder != 3) return CB_ERR_UNSUPPORTED;
+    } else if (!std::strcmp(a, "-verbosity")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->verbosity = std::atoi(val);
+    } else if (!std::strcmp(a, "-disablesmoothing") || !std::strcmp(a, "-synthetic")) {
+      if (!std::strcmp(a, "-synthetic") && i + 1 < argc && argv[i + 1][0] != '-') ++i;
+    } else {
+      return CB_ERR_ARG;
+    }
+  }
+  return CB_OK;
+}
+
+long long claire_b200_estimate_bytes(const claire_b200_opts* o, int nbatch) {
+  if (!o) return -1;
+  return Solver::estimate_bytes(*o, nbatch);
+}
+
+int claire_b200_create(const claire_b200_opts* o, int nbatch, claire_b200_ctx** out) {
+  if (!o || !out) return CB_ERR_ARG;
+  *out = nullptr;
+  claire_b200_ctx* c = new (std::nothrow) claire_b200_ctx();
+  if (!c) return CB_ERR_ALLOC;
+  int e = c->solver.init(*o, nbatch);
+  if (e) {
+    delete c;
+    return e < 0 ? e : CB_ERR_CUDA;
+  }
+  *out = c;
+  return CB_OK;
+}
+
+int claire_b200_destroy(claire_b200_ctx* c) {
+  delete c;
+  return CB_OK;
+}
+
+const char* claire_b200_last_error(const claire_b200_ctx* c) {
+  if (!c) return "null context";
+  return c->solver.err.c_str();
+}
+
+long long claire_b200_footprint_bytes(const claire_b200_ctx* c) { return c ? c->solver.footprint() : -1; }
+
+int claire_b200_set_problem_opts(claire_b200_ctx* c, int b, const claire_b200_opts* o) {
+  if (!c || !o) return CB_ERR_ARG;
+  return c->solver.set_problem(b, *o);
+}
+
+static int copy_in(Solver& s, float* dst, const float* src, long long count, int on_device) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * count,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s.stream);
+  if (e != cudaSuccess) return CB_ERR_CUDA;
+  return cudaStreamSynchronize(s.stream) == cudaSuccess ? CB_OK : CB_ERR_CUDA;
+}
+
+static int copy_out(Solver& s, float* dst, const float* src, long long count, int on_device) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, sizeof(float) * count,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s.stream);
+  if (e != cudaSuccess) return CB_ERR_CUDA;
+  return cudaStreamSynchronize(s.stream) == cudaSuccess ? CB_OK : CB_ERR_CUDA;
+}
+
+int claire_b200_set_images(claire_b200_ctx* c, int b, const float* mR, const float* mT, int on_device) {
+  if (!c || !mR || !mT || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = copy_in(s, s.mR + b * s.n, mR, s.n, on_device);
+  if (!e) e = copy_in(s, s.mT + b * s.n, mT, s.n, on_device);
+  s.state_of[b] = 0;
+  return e;
+}
+
+int claire_b200_set_velocity(claire_b200_ctx* c, int b, const float* v, int on_device) {
+  if (!c || !v || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  s.state_of[b] = 0;
+  return copy_in(s, s.v + b * 3 * s.n, v, 3 * s.n, on_device);
+}
+
+int claire_b200_get_velocity(const claire_b200_ctx* c, int b, float* v, int on_device) {
+  if (!c || !v || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = const_cast<Solver&>(c->solver);
+  return copy_out(s, v, s.v + b * 3 * s.n, 3 * s.n, on_device);
+}
+
+int claire_b200_run(claire_b200_ctx* c) {
+  if (!c) return CB_ERR_ARG;
+  std::vector<int> sel(c->solver.B, 1);
+  return cuda_status(c->solver.run(sel));
+}
+
+int claire_b200_run_masked(claire_b200_ctx* c, const int* mask) {
+  if (!c || !mask) return CB_ERR_ARG;
+  std::vector<int> sel(mask, mask + c->solver.B);
+  return cuda_status(c->solver.run(sel));
+}
+
+int claire_b200_get_final_state(claire_b200_ctx* c, int b, float* m1, int on_device) {
+  if (!c || !m1 || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  float* tmp = nullptr;
+  if (!on_device) {
+    if (cudaMalloc(&tmp, sizeof(float) * s.n) != cudaSuccess) return CB_ERR_ALLOC;
+  }
+  int e = s.final_state(on_device ? m1 : tmp, b);
+  if (!e && !on_device) e = copy_out(s, m1, tmp, s.n, 0);
+  if (tmp) cudaFree(tmp);
+  return cuda_status(e);
+}
+
+int claire_b200_forward(claire_b200_ctx* c, int b, const float* m0, float* m1, int on_device) {
+  if (!c || !m0 || !m1 || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  // stage through the work field r (problem stride 3n, first n entries)
+  float* in = s.r + b * 3 * s.n;
+  float* out = s.z + b * 3 * s.n;
+  int e = copy_in(s, in, m0, s.n, on_device);
+  if (e) return e;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  // forward() uses a problem stride of n for m0/m1: pass shifted bases
+  e = s.forward(s.r + b * 3 * s.n - b * s.n, s.z + b * 3 * s.n - b * s.n, sel);
+  if (e) return cuda_status(e);
+  return copy_out(s, m1, out, s.n, on_device);
+}
+
+int claire_b200_get_stats(const claire_b200_ctx* c, int b, claire_b200_stats* st) {
+  if (!c || !st || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  const ProbState& p = c->solver.ps[b];
+  st->gn_iterations = p.iter;
+  st->pcg_iterations = p.pcg_total;
+  st->obj_evals = p.obj_evals;
+  st->grad_evals = p.grad_evals;
+  st->hess_matvecs = p.hess_matvecs;
+  st->pc_matvecs = p.pc_matvecs;
+  st->pde_solves = p.pde_solves;
+  st->converged_reason = p.reason;
+  st->J = p.J;
+  st->J0 = p.J0;
+  st->D = p.D;
+  st->D0 = p.D0;
+  st->R = p.R;
+  st->gnorm = p.gnorm;
+  st->gnorm0 = p.gnorm0;
+  st->rel_mismatch = p.rel_mismatch;
+  st->seconds = p.seconds;
+  return CB_OK;
+}
+
+int claire_b200_objective(claire_b200_ctx* c, int b, const float* v, double* J, double* D, double* R) {
+  if (!c || !v || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = claire_b200_set_velocity(c, b, v, 0);
+  if (e) return e;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  e = s.objective_at(s.v, sel);
+  if (e) return cuda_status(e);
+  if (J) *J = s.ps[b].J;
+  if (D) *D = s.ps[b].D;
+  if (R) *R = s.ps[b].R;
+  return CB_OK;
+}
+
+int claire_b200_gradient(claire_b200_ctx* c, int b, const float* v, float* gout) {
+  if (!c || !v || !gout || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = claire_b200_set_velocity(c, b, v, 0);
+  if (e) return e;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  e = s.gradient_at_current(sel);
+  if (e) return cuda_status(e);
+  return copy_out(s, gout, s.g + b * 3 * s.n, 3 * s.n, 0);
+}
+
+int claire_b200_hessian_matvec(claire_b200_ctx* c, int b, const float* v, const float* vt, float* hvt) {
+  if (!c || !v || !vt || !hvt || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = claire_b200_set_velocity(c, b, v, 0);
+  if (e) return e;
+  e = copy_in(s, s.pv + b * 3 * s.n, vt, 3 * s.n, 0);
+  if (e) return e;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  e = s.hessian_matvec(s.pv, s.q, sel);
+  if (e) return cuda_status(e);
+  return copy_out(s, hvt, s.q + b * 3 * s.n, 3 * s.n, 0);
+}
+
+int claire_b200_precond(claire_b200_ctx* c, int b, const float* xin, float* px) {
+  if (!c || !xin || !px || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = copy_in(s, s.r + b * 3 * s.n, xin, 3 * s.n, 0);
+  if (e) return e;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  e = s.precond(s.r, s.z, sel);
+  if (e) return cuda_status(e);
+  return copy_out(s, px, s.z + b * 3 * s.n, 3 * s.n, 0);
+}
+
+int claire_b200_get_adjoint(claire_b200_ctx* c, int b, float* lambda0, float* body_force) {
+  if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  int e = CB_OK;
+  if (lambda0) e = copy_out(s, lambda0, s.lam + b * s.n, s.n, 0);
+  if (!e && body_force) e = copy_out(s, body_force, s.bf + b * 3 * s.n, 3 * s.n, 0);
+  return e;
+}
+
+int claire_b200_synchronize(claire_b200_ctx* c) {
+  if (!c) return CB_ERR_ARG;
+  return cudaStreamSynchronize(c->solver.stream) == cudaSuccess ? CB_OK : CB_ERR_CUDA;
+}
+
+int claire_b200_set_stream(claire_b200_ctx* c, void* stream) {
+  if (!c) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  if (cudaStreamSynchronize(s.stream) != cudaSuccess) return CB_ERR_CUDA;
+  s.stream = stream ? (cudaStream_t)stream : s.own_stream;
+  return CB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operator seams; scratch comes from the stream-ordered allocator
+// ---------------------------------------------------------------------------
+static bool dims_ok(const int nx[3]) {
+  return nx && nx[0] > 0 && nx[1] > 0 && nx[2] > 0;
+}
+static bool fft_ok(const int nx[3]) {
+  return nx[0] == nx[1] && nx[1] == nx[2] && fft_size_supported(nx[0]);
+}
+
+int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt, int flag, void* stream) {
+  if (!v || !disp || !dims_ok(nx) || nt < 1 || (flag != 0 && flag != 1)) return CB_ERR_ARG;
+  Dims d{nx[0], nx[1], nx[2]};
+  const float sign = flag == 0 ? 1.f : -1.f;
+  note_launches(1);
+  return cuda_status(launch_trajectory(v, 0, disp, 0, 1, d, (float)(1.0 / nt), sign, nullptr, (cudaStream_t)stream));
+}
+
+int claire_b200_interp3(const float* f, const float* disp, float* out, const int nx[3], int dof, void* stream) {
+  if (!f || !disp || !out || !dims_ok(nx) || (dof != 1 && dof != 3)) return CB_ERR_ARG;
+  Dims d{nx[0], nx[1], nx[2]};
+  note_launches(1);
+  return cuda_status(launch_interp(f, 0, d.n(), disp, 0, out, 0, d.n(), dof, 1, d, nullptr, (cudaStream_t)stream));
+}
+
+int claire_b200_fft_grad(const float* f, float* gout, const int nx[3], void* stream) {
+  if (!f || !gout || !dims_ok(nx)) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  const long long n = d.n();
+  for (int a = 0; a < 3; ++a) {
+    int e = launch_deriv(f, 0, n, gout + a * n, 0, n, 1, 1, d, a, EPI_STORE, nullptr, 0, nullptr, (cudaStream_t)stream);
+    if (e) return cuda_status(e);
+  }
+  note_launches(3);
+  return CB_OK;
+}
+
+int claire_b200_fft_div(const float* v, float* dout, const int nx[3], void* stream) {
+  if (!v || !dout || !dims_ok(nx)) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  const long long n = d.n();
+  for (int a = 0; a < 3; ++a) {
+    int e = launch_deriv(v + a * n, 0, n, dout, 0, n, 1, 1, d, a, a == 0 ? EPI_STORE : EPI_ADD, nullptr, 0, nullptr,
+                         (cudaStream_t)stream);
+    if (e) return cuda_status(e);
+  }
+  note_launches(3);
+  return CB_OK;
+}
+
+// scratch for a 3-field spectral op: spectrum, params, partials, result slot
+struct Scratch {
+  float2* spec = nullptr;
+  SpecParams* params = nullptr;
+  double* partials = nullptr;
+  double* result = nullptr;
+  cudaStream_t s = nullptr;
+  int alloc(const Dims& d, int nparts, cudaStream_t st) {
+    s = st;
+    if (cudaMallocAsync((void**)&spec, sizeof(float2) * 3 * d.nc(), s) != cudaSuccess) return CB_ERR_ALLOC;
+    if (cudaMallocAsync((void**)&params, sizeof(SpecParams), s) != cudaSuccess) return CB_ERR_ALLOC;
+    if (cudaMallocAsync((void**)&partials, sizeof(double) * (nparts + 1), s) != cudaSuccess) return CB_ERR_ALLOC;
+    result = partials + nparts;
+    return CB_OK;
+  }
+  ~Scratch() {
+    if (spec) cudaFreeAsync(spec, s);
+    if (params) cudaFreeAsync(params, s);
+    if (partials) cudaFreeAsync(partials, s);
+  }
+};
+
+static SpecParams make_params(const Dims& d, int regnorm, const double* beta, double beta2) {
+  SpecParams p{};
+  p.norm = regnorm;
+  p.beta0 = beta ? (float)beta[0] : 0.f;
+  p.beta1 = beta ? (float)beta[1] : 0.f;
+  p.beta2 = (float)beta2;
+  p.hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
+  p.sigma[0] = p.sigma[1] = p.sigma[2] = 1.f;
+  return p;
+}
+
+static int spectral3(const float* in, float* out, const Dims& d, int op, const SpecParams& hp, int epi,
+                     double* sumsq, cudaStream_t st) {
+  Scratch sc;
+  const int np = std::max(1, c2r_partials(d, 3));
+  int e = sc.alloc(d, np, st);
+  if (e) return e;
+  if (cudaMemcpyAsync(sc.params, &hp, sizeof(SpecParams), cudaMemcpyHostToDevice, st) != cudaSuccess) return CB_ERR_CUDA;
+  const long long n = d.n(), nc = d.nc();
+  e = launch_r2c3d(in, 0, n, sc.spec, 0, 3, 1, d, nullptr, st);
+  if (!e) e = launch_pencil(sc.spec, 0, 1, d, op, sc.params, 3, 3, nullptr, st);
+  if (!e) e = launch_c2r3d(sc.spec, 0, out, 0, n, 3, 1, d, epi, nullptr, sc.partials, np, nullptr, st);
+  if (!e && epi == EPI_SUMSQ) e = launch_finalize(sc.partials, np, np, sc.result, 1, 1.0, false, st);
+  note_launches(6);
+  if (e) return cuda_status(e);
+  if (epi == EPI_SUMSQ && sumsq) {
+    if (cudaMemcpyAsync(sumsq, sc.result, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CB_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return CB_ERR_CUDA;
+  }
+  (void)nc;
+  return CB_OK;
+}
+
+int claire_b200_reg_apply(const float* v, float* out, const int nx[3], int regnorm, const double beta[2],
+                          int kind, void* stream) {
+  if (!v || !out || !dims_ok(nx) || !beta || regnorm < 0 || regnorm > CB_NORM_H3SN) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  cudaStream_t st = (cudaStream_t)stream;
+  if (regnorm == CB_NORM_L2 || beta[0] == 0.0) {
+    // src/RegularizationL2.cpp:100-215: beta*v and v/beta in real space
+    double c = 1.0;
+    if (beta[0] != 0.0) c = (kind == CB_REG_GRADIENT) ? beta[0] : (kind == CB_REG_INVERSE ? 1.0 / beta[0] : 1.0 / std::sqrt(beta[0]));
+    else if (kind == CB_REG_GRADIENT) c = 0.0;
+    note_launches(1);
+    return cuda_status(launch_lincomb(out, 0, v, 0, nullptr, c, nullptr, 0, nullptr, 0.0, 3 * d.n(), 1, nullptr, st));
+  }
+  int op = kind == CB_REG_GRADIENT ? OP_REG_GRAD : (kind == CB_REG_INVERSE ? OP_REG_INV : OP_REG_SQRTINV);
+  return spectral3(v, out, d, op, make_params(d, regnorm, beta, 0.0), EPI_STORE, nullptr, st);
+}
+
+int claire_b200_reg_functional(const float* v, double* R, const int nx[3], int regnorm, const double beta[2],
+                               void* stream) {
+  if (!v || !R || !dims_ok(nx) || !beta || regnorm < 0 || regnorm > CB_NORM_H3SN) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  cudaStream_t st = (cudaStream_t)stream;
+  const double hd = (kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3);
+  if (beta[0] == 0.0) {
+    *R = 0.0;
+    return CB_OK;
+  }
+  const long long n = d.n();
+  if (regnorm == CB_NORM_H1 || regnorm == CB_NORM_H1SN || regnorm == CB_NORM_L2) {
+    int np = dot_partials(3 * n);
+    for (int a = 0; a < 3; ++a) np = std::max(np, deriv_partials(d, a, 3));
+    double* buf = nullptr;
+    if (cudaMallocAsync((void**)&buf, sizeof(double) * (np + 2), st) != cudaSuccess) return CB_ERR_ALLOC;
+    double* res = buf + np;
+    int e = 0;
+    if (regnorm != CB_NORM_L2) {
+      for (int a = 0; a < 3 && !e; ++a) {
+        const int p = deriv_partials(d, a, 3);
+        e = launch_deriv(v, 0, n, nullptr, 0, 0, 3, 1, d, a, EPI_SUMSQ, buf, np, nullptr, st);
+        if (!e) e = launch_finalize(buf, np, p, res, 1, 1.0, a > 0, st);
+      }
+      note_launches(6);
+    }
+    if (!e) e = launch_dot(v, 0, v, 0, 3 * n, 1, buf, np, nullptr, st);
+    if (!e) e = launch_finalize(buf, np, dot_partials(3 * n), res + 1, 1, 1.0, false, st);
+    note_launches(2);
+    double h[2] = {0.0, 0.0};
+    if (!e && cudaMemcpyAsync(h, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) e = CB_ERR_CUDA;
+    if (!e && cudaStreamSynchronize(st) != cudaSuccess) e = CB_ERR_CUDA;
+    cudaFreeAsync(buf, st);
+    if (e) return cuda_status(e);
+    if (regnorm == CB_NORM_H1SN) *R = 0.5 * hd * beta[0] * h[0];
+    else if (regnorm == CB_NORM_H1) *R = 0.5 * hd * beta[0] * (h[0] + beta[1] * h[1]);
+    else *R = 0.5 * hd * beta[0] * h[1];
+    return CB_OK;
+  }
+  double s = 0.0;
+  int e = spectral3(v, nullptr, d, OP_REG_FUNC, make_params(d, regnorm, beta, 0.0), EPI_SUMSQ, &s, st);
+  if (e) return e;
+  if (regnorm == CB_NORM_H2SN || regnorm == CB_NORM_H3SN) *R = 0.5 * hd * beta[0] * s;
+  else *R = 0.5 * hd * s;
+  return CB_OK;
+}
+
+int claire_b200_leray(float* b, const int nx[3], int model, const double beta[3], void* stream) {
+  if (!b || !dims_ok(nx) || (model != CB_MODEL_STOKES && model != CB_MODEL_RELAXEDSTOKES)) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  double bb[2] = {beta ? beta[0] : 1e-2, beta ? beta[1] : 1e-4};
+  SpecParams p = make_params(d, CB_NORM_H1SN, bb, beta ? beta[2] : 1e-4);
+  return spectral3(b, b, d, model == CB_MODEL_STOKES ? OP_LERAY : OP_LERAY_RELAXED, p, EPI_ADD, nullptr,
+                   (cudaStream_t)stream);
+}
+
+int claire_b200_smooth(const float* f, float* out, const int nx[3], const double sigma[3], void* stream) {
+  if (!f || !out || !dims_ok(nx) || !sigma) return CB_ERR_ARG;
+  if (!fft_ok(nx)) return CB_ERR_UNSUPPORTED;
+  Dims d{nx[0], nx[1], nx[2]};
+  cudaStream_t st = (cudaStream_t)stream;
+  Scratch sc;
+  int e = sc.alloc(d, 1, st);
+  if (e) return e;
+  SpecParams p = make_params(d, 0, nullptr, 0.0);
+  for (int k = 0; k < 3; ++k) p.sigma[k] = (float)sigma[k];
+  if (cudaMemcpyAsync(sc.params, &p, sizeof(SpecParams), cudaMemcpyHostToDevice, st) != cudaSuccess) return CB_ERR_CUDA;
+  const long long n = d.n();
+  e = launch_r2c3d(f, 0, n, sc.spec, 0, 1, 1, d, nullptr, st);
+  if (!e) e = launch_pencil(sc.spec, 0, 1, d, OP_GAUSS, sc.params, 1, 1, nullptr, st);
+  if (!e) e = launch_c2r3d(sc.spec, 0, out, 0, n, 1, 1, d, EPI_STORE, nullptr, nullptr, 0, nullptr, st);
+  note_launches(5);
+  return cuda_status(e);
+}
+
+int claire_b200_distance(const float* mR, const float* m1, const int nx[3], double* D, void* stream) {
+  if (!mR || !m1 || !D || !dims_ok(nx)) return CB_ERR_ARG;
+  Dims d{nx[0], nx[1], nx[2]};
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = d.n();
+  const int np = dot_partials(n);
+  double* buf = nullptr;
+  if (cudaMallocAsync((void**)&buf, sizeof(double) * (np + 1), st) != cudaSuccess) return CB_ERR_ALLOC;
+  const double hd = (kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3);
+  int e = launch_diff_sumsq(mR, 0, m1, 0, n, 1, buf, np, nullptr, st);
+  if (!e) e = launch_finalize(buf, np, np, buf + np, 1, 0.5 * hd, false, st);
+  note_launches(2);
+  if (!e && cudaMemcpyAsync(D, buf + np, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) e = CB_ERR_CUDA;
+  if (!e && cudaStreamSynchronize(st) != cudaSuccess) e = CB_ERR_CUDA;
+  cudaFreeAsync(buf, st);
+  return cuda_status(e);
+}
+
+long long claire_b200_kernel_launches(void) { return launches(); }
+
+}  // extern "C"

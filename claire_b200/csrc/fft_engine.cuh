@@ -1,0 +1,190 @@
+// In-shared-memory batched complex FFT engine (mixed radix, Stockham).
+//
+// A CTA transforms `nlines` complex lines of length N that live in shared
+// memory as split real/imaginary arrays: element e of line p sits at
+// re[e*pitch + p], im[e*pitch + p] (line index fastest, pitch odd so that
+// consecutive lines hit distinct banks).  Every plan has exactly two radix
+// stages (N = R0*R1, R0, R1 in {4, 8, 12, 16}), each an in-register DFT
+// followed by one shared-memory exchange, so the result lands back in the
+// source buffer after one ping-pong through the scratch buffer.
+//
+// Stockham stage with radix R and span Ns (product of earlier radices):
+//   for j in [0, N/R): k = j mod Ns
+//     v[r] = x[j + r*N/R] * W_N^(r*k*N/(Ns*R));  v = DFT_R(v)
+//     y[(j - k)*R + k + r*Ns] = v[r]
+// Twiddles W_N^m = exp(-2*pi*i*m/N) come from a table computed on the host
+// in double precision and staged in shared memory.
+#pragma once
+
+#include "common.cuh"
+
+namespace cb {
+
+// exp(-2*pi*i*m/16) and exp(-2*pi*i*m/12), m = 0..R-1.
+__device__ __constant__ float2 kTw16[16] = {
+    {1.000000000f, -0.000000000f}, {0.923879533f, -0.382683432f}, {0.707106781f, -0.707106781f},
+    {0.382683432f, -0.923879533f}, {0.000000000f, -1.000000000f}, {-0.382683432f, -0.923879533f},
+    {-0.707106781f, -0.707106781f}, {-0.923879533f, -0.382683432f}, {-1.000000000f, -0.000000000f},
+    {-0.923879533f, 0.382683432f}, {-0.707106781f, 0.707106781f}, {-0.382683432f, 0.923879533f},
+    {-0.000000000f, 1.000000000f}, {0.382683432f, 0.923879533f}, {0.707106781f, 0.707106781f},
+    {0.923879533f, 0.382683432f}};
+__device__ __constant__ float2 kTw12[12] = {
+    {1.000000000f, -0.000000000f}, {0.866025404f, -0.500000000f}, {0.500000000f, -0.866025404f},
+    {0.000000000f, -1.000000000f}, {-0.500000000f, -0.866025404f}, {-0.866025404f, -0.500000000f},
+    {-1.000000000f, -0.000000000f}, {-0.866025404f, 0.500000000f}, {-0.500000000f, 0.866025404f},
+    {-0.000000000f, 1.000000000f}, {0.500000000f, 0.866025404f}, {0.866025404f, 0.500000000f}};
+
+CB_DEVICE float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+CB_DEVICE float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+CB_DEVICE float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+CB_DEVICE float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// W_R^m (forward) or its conjugate (inverse), R divides 16 or 12.
+template <int R, bool INV>
+CB_DEVICE float2 wsmall(int m) {
+  float2 w;
+  if (16 % R == 0) w = kTw16[(m * (16 / R)) % 16];
+  else w = kTw12[(m * (12 / R)) % 12];
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+template <int R> struct Factor;
+template <> struct Factor<6> { static constexpr int A = 2, B = 3; };
+template <> struct Factor<8> { static constexpr int A = 2, B = 4; };
+template <> struct Factor<12> { static constexpr int A = 3, B = 4; };
+template <> struct Factor<16> { static constexpr int A = 4, B = 4; };
+
+template <int R, bool INV> struct Dft;
+
+template <bool INV> struct Dft<2, INV> {
+  static CB_DEVICE void run(float2 (&v)[2]) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <bool INV> struct Dft<3, INV> {
+  static CB_DEVICE void run(float2 (&v)[3]) {
+    const float s = INV ? -0.866025404f : 0.866025404f;
+    float2 t = cadd(v[1], v[2]);
+    float2 u = csub(v[1], v[2]);
+    float2 a = make_float2(v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y);
+    // -i*s*u = (s*u.y, -s*u.x)
+    float2 r = make_float2(s * u.y, -s * u.x);
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(a, r);
+    v[2] = csub(a, r);
+  }
+};
+
+template <bool INV> struct Dft<4, INV> {
+  static CB_DEVICE void run(float2 (&v)[4]) {
+    float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    float2 t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
+    // forward: y1 = t1 - i*t3, y3 = t1 + i*t3
+    float2 it3 = INV ? make_float2(-t3.y, t3.x) : make_float2(t3.y, -t3.x);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, it3);
+    v[3] = csub(t1, it3);
+  }
+};
+
+// Composite R = A*B: X[k1 + A*k2] = sum_n2 W_B^(n2 k2) W_R^(n2 k1) sum_n1 x[B n1 + n2] W_A^(n1 k1)
+template <int R, bool INV> struct Dft {
+  static CB_DEVICE void run(float2 (&v)[R]) {
+    constexpr int A = Factor<R>::A, B = Factor<R>::B;
+    float2 y[A][B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      float2 t[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) t[n1] = v[B * n1 + n2];
+      Dft<A, INV>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) {
+        y[k1][n2] = (n2 * k1 == 0) ? t[k1] : cmul(t[k1], wsmall<R, INV>(n2 * k1));
+      }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      float2 t[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) t[n2] = y[k1][n2];
+      Dft<B, INV>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = t[k2];
+    }
+  }
+};
+
+// Two-stage plans N = R0 * R1.
+template <int N> struct Plan;
+template <> struct Plan<16> { static constexpr int R0 = 4, R1 = 4; };
+template <> struct Plan<32> { static constexpr int R0 = 4, R1 = 8; };
+template <> struct Plan<48> { static constexpr int R0 = 12, R1 = 4; };
+template <> struct Plan<64> { static constexpr int R0 = 8, R1 = 8; };
+template <> struct Plan<96> { static constexpr int R0 = 12, R1 = 8; };
+template <> struct Plan<128> { static constexpr int R0 = 16, R1 = 8; };
+template <> struct Plan<192> { static constexpr int R0 = 12, R1 = 16; };
+template <> struct Plan<256> { static constexpr int R0 = 16, R1 = 16; };
+
+template <int N, int R, int NS, bool INV>
+CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict__ sim,
+                         float* __restrict__ dre, float* __restrict__ dim, int nlines,
+                         int pitch, const float2* __restrict__ tw) {
+  constexpr int J = N / R;
+  const int total = nlines * J;
+  for (int u = threadIdx.x; u < total; u += blockDim.x) {
+    const int p = u % nlines;
+    const int j = u / nlines;
+    const int k = j % NS;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int idx = (j + r * J) * pitch + p;
+      v[r] = make_float2(sre[idx], sim[idx]);
+    }
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k * (N / (NS * R))];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    Dft<R, INV>::run(v);
+    const int o = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int idx = (o + r * NS) * pitch + p;
+      dre[idx] = v[r].x;
+      dim[idx] = v[r].y;
+    }
+  }
+}
+
+// Transform nlines lines held in (re, im); (sre, sim) is scratch of the same
+// size.  The result is back in (re, im).  Caller synchronises before; this
+// function synchronises after each stage.
+template <int N, bool INV>
+CB_DEVICE void fft_lines(float* re, float* im, float* sre, float* sim, int nlines, int pitch,
+                         const float2* tw) {
+  using P = Plan<N>;
+  fft_stage<N, P::R0, 1, INV>(re, im, sre, sim, nlines, pitch, tw);
+  __syncthreads();
+  fft_stage<N, P::R1, P::R0, INV>(sre, sim, re, im, nlines, pitch, tw);
+  __syncthreads();
+}
+
+// Stage the N-entry twiddle table into shared memory.
+template <int N>
+CB_DEVICE void load_twiddles(float2* dst, const float2* __restrict__ src) {
+  for (int i = threadIdx.x; i < N; i += blockDim.x) dst[i] = src[i];
+}
+
+}  // namespace cb

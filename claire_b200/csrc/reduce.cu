@@ -1,0 +1,111 @@
+// FP64 reductions (dot products, squared distances) and fused elementwise
+// vector updates used by the distance, the PCG and the line search.
+//
+// Replaces PETSc VecTDot / VecNorm / VecAXPY / VecWAXPY on the hot path
+// (e.g. src/RegularizationH1.cpp:105-143, src/VecField.cpp:577-694) and the
+// serial loop of src/DistanceMeasureSL2.cpp:119-150.
+#include "reduce.cuh"
+#include "sl.cuh"
+
+namespace cb {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 148 * 2;  // per problem; one wave on 148 SMs
+
+int dot_partials(long long len) {
+  long long need = (len + kRedThreads * 4 - 1) / (kRedThreads * 4);
+  return (int)(need < kRedBlocks ? (need < 1 ? 1 : need) : kRedBlocks);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_dot(const float* __restrict__ a, long long ap,
+                                                      const float* __restrict__ b, long long bp,
+                                                      long long len, double* __restrict__ partials,
+                                                      int nparts, const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const float* pa = a + blockIdx.y * ap;
+  const float* pb = b + blockIdx.y * bp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x)
+    acc += (double)pa[i] * (double)pb[i];
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_diff_sumsq(const float* __restrict__ a, long long ap,
+                                                             const float* __restrict__ b, long long bp,
+                                                             long long len, double* __restrict__ partials,
+                                                             int nparts, const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const float* pa = a + blockIdx.y * ap;
+  const float* pb = b + blockIdx.y * bp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double d = (double)pa[i] - (double)pb[i];
+    acc += d * d;
+  }
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+__global__ void k_finalize(const double* __restrict__ partials, int stride, int nparts,
+                           double* __restrict__ out, double scale, int accumulate) {
+  const double* p = partials + (long long)blockIdx.x * stride;
+  double acc = 0.0;
+  // fixed-order: thread t sums entries t, t+32, ...; then a fixed shuffle tree
+  for (int i = threadIdx.x; i < nparts; i += 32) acc += p[i];
+  acc = warp_sum(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = (accumulate ? out[blockIdx.x] : 0.0) + scale * acc;
+}
+
+int launch_finalize(const double* partials, int stride, int count, double* out, int nprob, double scale,
+                    bool accumulate, cudaStream_t s) {
+  k_finalize<<<nprob, 32, 0, s>>>(partials, stride, count, out, scale, accumulate ? 1 : 0);
+  return (int)cudaGetLastError();
+}
+
+int launch_dot(const float* a, long long ap, const float* b, long long bp, long long len, int nprob,
+               double* partials, int stride, const int* active, cudaStream_t s) {
+  dim3 grid(dot_partials(len), nprob);
+  k_dot<<<grid, kRedThreads, 0, s>>>(a, ap, b, bp, len, partials, stride, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_diff_sumsq(const float* a, long long ap, const float* b, long long bp, long long len,
+                      int nprob, double* partials, int stride, const int* active, cudaStream_t s) {
+  dim3 grid(dot_partials(len), nprob);
+  k_diff_sumsq<<<grid, kRedThreads, 0, s>>>(a, ap, b, bp, len, partials, stride, active);
+  return (int)cudaGetLastError();
+}
+
+// y = (sa*ca[p]) * a + (sb*cb[p]) * b   (ca / cb may be null: coefficient sa / sb)
+// Inactive problems (active[p] == 0) are skipped.
+__global__ void k_lincomb(float* y, long long yp, const float* a, long long ap,
+                          const double* __restrict__ ca, double sa, const float* b,
+                          long long bp, const double* __restrict__ cb, double sb, long long len,
+                          const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const float fa = (float)(sa * (ca ? ca[p] : 1.0));
+  const float fb = b ? (float)(sb * (cb ? cb[p] : 1.0)) : 0.f;
+  float* py = y + p * yp;
+  const float* pa = a + p * ap;
+  const float* pb = b ? b + p * bp : nullptr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    float v = fa * pa[i];
+    if (pb) v += fb * pb[i];
+    py[i] = v;
+  }
+}
+
+int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
+                   const float* b, long long bp, const double* cb, double sb, long long len,
+                   int nprob, const int* active, cudaStream_t s) {
+  long long blocks = (len + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  dim3 grid((unsigned)blocks, nprob);
+  k_lincomb<<<grid, 256, 0, s>>>(y, yp, a, ap, ca, sa, b, bp, cb, sb, len, active);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace cb

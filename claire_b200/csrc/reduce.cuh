@@ -1,0 +1,53 @@
+// Deterministic FP64 reductions and fused vector updates.
+//
+// Reductions are two-level: each CTA reduces its share in FP64 with warp
+// shuffles and stores one partial per CTA; a finalize kernel sums a problem's
+// partials in a fixed order.  The result does not depend on scheduling, so a
+// problem gives the same numbers alone and inside a batch.
+#pragma once
+
+#include "common.cuh"
+
+namespace cb {
+
+CB_DEVICE double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the CTA; thread 0 stores the result to dst[idx].  All threads of
+// the CTA must call it.
+CB_DEVICE void block_reduce_store(double v, double* dst, int idx) {
+  __shared__ double ws[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double t = (lane < nw) ? ws[lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) dst[idx] = t;
+  }
+}
+
+// Host launchers.  Problem p's partials start at partials + p*stride.
+// out[p] = scale * sum(partials[p][0..count)) (+ out[p] when accumulate).
+int launch_finalize(const double* partials, int stride, int count, double* out, int nprob, double scale,
+                    bool accumulate, cudaStream_t s);
+
+// Partials written by the dot / norm kernels for vectors of length len.
+int dot_partials(long long len);
+
+// partials[p*stride + k], k < dot_partials(len) <- partial sums of a[p][i]*b[p][i]
+// (FP32 inputs, FP64 sums).  Inactive problems are skipped.
+int launch_dot(const float* a, long long ap, const float* b, long long bp, long long len, int nprob,
+               double* partials, int stride, const int* active, cudaStream_t s);
+
+// same layout, partial sums of (a[p][i] - b[p][i])^2
+int launch_diff_sumsq(const float* a, long long ap, const float* b, long long bp, long long len,
+                      int nprob, double* partials, int stride, const int* active, cudaStream_t s);
+
+}  // namespace cb

@@ -1,0 +1,110 @@
+// Semi-Lagrangian transport: tricubic gathers and fused time-step kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace cb {
+
+// Tricubic Lagrange stencil at point i + disp (grid units), periodic.
+// Reference: src/interp3.cpp:2492-2719 (base = floor(q) - 1, t = q - base in
+// [1,2), w_k(t) = c_k prod_{l != k}(t - l)).  With s = t - 1 = frac(disp):
+//   w0 = -s(s-1)(s-2)/6, w1 = (s+1)(s-1)(s-2)/2, w2 = -(s+1)s(s-2)/2,
+//   w3 = (s+1)s(s-1)/6.
+// Splitting q = i + disp into floor/frac on the displacement keeps the
+// fraction exact to float precision for every grid size.
+struct Stencil {
+  int o1[4], o2[4], o3[4];
+  float w1[4], w2[4], w3[4];
+};
+
+CB_DEVICE void axis_stencil(int i, float disp, int n, int stride, int (&o)[4], float (&w)[4]) {
+  const float fl = floorf(disp);
+  const float s = disp - fl;
+  int b = wrap(i + (int)fl - 1, n);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    o[k] = b * stride;
+    b = (b + 1 == n) ? 0 : b + 1;
+  }
+  const float sm1 = s - 1.f, sm2 = s - 2.f, sp1 = s + 1.f;
+  w[0] = (-1.f / 6.f) * s * sm1 * sm2;
+  w[1] = 0.5f * sp1 * sm1 * sm2;
+  w[2] = -0.5f * sp1 * s * sm2;
+  w[3] = (1.f / 6.f) * sp1 * s * sm1;
+}
+
+CB_DEVICE void make_stencil(int i1, int i2, int i3, float d1, float d2, float d3, const Dims& d,
+                            Stencil& st) {
+  axis_stencil(i1, d1, d.n1, d.n2 * d.n3, st.o1, st.w1);
+  axis_stencil(i2, d2, d.n2, d.n3, st.o2, st.w2);
+  axis_stencil(i3, d3, d.n3, 1, st.o3, st.w3);
+}
+
+// Sum over one x1 plane of the stencil (16 taps).
+CB_DEVICE float gather_plane(const float* __restrict__ plane, const Stencil& st) {
+  float acc = 0.f;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const float* row = plane + st.o2[b];
+    const float r = st.w3[0] * __ldg(row + st.o3[0]) + st.w3[1] * __ldg(row + st.o3[1]) +
+                    st.w3[2] * __ldg(row + st.o3[2]) + st.w3[3] * __ldg(row + st.o3[3]);
+    acc += st.w2[b] * r;
+  }
+  return acc;
+}
+
+// 64-tap gather.  The x1 planes are visited one after another (16 loads in
+// flight per thread) so the kernel stays at a register count that keeps 32+
+// warps resident per SM; the plane loop selects offsets and weights with
+// compile-time indices only.
+CB_DEVICE float gather(const float* __restrict__ f, const Stencil& st) {
+  float acc = st.w1[0] * gather_plane(f + st.o1[0], st);
+  acc += st.w1[1] * gather_plane(f + st.o1[1], st);
+  acc += st.w1[2] * gather_plane(f + st.o1[2], st);
+  acc += st.w1[3] * gather_plane(f + st.o1[3], st);
+  return acc;
+}
+
+CB_DEVICE void point_index(long long i, const Dims& d, int& i1, int& i2, int& i3) {
+  i3 = (int)(i % d.n3);
+  const long long t = i / d.n3;
+  i2 = (int)(t % d.n2);
+  i1 = (int)(t / d.n2);
+}
+
+// ---- host launchers ---------------------------------------------------------
+// disp[p] (3 fields, each n) <- RK2 characteristic of v[p]; sign +1 state, -1 adjoint.
+int launch_trajectory(const float* v, long long vp, float* disp, long long dp, int nprob,
+                      const Dims& d, float ht, float sign, const int* active, cudaStream_t s);
+
+// out[p][f] <- f[p][f](i + disp[p](i)), f = 0..nf-1; fields ff apart.
+int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp,
+                  float* out, long long op, long long of, int nf, int nprob, const Dims& d,
+                  const int* active, cudaStream_t s);
+
+// One backward RK2 step of the (incremental) adjoint with body-force update
+// (src/CLAIRE.cpp:2646-2686, 3940-3971):
+//   lx = lam_in(X); rhs0 = lx*divvx; rhs1 = (lx + ht*rhs0)*divv;
+//   b += w * g * lam_in;  lam_out = lx + ht/2 (rhs0 + rhs1)
+int launch_adjoint_step(const float* lam_in, float* lam_out, long long lp, const float* disp,
+                        long long dp, const float* divv, const float* divvx, long long vp,
+                        const float* g, long long gp, float* b, long long bp, float ht, float w,
+                        int nprob, const Dims& d, const int* active, cudaStream_t s);
+
+// b = hd_scale * (b + w * g * lam)   (t = 0 trapezoid term, src/CLAIRE.cpp:2689-2709)
+int launch_body_force_final(float* b, long long bp, const float* g, long long gp, const float* lam,
+                            long long lp, float w, float hd_scale, int nprob, long long n,
+                            const int* active, cudaStream_t s);
+
+// One incremental state step (src/CLAIRE.cpp:3220-3276):
+//   mt_out = mt_in(X) - ht/2 * (gx . vtx) - ht/2 * (g1 . vt)
+int launch_incstate_step(const float* mt_in, float* mt_out, long long mp, const float* disp,
+                         long long dp, const float* gx, long long gxp, const float* vtx,
+                         const float* g1, long long g1p, const float* vt, long long vtp, float ht,
+                         int nprob, const Dims& d, const int* active, cudaStream_t s);
+
+int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
+                   const float* b, long long bp, const double* cb, double sb, long long len,
+                   int nprob, const int* active, cudaStream_t s);
+
+}  // namespace cb

@@ -1,0 +1,815 @@
+// Gauss-Newton-Krylov driver (host C++) for a batch of registration problems.
+//
+// Restates, for one GPU, the control flow of the reference's
+// CLAIREInterface::RunSolver -> Optimizer::Run -> TAO nls (PETSc 3.9.1) with
+// KSPCG + PCSHELL (INVREG) + Armijo (src/CLAIREInterface.cpp:771-885,
+// src/Optimizer.cpp:235-530, src/TaoInterface.cpp:40-606,
+// src/KrylovInterface.cpp:79-196), and the problem class CLAIRE's objective /
+// gradient / GN Hessian matvec (src/CLAIRE.cpp:227-357, 793-1042,
+// 1218-1379).  Scalars that steer the PCG (alpha, beta, residual checks) are
+// computed on the device; the host reads one flag vector per PCG iteration.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "reduce.cuh"
+#include "sl.cuh"
+#include "solver.cuh"
+
+namespace cb {
+
+#define CB_TRY(x)                      \
+  do {                                 \
+    int _e = (x);                      \
+    if (_e) return _e;                 \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// small scalar kernels (one thread per problem)
+// ---------------------------------------------------------------------------
+// rn0 = sqrt(rr); tol = max(rtol*rn0, atol); stop when rn0 <= tol
+__global__ void k_pcg_init(double* __restrict__ sc, int* __restrict__ isc, int* __restrict__ act, int B,
+                           double atol) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B || !act[p]) return;
+  double* RR = sc + Solver::S_RR * B;
+  double* RN0 = sc + Solver::S_RN0 * B;
+  double* TOL = sc + Solver::S_TOL * B;
+  double* RTOL = sc + Solver::S_RTOL * B;
+  const double rn0 = sqrt(RR[p]);
+  RN0[p] = rn0;
+  TOL[p] = fmax(RTOL[p] * rn0, atol);
+  isc[Solver::I_IT * B + p] = 0;
+  isc[Solver::I_REASON * B + p] = 0;
+  if (rn0 <= TOL[p]) {
+    act[p] = 0;
+    isc[Solver::I_REASON * B + p] = 1;  // converged
+  }
+}
+
+// alpha = rz / pq, stop on non-positive curvature
+__global__ void k_pcg_alpha(double* __restrict__ sc, int* __restrict__ isc, int* __restrict__ act, int B) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B || !act[p]) return;
+  const double pq = sc[Solver::S_PQ * B + p];
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    act[p] = 0;
+    sc[Solver::S_ALPHA * B + p] = 0.0;
+    isc[Solver::I_REASON * B + p] = 3;  // indefinite
+    return;
+  }
+  sc[Solver::S_ALPHA * B + p] = sc[Solver::S_RZ * B + p] / pq;
+}
+
+// residual test after x += alpha p, r -= alpha q (KSPConvergedDefault)
+__global__ void k_pcg_check(double* __restrict__ sc, int* __restrict__ isc, int* __restrict__ act, int B,
+                            int maxit, double dtol) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B || !act[p]) return;
+  const int it = ++isc[Solver::I_IT * B + p];
+  const double rn = sqrt(sc[Solver::S_RR * B + p]);
+  if (rn <= sc[Solver::S_TOL * B + p]) {
+    act[p] = 0;
+    isc[Solver::I_REASON * B + p] = 1;
+  } else if (rn > dtol * sc[Solver::S_RN0 * B + p] || !isfinite(rn)) {
+    act[p] = 0;
+    isc[Solver::I_REASON * B + p] = 4;  // diverged
+  } else if (it >= maxit) {
+    act[p] = 0;
+    isc[Solver::I_REASON * B + p] = 2;  // maxit
+  }
+}
+
+// beta = rz_new / rz; rz = rz_new
+__global__ void k_pcg_beta(double* __restrict__ sc, int* __restrict__ act, int B) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B || !act[p]) return;
+  const double rzn = sc[Solver::S_RZNEW * B + p];
+  sc[Solver::S_BETA * B + p] = rzn / sc[Solver::S_RZ * B + p];
+  sc[Solver::S_RZ * B + p] = rzn;
+}
+
+static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+Solver::~Solver() {
+  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, gm, gx, divv, divvx, lam, lam2, bf, g, x,
+                  r, z, pv, q, vtx, mt, mt2, work3, spec, partials, dsc, dact, dint, dparams};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (hsc) cudaFreeHost(hsc);
+  if (hint) cudaFreeHost(hint);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+int Solver::alloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    err = std::string("cudaMalloc failed: ") + cudaGetErrorString(e);
+    return CB_ERR_ALLOC;
+  }
+  bytes_ += (long long)bytes;
+  return 0;
+}
+
+static int max_parts(const Dims& d) {
+  int mp = dot_partials(3 * d.n());
+  for (int a = 0; a < 3; ++a) mp = std::max(mp, deriv_partials(d, a, 3));
+  mp = std::max(mp, c2r_partials(d, 3));
+  return mp;
+}
+
+long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
+  Dims d{o.nx[0], o.nx[1], o.nx[2]};
+  const long long n = d.n(), nc = d.nc();
+  const int nt = o.nt;
+  long long floats = 0;
+  floats += 2 * n;                    // mR, mT
+  floats += 2 * 3 * n;                // v, vtrial
+  floats += (nt + 1) * n;             // state
+  floats += 2 * 3 * n;                // trajectories
+  floats += (nt + 1) * 3 * n;         // grad m cache
+  floats += nt * 3 * n;               // grad m (X) cache
+  floats += 2 * n + 2 * n + 2 * n;    // divv, divvx, lam x2, mt x2
+  floats += 3 * n * 9;                // bf, g, x, r, z, p, q, vtx, work3
+  long long bytes = floats * 4 + 3 * nc * 8;
+  bytes += (long long)max_parts(d) * 8;
+  return bytes * B;
+}
+
+int Solver::init(const claire_b200_opts& o, int Bn) {
+  opts = o;
+  B = Bn;
+  d = Dims{o.nx[0], o.nx[1], o.nx[2]};
+  nt = o.nt;
+  if (B < 1 || B > 1024 || nt < 1) {
+    err = "invalid batch size or nt";
+    return CB_ERR_ARG;
+  }
+  if (!(d.n1 == d.n2 && d.n2 == d.n3 && fft_size_supported(d.n1))) {
+    err = "grid size has no FFT plan (supported: cubic 16,32,48,64,96,128,192,256)";
+    return CB_ERR_UNSUPPORTED;
+  }
+  n = d.n();
+  nc = d.nc();
+  ht = (float)(1.0 / nt);
+  hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
+  if (cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    err = "stream creation failed";
+    return CB_ERR_CUDA;
+  }
+  stream = own_stream;
+  const size_t S = sizeof(float) * n * B, V = 3 * S;
+  CB_TRY(alloc((void**)&mR, S));
+  CB_TRY(alloc((void**)&mT, S));
+  CB_TRY(alloc((void**)&v, V));
+  CB_TRY(alloc((void**)&vtrial, V));
+  CB_TRY(alloc((void**)&m, S * (nt + 1)));
+  CB_TRY(alloc((void**)&disp_st, V));
+  CB_TRY(alloc((void**)&disp_adj, V));
+  CB_TRY(alloc((void**)&gm, V * (nt + 1)));
+  CB_TRY(alloc((void**)&gx, V * nt));
+  CB_TRY(alloc((void**)&divv, S));
+  CB_TRY(alloc((void**)&divvx, S));
+  CB_TRY(alloc((void**)&lam, S));
+  CB_TRY(alloc((void**)&lam2, S));
+  CB_TRY(alloc((void**)&mt, S));
+  CB_TRY(alloc((void**)&mt2, S));
+  CB_TRY(alloc((void**)&bf, V));
+  CB_TRY(alloc((void**)&g, V));
+  CB_TRY(alloc((void**)&x, V));
+  CB_TRY(alloc((void**)&r, V));
+  CB_TRY(alloc((void**)&z, V));
+  CB_TRY(alloc((void**)&pv, V));
+  CB_TRY(alloc((void**)&q, V));
+  CB_TRY(alloc((void**)&vtx, V));
+  CB_TRY(alloc((void**)&work3, V));
+  CB_TRY(alloc((void**)&spec, sizeof(float2) * 3 * nc * B));
+  maxparts = max_parts(d);
+  CB_TRY(alloc((void**)&partials, sizeof(double) * maxparts * B));
+  CB_TRY(alloc((void**)&dsc, sizeof(double) * NSLOT * B));
+  CB_TRY(alloc((void**)&dact, sizeof(int) * 8 * B));
+  dact2 = dact + B;
+  CB_TRY(alloc((void**)&dint, sizeof(int) * NISLOT * B));
+  CB_TRY(alloc((void**)&dparams, sizeof(SpecParams) * B));
+  if (cudaMallocHost((void**)&hsc, sizeof(double) * NSLOT * B) != cudaSuccess ||
+      cudaMallocHost((void**)&hint, sizeof(int) * NISLOT * B) != cudaSuccess) {
+    err = "pinned host allocation failed";
+    return CB_ERR_ALLOC;
+  }
+  cudaMemsetAsync(v, 0, V, stream);
+  cudaMemsetAsync(mR, 0, S, stream);
+  cudaMemsetAsync(mT, 0, S, stream);
+  cudaMemsetAsync(dsc, 0, sizeof(double) * NSLOT * B, stream);
+  cudaMemsetAsync(dint, 0, sizeof(int) * NISLOT * B, stream);
+  ps.assign(B, ProbState());
+  for (int b = 0; b < B; ++b) {
+    ps[b].norm = o.regnorm;
+    ps[b].model = o.model;
+    ps[b].beta0 = o.beta[0];
+    ps[b].beta1 = o.beta[1];
+    ps[b].beta2 = o.beta[2];
+  }
+  state_of.assign(B, 0);
+  CB_TRY(upload_params());
+  if (cudaStreamSynchronize(stream) != cudaSuccess) {
+    err = "initialisation failed";
+    return CB_ERR_CUDA;
+  }
+  return 0;
+}
+
+int Solver::set_problem(int b, const claire_b200_opts& o) {
+  if (b < 0 || b >= B) return CB_ERR_ARG;
+  if (o.nx[0] != d.n1 || o.nx[1] != d.n2 || o.nx[2] != d.n3 || o.nt != nt) {
+    err = "per-problem options must keep nx and nt";
+    return CB_ERR_ARG;
+  }
+  ps[b].norm = o.regnorm;
+  ps[b].beta0 = o.beta[0];
+  ps[b].beta1 = o.beta[1];
+  ps[b].beta2 = o.beta[2];
+  return upload_params();
+}
+
+int Solver::upload_params() {
+  std::vector<SpecParams> h(B);
+  for (int b = 0; b < B; ++b) {
+    h[b].norm = ps[b].norm;
+    h[b].beta0 = (float)ps[b].beta0;
+    h[b].beta1 = (float)ps[b].beta1;
+    h[b].beta2 = (float)ps[b].beta2;
+    h[b].hd = hd;
+    h[b].sigma[0] = h[b].sigma[1] = h[b].sigma[2] = 1.f;
+  }
+  if (cudaMemcpyAsync(dparams, h.data(), sizeof(SpecParams) * B, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    return CB_ERR_CUDA;
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
+int Solver::upload_mask(const std::vector<int>& sel, int* dmask) {
+  if (cudaMemcpyAsync(dmask, sel.data(), sizeof(int) * B, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    return CB_ERR_CUDA;
+  return 0;
+}
+
+int Solver::fetch_scalars() {
+  cudaMemcpyAsync(hsc, dsc, sizeof(double) * NSLOT * B, cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hint, dint, sizeof(int) * NISLOT * B, cudaMemcpyDeviceToHost, stream);
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    err = std::string("device error: ") + cudaGetErrorString(e);
+    return CB_ERR_CUDA;
+  }
+  return 0;
+}
+
+int Solver::dot(const float* a, long long ap, const float* b, long long bp, long long len, int s,
+                const int* act, double scale) {
+  const int np = dot_partials(len);
+  CB_TRY(launch_dot(a, ap, b, bp, len, B, partials, maxparts, act, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(s), B, scale, false, stream));
+  note_launches(2);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// forward problem (src/CLAIRE.cpp:1861-1984, 2116-2175)
+// ---------------------------------------------------------------------------
+int Solver::state_solve(const float* vel, const int* act) {
+  const long long PM = (nt + 1) * n;
+  CB_TRY(launch_trajectory(vel, 3 * n, disp_st, 3 * n, B, d, ht, 1.f, act, stream));
+  CB_TRY(launch_lincomb(m, PM, mT, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+  for (int j = 0; j < nt; ++j)
+    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, m + (j + 1) * n, PM, n, 1, B, d, act, stream));
+  note_launches(2 + nt);
+  return 0;
+}
+
+// D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)
+int Solver::distance(const int* act) {
+  const long long PM = (nt + 1) * n;
+  const int np = dot_partials(n);
+  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, act, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_D), B, 0.5 * (double)hd, false, stream));
+  note_launches(2);
+  return 0;
+}
+
+// Regularization::EvaluateFunctional.  Raw sums land in S_R (and S_RV for
+// H1's L2 part); the per-norm factors are applied on the host.
+int Solver::reg_functional(const float* vel, const std::vector<int>& sel, const int* act) {
+  std::vector<int> ma(B, 0), mb(B, 0);
+  bool any_a = false, any_b = false;
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    if (ps[b].norm == NORM_H1 || ps[b].norm == NORM_H1SN) { ma[b] = 1; any_a = true; }
+    else { mb[b] = 1; any_b = true; }
+  }
+  int* dma = dact + 4 * B;
+  int* dmb = dact + 5 * B;
+  if (any_a) {
+    // sum_i sum_k ||d/dx_k v_i||^2 with spectral derivatives (src/RegularizationH1SN.cpp:84-141)
+    CB_TRY(upload_mask(ma, dma));
+    for (int a = 0; a < 3; ++a) {
+      const int np = deriv_partials(d, a, 3);
+      CB_TRY(launch_deriv(vel, 3 * n, n, nullptr, 0, 0, 3, B, d, a, EPI_SUMSQ, partials, maxparts, dma, stream));
+      CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, a > 0, stream));
+    }
+    note_launches(6);
+    CB_TRY(dot(vel, 3 * n, vel, 3 * n, 3 * n, S_RV, dma));
+  }
+  if (any_b) {
+    CB_TRY(upload_mask(mb, dmb));
+    CB_TRY(launch_r2c3d(vel, 3 * n, n, spec, 3 * nc, 3, B, d, dmb, stream));
+    CB_TRY(launch_pencil(spec, 3 * nc, B, d, OP_REG_FUNC, dparams, 3, 3, dmb, stream));
+    const int np = c2r_partials(d, 3);
+    CB_TRY(launch_c2r3d(spec, 3 * nc, nullptr, 0, 0, 3, B, d, EPI_SUMSQ, nullptr, partials, maxparts, dmb, stream));
+    // finalize only the selected problems' slots: unselected keep stale values
+    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, false, stream));
+    note_launches(6);
+    (void)any_a;
+  }
+  (void)act;
+  return 0;
+}
+
+static double reg_factor(const ProbState& s, double hd, double sumsq, double vv) {
+  switch (s.norm) {
+    case NORM_H1SN: return 0.5 * hd * s.beta0 * sumsq;
+    case NORM_H1: return 0.5 * hd * s.beta0 * (sumsq + s.beta1 * vv);
+    case NORM_L2: return 0.5 * hd * sumsq;               // symbol sqrt(beta)
+    case NORM_H2: return 0.5 * hd * sumsq;
+    case NORM_H2SN: return 0.5 * hd * s.beta0 * sumsq;
+    case NORM_H3: return 0.5 * hd * sumsq;
+    case NORM_H3SN: return 0.5 * hd * s.beta0 * sumsq;
+    default: return 0.0;
+  }
+}
+
+int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(state_solve(vel, dact));
+  CB_TRY(distance(dact));
+  // mixed-class batches run reg_functional's two passes with their own masks;
+  // the finalize of the second pass must not clobber the first, so run classes
+  // one after another and read back in between.
+  std::vector<int> sa(B, 0), sb(B, 0);
+  bool any_a = false, any_b = false;
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    if (ps[b].norm == NORM_H1 || ps[b].norm == NORM_H1SN) { sa[b] = 1; any_a = true; }
+    else { sb[b] = 1; any_b = true; }
+  }
+  std::vector<double> R(B, 0.0);
+  if (any_a) {
+    CB_TRY(reg_functional(vel, sa, dact));
+    CB_TRY(fetch_scalars());
+    for (int b = 0; b < B; ++b)
+      if (sa[b]) R[b] = reg_factor(ps[b], hd, hsc[S_R * B + b], hsc[S_RV * B + b]);
+  }
+  if (any_b) {
+    CB_TRY(reg_functional(vel, sb, dact));
+  }
+  CB_TRY(fetch_scalars());
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    if (sb[b]) R[b] = reg_factor(ps[b], hd, hsc[S_R * B + b], 0.0);
+    ps[b].D = hsc[S_D * B + b];
+    ps[b].R = R[b];
+    ps[b].J = ps[b].D + ps[b].R;
+    ps[b].obj_evals++;
+    ps[b].pde_solves++;
+    state_of[b] = (vel == v) ? 1 : 2;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// spectral building blocks
+// ---------------------------------------------------------------------------
+int Solver::reg_op(const float* vin, float* out, int op, int epi, const int* act) {
+  CB_TRY(launch_r2c3d(vin, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
+  CB_TRY(launch_pencil(spec, 3 * nc, B, d, op, dparams, 3, 3, act, stream));
+  CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, epi, nullptr, nullptr, 0, act, stream));
+  note_launches(5);
+  return 0;
+}
+
+// out[level j][axis a] = d/dx_a f[level j]
+int Solver::grad_fields(const float* f, long long fp, long long ifs, float* out, long long op,
+                        long long ofs, int nf, const int* act) {
+  for (int a = 0; a < 3; ++a)
+    CB_TRY(launch_deriv(f, fp, ifs, out + a * n, op, ofs, nf, B, d, a, EPI_STORE, nullptr, 0, act, stream));
+  note_launches(3);
+  return 0;
+}
+
+int Solver::divergence(const float* vel, float* out, const int* act) {
+  for (int a = 0; a < 3; ++a)
+    CB_TRY(launch_deriv(vel + a * n, 3 * n, n, out, n, n, 1, B, d, a, a == 0 ? EPI_STORE : EPI_ADD, nullptr, 0,
+                        act, stream));
+  note_launches(3);
+  return 0;
+}
+
+// Backward RK2 sweep with trapezoid body force (src/CLAIRE.cpp:2646-2709,
+// 3940-3999), projection (src/CLAIRE.cpp:2338) and the hd scaling (:2341).
+// On entry `lam` holds lambda(t=1); on exit lambda(t=0) is in `lam`.
+int Solver::adjoint_sweep(float* bout, const int* act) {
+  const long long PGM = (nt + 1) * 3 * n;
+  cudaMemsetAsync(bout, 0, sizeof(float) * 3 * n * B, stream);
+  float* cur = lam;
+  float* nxt = lam2;
+  for (int j = 0; j < nt; ++j) {
+    const float w = (j == 0) ? 0.5f * ht : ht;
+    CB_TRY(launch_adjoint_step(cur, nxt, n, disp_adj, 3 * n, divv, divvx, n, gm + (nt - j) * 3 * n, PGM, bout,
+                               3 * n, ht, w, B, d, act, stream));
+    std::swap(cur, nxt);
+  }
+  const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
+  CB_TRY(launch_body_force_final(bout, 3 * n, gm, PGM, cur, n, 0.5f * ht, proj ? 1.f : hd, B, n, act, stream));
+  note_launches(nt + 1);
+  if (proj) {
+    CB_TRY(launch_r2c3d(bout, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
+    CB_TRY(launch_pencil(spec, 3 * nc, B, d, opts.model == CB_MODEL_STOKES ? OP_LERAY : OP_LERAY_RELAXED, dparams,
+                         3, 3, act, stream));
+    CB_TRY(launch_c2r3d(spec, 3 * nc, bout, 3 * n, n, 3, B, d, EPI_ADD, nullptr, nullptr, 0, act, stream));
+    CB_TRY(launch_lincomb(bout, 3 * n, bout, 3 * n, nullptr, (double)hd, nullptr, 0, nullptr, 0.0, 3 * n, B, act,
+                          stream));
+    note_launches(6);
+  }
+  if (cur != lam) {
+    CB_TRY(launch_lincomb(lam, n, cur, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+    note_launches(1);
+  }
+  return 0;
+}
+
+// EvaluateGradient at v (src/CLAIRE.cpp:871-1042); the state must be valid for v.
+int Solver::gradient(const int* act) {
+  const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n;
+  CB_TRY(launch_trajectory(v, 3 * n, disp_adj, 3 * n, B, d, ht, -1.f, act, stream));
+  CB_TRY(grad_fields(m, PM, n, gm, PGM, 3 * n, nt + 1, act));
+  CB_TRY(divergence(v, divv, act));
+  CB_TRY(launch_interp(divv, n, n, disp_adj, 3 * n, divvx, n, n, 1, B, d, act, stream));
+  // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222)
+  CB_TRY(launch_lincomb(lam, n, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
+  note_launches(3);
+  CB_TRY(adjoint_sweep(bf, act));
+  CB_TRY(reg_op(v, g, OP_REG_GRAD, EPI_STORE, act));
+  CB_TRY(launch_lincomb(g, 3 * n, g, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
+  note_launches(1);
+  CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, act));
+  return 0;
+}
+
+// caches for the Hessian: (grad m^j)(X_state), j < nt
+int Solver::hessian_prep(const int* act) {
+  const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n;
+  CB_TRY(launch_interp(gm, PGM, n, disp_st, 3 * n, gx, PGX, n, 3 * nt, B, d, act, stream));
+  note_launches(1);
+  return 0;
+}
+
+// GN Hessian matvec (src/CLAIRE.cpp:1311-1379, 3147-3290, 3307-3490, 3849-4012)
+int Solver::hessian(const float* vin, float* hout, const int* act) {
+  const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n;
+  CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, vtx, 3 * n, n, 3, B, d, act, stream));
+  cudaMemsetAsync(mt, 0, sizeof(float) * n * B, stream);
+  float* cur = mt;
+  float* nxt = mt2;
+  for (int j = 0; j < nt; ++j) {
+    CB_TRY(launch_incstate_step(cur, nxt, n, disp_st, 3 * n, gx + j * 3 * n, PGX, vtx, gm + (j + 1) * 3 * n, PGM,
+                                vin, 3 * n, ht, B, d, act, stream));
+    std::swap(cur, nxt);
+  }
+  // lambda~(t=1) = -m~(t=1) (src/DistanceMeasureSL2.cpp:223-283)
+  CB_TRY(launch_lincomb(lam, n, cur, n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+  note_launches(2 + nt);
+  CB_TRY(adjoint_sweep(bf, act));
+  CB_TRY(reg_op(vin, hout, OP_REG_GRAD, EPI_STORE, act));
+  CB_TRY(launch_lincomb(hout, 3 * n, hout, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
+  note_launches(1);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// public single-shot operations
+// ---------------------------------------------------------------------------
+int Solver::gradient_at_current(const std::vector<int>& sel) {
+  std::vector<int> need(B, 0);
+  bool any = false;
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && state_of[b] != 1) { need[b] = 1; any = true; }
+  if (any) CB_TRY(objective_at(v, need));
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(gradient(dact));
+  CB_TRY(fetch_scalars());
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ps[b].gnorm = std::sqrt(hsc[S_GG * B + b]);
+      ps[b].grad_evals++;
+      ps[b].pde_solves++;
+    }
+  return 0;
+}
+
+int Solver::hessian_matvec(const float* vin, float* hout, const std::vector<int>& sel) {
+  CB_TRY(gradient_at_current(sel));  // state, adjoint trajectory and caches for v
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(hessian_prep(dact));
+  CB_TRY(hessian(vin, hout, dact));
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return CB_ERR_CUDA;
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) ps[b].hess_matvecs++;
+  return 0;
+}
+
+int Solver::precond(const float* rin, float* zout, const std::vector<int>& sel) {
+  CB_TRY(upload_mask(sel, dact));
+  if (opts.precond) CB_TRY(reg_op(rin, zout, OP_REG_INV, EPI_STORE, dact));
+  else CB_TRY(launch_lincomb(zout, 3 * n, rin, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact, stream));
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) ps[b].pc_matvecs++;
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
+int Solver::forward(const float* m0, float* m1, const std::vector<int>& sel) {
+  // m0 / m1 are device arrays laid out like mT (problem stride n)
+  CB_TRY(upload_mask(sel, dact));
+  const long long PM = (nt + 1) * n;
+  CB_TRY(launch_trajectory(v, 3 * n, disp_st, 3 * n, B, d, ht, 1.f, dact, stream));
+  CB_TRY(launch_lincomb(m, PM, m0, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
+  for (int j = 0; j < nt; ++j)
+    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, m + (j + 1) * n, PM, n, 1, B, d, dact, stream));
+  CB_TRY(launch_lincomb(m1, n, m + nt * n, PM, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
+  note_launches(3 + nt);
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) state_of[b] = 0;  // state now belongs to m0, not mT
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
+int Solver::final_state(float* m1, int b) {
+  if (state_of[b] != 1) {
+    std::vector<int> sel(B, 0);
+    sel[b] = 1;
+    CB_TRY(objective_at(v, sel));
+  }
+  const long long PM = (nt + 1) * n;
+  if (cudaMemcpyAsync(m1, m + b * PM + nt * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+    return CB_ERR_CUDA;
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// PCG (KSPCG, unpreconditioned residual norm, zero initial guess;
+// src/Optimizer.cpp:296-356)
+// ---------------------------------------------------------------------------
+int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
+  const int maxit = (int)maxit_d;
+  int* act = dact2;
+  CB_TRY(upload_mask(sel, act));
+  // r = -g, x = 0
+  CB_TRY(launch_lincomb(r, 3 * n, g, 3 * n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+  CB_TRY(launch_lincomb(x, 3 * n, g, 3 * n, nullptr, 0.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+  note_launches(2);
+  CB_TRY(dot(r, 3 * n, r, 3 * n, 3 * n, S_RR, act));
+  k_pcg_init<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, opts.krylovtol[1]);
+  note_launches(1);
+  auto apply_pc = [&]() -> int {
+    if (opts.precond) return reg_op(r, z, OP_REG_INV, EPI_STORE, act);
+    note_launches(1);
+    return launch_lincomb(z, 3 * n, r, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream);
+  };
+  CB_TRY(apply_pc());
+  CB_TRY(dot(r, 3 * n, z, 3 * n, 3 * n, S_RZ, act));
+  CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+  note_launches(1);
+  std::vector<int> hact(B);
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) ps[b].pc_matvecs++;
+  for (int it = 0; it <= maxit; ++it) {
+    cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+      err = "device error in PCG";
+      return CB_ERR_CUDA;
+    }
+    bool any = false;
+    for (int b = 0; b < B; ++b)
+      if (hact[b]) {
+        any = true;
+        ps[b].hess_matvecs++;
+      }
+    if (!any || maxit == 0) break;
+    CB_TRY(hessian(pv, q, act));
+    CB_TRY(dot(pv, 3 * n, q, 3 * n, 3 * n, S_PQ, act));
+    k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
+    CB_TRY(launch_lincomb(x, 3 * n, x, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_ALPHA), 1.0, 3 * n, B, act, stream));
+    CB_TRY(launch_lincomb(r, 3 * n, r, 3 * n, nullptr, 1.0, q, 3 * n, slot(S_ALPHA), -1.0, 3 * n, B, act, stream));
+    note_launches(3);
+    CB_TRY(dot(r, 3 * n, r, 3 * n, 3 * n, S_RR, act));
+    k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
+    note_launches(1);
+    CB_TRY(apply_pc());
+    for (int b = 0; b < B; ++b)
+      if (hact[b]) ps[b].pc_matvecs++;
+    CB_TRY(dot(r, 3 * n, z, 3 * n, 3 * n, S_RZNEW, act));
+    k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
+    CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
+    note_launches(2);
+  }
+  CB_TRY(fetch_scalars());
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) ps[b].pcg_total += hint[I_IT * B + b];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Armijo backtracking (PETSc TaoLineSearch "armijo": alpha0 = 1, beta = 1/2,
+// sigma = 1e-4) on the step x; accepted problems get v <- v + alpha x.
+// ---------------------------------------------------------------------------
+int Solver::line_search(std::vector<int>& sel) {
+  // descent test g.x < 0, else fall back to the steepest-descent direction
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(dot(g, 3 * n, x, 3 * n, 3 * n, S_GD, dact));
+  CB_TRY(fetch_scalars());
+  std::vector<double> gd(B, 0.0), alpha(B, 1.0);
+  std::vector<int> fallback(B, 0);
+  bool anyfb = false;
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    gd[b] = hsc[S_GD * B + b];
+    if (!(gd[b] < 0.0)) {
+      fallback[b] = 1;
+      anyfb = true;
+      gd[b] = -ps[b].gnorm * ps[b].gnorm;
+    }
+  }
+  if (anyfb) {
+    CB_TRY(upload_mask(fallback, dact + 3 * B));
+    CB_TRY(launch_lincomb(x, 3 * n, g, 3 * n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact + 3 * B, stream));
+    note_launches(1);
+  }
+  std::vector<int> trial = sel, accepted(B, 0);
+  const int max_trials = 30;
+  const double sigma = 1e-4;
+  for (int t = 0; t < max_trials; ++t) {
+    bool any = false;
+    for (int b = 0; b < B; ++b) any |= (trial[b] != 0);
+    if (!any) break;
+    // vtrial = v + alpha x  (alpha per problem through S_ALPHA)
+    std::vector<double> al(B, 0.0);
+    for (int b = 0; b < B; ++b) al[b] = alpha[b];
+    cudaMemcpyAsync(slot(S_ALPHA), al.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+    CB_TRY(upload_mask(trial, dact + 6 * B));
+    CB_TRY(launch_lincomb(vtrial, 3 * n, v, 3 * n, nullptr, 1.0, x, 3 * n, slot(S_ALPHA), 1.0, 3 * n, B,
+                          dact + 6 * B, stream));
+    note_launches(1);
+    const double* Jold = nullptr;
+    (void)Jold;
+    std::vector<double> J0(B);
+    for (int b = 0; b < B; ++b) J0[b] = ps[b].J;
+    std::vector<double> D0(B), R0(B);
+    for (int b = 0; b < B; ++b) { D0[b] = ps[b].D; R0[b] = ps[b].R; }
+    CB_TRY(objective_at(vtrial, trial));
+    for (int b = 0; b < B; ++b) {
+      if (!trial[b]) continue;
+      const double Jt = ps[b].J;
+      if (std::isfinite(Jt) && Jt <= J0[b] + sigma * alpha[b] * gd[b]) {
+        accepted[b] = 1;
+        trial[b] = 0;
+        ps[b].step = alpha[b];
+      } else {
+        // restore the monitor values of the current iterate
+        ps[b].J = J0[b];
+        ps[b].D = D0[b];
+        ps[b].R = R0[b];
+        alpha[b] *= 0.5;
+      }
+    }
+  }
+  for (int b = 0; b < B; ++b)
+    if (trial[b]) {  // line search failed
+      sel[b] = 0;
+      ps[b].done = true;
+      ps[b].reason = 5;
+    }
+  bool anyacc = false;
+  for (int b = 0; b < B; ++b) anyacc |= (accepted[b] != 0);
+  if (anyacc) {
+    CB_TRY(upload_mask(accepted, dact + 7 * B));
+    CB_TRY(launch_lincomb(v, 3 * n, vtrial, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact + 7 * B,
+                          stream));
+    note_launches(1);
+    for (int b = 0; b < B; ++b)
+      if (accepted[b]) state_of[b] = 1;  // the state was computed at vtrial == new v
+  }
+  for (int b = 0; b < B; ++b) sel[b] = accepted[b];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// GN loop with CLAIRE's stopping test (src/TaoInterface.cpp:391-527)
+// ---------------------------------------------------------------------------
+int Solver::run(const std::vector<int>& sel_in) {
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<int> sel = sel_in;
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ProbState keep = ps[b];
+      ps[b] = ProbState();
+      ps[b].norm = keep.norm;
+      ps[b].model = keep.model;
+      ps[b].beta0 = keep.beta0;
+      ps[b].beta1 = keep.beta1;
+      ps[b].beta2 = keep.beta2;
+      state_of[b] = 0;
+    }
+  // InitializeOptimization (src/CLAIRE.cpp:227-357): J0, D0, ||g0|| at the initial guess
+  CB_TRY(objective_at(v, sel));
+  CB_TRY(gradient_at_current(sel));
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ps[b].J0 = ps[b].J;
+      ps[b].D0 = ps[b].D;
+      ps[b].gnorm0 = ps[b].gnorm > 0.0 ? ps[b].gnorm : 1.0;
+    }
+  const double gttol = opts.opttol, gatol = opts.gatol, minstep = 1.0 / 1024.0;
+  while (true) {
+    std::vector<int> act(B, 0);
+    bool any = false;
+    for (int b = 0; b < B; ++b) {
+      if (!sel[b] || ps[b].done) continue;
+      ProbState& s = ps[b];
+      if (!std::isfinite(s.J) || !std::isfinite(s.gnorm)) { s.done = true; s.reason = -1; continue; }
+      if (s.step < minstep) { s.done = true; s.reason = 4; continue; }
+      if (s.gnorm < gttol * s.gnorm0) { s.done = true; s.reason = 1; continue; }
+      if (s.gnorm < gatol) { s.done = true; s.reason = 2; continue; }
+      if (s.iter > opts.maxit - 1) { s.done = true; s.reason = 3; continue; }
+      act[b] = 1;
+      any = true;
+    }
+    if (!any) break;
+    // forcing sequence (src/KrylovInterface.cpp:134-165)
+    std::vector<double> rtol(B, opts.krylovtol[0]);
+    for (int b = 0; b < B; ++b) {
+      if (!act[b]) continue;
+      ProbState& s = ps[b];
+      if (opts.krylovfseq != CB_FSEQ_NONE) {
+        if (s.krylov_g0 < 0) s.krylov_g0 = s.gnorm;
+        const double gr = s.gnorm / s.krylov_g0;
+        double rt = (opts.krylovfseq == CB_FSEQ_QUADRATIC) ? gr : std::sqrt(gr);
+        rt = std::max(1e-16, std::min(0.5, rt));
+        rtol[b] = rt;
+      }
+    }
+    cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+    CB_TRY(upload_mask(act, dact));
+    CB_TRY(hessian_prep(dact));
+    CB_TRY(pcg(act, std::max(0, opts.krylovmaxit - 1)));
+    std::vector<int> acc = act;
+    CB_TRY(line_search(acc));
+    bool anyacc = false;
+    for (int b = 0; b < B; ++b) anyacc |= (acc[b] != 0);
+    if (anyacc) CB_TRY(gradient_at_current(acc));
+    for (int b = 0; b < B; ++b)
+      if (acc[b]) ps[b].iter++;
+    if (opts.verbosity > 0) {
+      // OptimizationMonitor line (src/TaoInterface.cpp:529-606)
+      for (int b = 0; b < B; ++b)
+        if (act[b])
+          std::fprintf(stderr, "[claire_b200] p%d it %d J/J0 %.6e D/D0 %.6e |g|/|g0| %.6e pcg %d reason %d step %.3e\n",
+                       b, ps[b].iter, ps[b].J / ps[b].J0, ps[b].D / ps[b].D0, ps[b].gnorm / ps[b].gnorm0,
+                       hint[I_IT * B + b], hint[I_REASON * B + b], ps[b].step);
+    }
+  }
+  // final relative mismatch ||mR - m1|| / ||mR - mT|| (src/CLAIRE.cpp:4232-4262)
+  std::vector<int> need(B, 0);
+  bool anyneed = false;
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && state_of[b] != 1) { need[b] = 1; anyneed = true; }
+  if (anyneed) CB_TRY(objective_at(v, need));
+  const long long PM = (nt + 1) * n;
+  const int np = dot_partials(n);
+  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, nullptr, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_PQ), B, 1.0, false, stream));
+  CB_TRY(launch_diff_sumsq(mR, n, mT, n, n, B, partials, maxparts, nullptr, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream));
+  note_launches(4);
+  CB_TRY(fetch_scalars());
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    const double num = std::sqrt(hsc[S_PQ * B + b]), den = std::sqrt(hsc[S_RR * B + b]);
+    ps[b].rel_mismatch = den > 0 ? num / den : num;
+    ps[b].seconds = secs;
+  }
+  return 0;
+}
+
+}  // namespace cb

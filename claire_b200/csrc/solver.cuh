@@ -1,0 +1,115 @@
+// Host-side Gauss-Newton-Krylov driver over the B200 kernels.
+//
+// One Solver owns B independent registration problems of one grid size and
+// time-step count (B = 1 is the plain single-problem path).  All problems'
+// fields live in one allocation per array (problem p at base + p*stride), so
+// every kernel launch covers the whole batch and a per-problem `active` mask
+// on the device switches problems off once they converge.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/claire_b200.h"
+#include "common.cuh"
+#include "spectral.cuh"
+
+namespace cb {
+
+void note_launches(int k);
+long long launches();
+
+struct ProbState {
+  int norm = NORM_H1SN;
+  int model = CB_MODEL_COMPRESSIBLE;
+  double beta0 = 1e-2, beta1 = 1e-4, beta2 = 1e-4;
+  // GN monitor values (src/RegOpt.hpp m_Monitor)
+  double J = 0, J0 = 0, D = 0, D0 = 0, R = 0, gnorm = 0, gnorm0 = 0, krylov_g0 = -1;
+  double step = 1.0;
+  int iter = 0, pcg_total = 0, reason = 0;
+  bool done = false;
+  int obj_evals = 0, grad_evals = 0, hess_matvecs = 0, pc_matvecs = 0, pde_solves = 0;
+  double seconds = 0.0, rel_mismatch = -1.0;
+};
+
+class Solver {
+ public:
+  Solver() = default;
+  ~Solver();
+  int init(const claire_b200_opts& o, int B);
+  static long long estimate_bytes(const claire_b200_opts& o, int B);
+
+  // ---- public operations (problems selected by the host mask `sel`) -------
+  int run(const std::vector<int>& sel);
+  int objective_at(const float* vel, const std::vector<int>& sel);  // fills ps[p].J/D/R
+  int gradient_at_current(const std::vector<int>& sel);              // g, ||g|| for v
+  int hessian_matvec(const float* vin, float* hout, const std::vector<int>& sel);
+  int precond(const float* rin, float* zout, const std::vector<int>& sel);
+  int forward(const float* m0, float* m1, const std::vector<int>& sel);
+  int final_state(float* m1, int b);
+  int set_problem(int b, const claire_b200_opts& o);
+  long long footprint() const { return bytes_; }
+
+  // grid and sizes
+  Dims d{};
+  int nt = 4, B = 0;
+  long long n = 0, nc = 0;
+  float ht = 0.25f, hd = 0.f;
+  claire_b200_opts opts{};
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  std::vector<ProbState> ps;
+  std::string err;
+
+  // device state (see DESIGN.md for the layout)
+  float *mR = nullptr, *mT = nullptr, *v = nullptr, *vtrial = nullptr, *m = nullptr;
+  float *disp_st = nullptr, *disp_adj = nullptr, *gm = nullptr, *gx = nullptr;
+  float *divv = nullptr, *divvx = nullptr, *lam = nullptr, *lam2 = nullptr, *bf = nullptr;
+  float *g = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *q = nullptr;
+  float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *work3 = nullptr;
+  float2* spec = nullptr;
+  double* partials = nullptr;
+  int maxparts = 0;
+  double* dsc = nullptr;   // device scalars [NSLOT][B]
+  int* dact = nullptr;     // device mask [B]
+  int* dact2 = nullptr;    // device mask [B] (PCG)
+  int* dint = nullptr;     // device ints [NISLOT][B]
+  SpecParams* dparams = nullptr;
+  double* hsc = nullptr;   // pinned host mirror of dsc
+  int* hint = nullptr;     // pinned host mirror of dint
+
+  enum Slot { S_D = 0, S_R, S_RV, S_GG, S_PQ, S_RR, S_RZ, S_RZNEW, S_ALPHA, S_BETA, S_TOL,
+              S_RN0, S_GD, S_RTOL, NSLOT };
+  enum ISlot { I_IT = 0, I_REASON, NISLOT };
+
+  // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
+  std::vector<int> state_of;
+
+ private:
+  long long bytes_ = 0;
+  int alloc(void** p, size_t bytes);
+  int upload_mask(const std::vector<int>& sel, int* dmask);
+  int upload_params();
+  double* slot(int s) { return dsc + (long long)s * B; }
+  int* islot(int s) { return dint + (long long)s * B; }
+  int fetch_scalars();
+
+  // building blocks (act: device mask)
+  int state_solve(const float* vel, const int* act);
+  int distance(const int* act);
+  int reg_functional(const float* vel, const std::vector<int>& sel, const int* act);
+  int reg_op(const float* vin, float* out, int op, int epi, const int* act);
+  int grad_fields(const float* f, long long fp, long long ifs, float* out, long long op,
+                  long long ofs, int nf, const int* act);
+  int divergence(const float* vel, float* out, const int* act);
+  int adjoint_sweep(float* bout, const int* act);
+  int gradient(const int* act);
+  int hessian_prep(const int* act);
+  int hessian(const float* vin, float* hout, const int* act);
+  int pcg(const std::vector<int>& sel, double maxit);
+  int line_search(std::vector<int>& sel);
+  int dot(const float* a, long long ap, const float* b, long long bp, long long len, int slot,
+          const int* act, double scale = 1.0);
+};
+
+}  // namespace cb

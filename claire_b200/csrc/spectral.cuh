@@ -1,0 +1,67 @@
+// Spectral operator parameters and the host-side launch interface of the FFT
+// kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace cb {
+
+// Regularisation norms, numbered like CLAIRE's -regnorm choices.
+enum RegNorm : int { NORM_L2 = 0, NORM_H1 = 1, NORM_H1SN = 2, NORM_H2 = 3, NORM_H2SN = 4,
+                     NORM_H3 = 5, NORM_H3SN = 6 };
+
+// Operators applied in the x1 pencil pass between the forward and the
+// inverse transform.
+enum SpecOp : int {
+  OP_REG_GRAD = 0,   // EvaluateGradient / HessianMatVec symbol, 3 -> 3
+  OP_REG_INV = 1,    // ApplyInverse symbol, 3 -> 3
+  OP_REG_SQRTINV = 2,// ApplyInverse with applysqrt, 3 -> 3
+  OP_REG_FUNC = 3,   // symbol whose squared output norm is the functional, 3 -> 3
+  OP_LERAY = 4,      // Stokes projection addend, 3 -> 3
+  OP_LERAY_RELAXED = 5, // relaxed-Stokes projection addend, 3 -> 3
+  OP_GAUSS = 6,      // Gaussian smoothing, 1 -> 1
+  OP_IDENTITY = 7,   // scale by 1/N^3 only (round-trip test), 1 -> 1
+};
+
+// Per-problem parameters read by the pencil kernel.
+struct SpecParams {
+  int norm;
+  float beta0, beta1, beta2;  // regularisation weights (beta2: relaxed Stokes)
+  float hd;                   // Lebesgue measure
+  float sigma[3];             // Gaussian width in grid cells
+};
+
+// Epilogue of the inverse row pass.
+enum Epi : int { EPI_STORE = 0, EPI_ADD = 1, EPI_SUMSQ = 2 };
+
+struct Batch {
+  int nprob;              // problems in the launch
+  long long pstride;      // elements between problems' fields
+};
+
+// ---- host launchers (return cudaError_t as int) ---------------------------
+// All take an optional per-problem `active` mask (null: all problems).
+// Forward r2c of nf real fields: in[p*ip + f*ifs] -> spec[p*sp + f*nc].
+int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, long long sp, int nf,
+                 int nprob, const Dims& d, const int* active, cudaStream_t s);
+// Apply op in the x1 pass (in place on spec, nin fields in, nout out).
+int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
+                  const SpecParams* dparams, int nin, int nout, const int* active, cudaStream_t s);
+// Inverse c2r of nf fields with epilogue: out[p*op + f*ofs] = alpha[p]*x (+ out) or sumsq.
+int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long long ofs, int nf,
+                 int nprob, const Dims& d, int epi, const float* alpha, double* partials, int nparts,
+                 const int* active, cudaStream_t s);
+
+// Spectral first derivative along one axis (0:x1, 1:x2, 2:x3) of nf real
+// fields with Nyquist set to zero; out = d/dx_axis in (+ out) or sumsq.
+int launch_deriv(const float* in, long long ip, long long ifs, float* out, long long op_,
+                 long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
+                 double* partials, int nparts, const int* active, cudaStream_t s);
+
+// Number of reduction partials a launch with these arguments writes per problem.
+int deriv_partials(const Dims& d, int axis, int nf);
+int c2r_partials(const Dims& d, int nf);
+
+bool fft_size_supported(int n);
+
+}  // namespace cb

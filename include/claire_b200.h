@@ -1,0 +1,156 @@
+/*
+ * claire_b200.h -- C ABI of the B200-native CLAIRE Gauss-Newton-Krylov path.
+ *
+ * Plain pointers, sizes and int status codes; no C++ or torch types.  Every
+ * entry point returns CB_OK (0) or a negative CB_ERR_* code.  Device pointers
+ * are float32 arrays on the current CUDA device; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).
+ *
+ * Grids are periodic on [0, 2*pi)^3, row-major with x3 fastest
+ * (include/CLAIREUtils.hpp:198-212 of the reference).  Vector fields are three
+ * consecutive scalar fields [x1 | x2 | x3] (src/VecField.cpp:396-478).
+ * Displacements ("disp") are characteristic foot points X minus the grid
+ * node, in grid units: X = (i + disp) * 2*pi / N.
+ */
+#ifndef CLAIRE_B200_H_
+#define CLAIRE_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CB_OK 0
+#define CB_ERR_ARG (-1)       /* invalid argument */
+#define CB_ERR_ALLOC (-2)     /* device or host allocation failed */
+#define CB_ERR_CUDA (-3)      /* a CUDA call or kernel launch failed */
+#define CB_ERR_NUMERIC (-4)   /* NaN / Inf in objective or gradient */
+#define CB_ERR_STATE (-5)     /* call out of order (e.g. run before images) */
+#define CB_ERR_UNSUPPORTED (-6) /* grid size without an FFT plan */
+
+/* Regularisation norms (-regnorm): l2 h1 h1s h2 h2s h3 h3s. */
+enum {
+  CB_NORM_L2 = 0, CB_NORM_H1 = 1, CB_NORM_H1SN = 2, CB_NORM_H2 = 3,
+  CB_NORM_H2SN = 4, CB_NORM_H3 = 5, CB_NORM_H3SN = 6
+};
+/* Registration models: CLAIRE (no projection), Stokes, relaxed Stokes. */
+enum { CB_MODEL_COMPRESSIBLE = 0, CB_MODEL_STOKES = 1, CB_MODEL_RELAXEDSTOKES = 2 };
+/* Krylov forcing sequences (-krylovfseq). */
+enum { CB_FSEQ_NONE = 0, CB_FSEQ_QUADRATIC = 1, CB_FSEQ_SUPERLINEAR = 2 };
+/* Regularisation operator kinds for claire_b200_reg_apply. */
+enum { CB_REG_GRADIENT = 0, CB_REG_INVERSE = 1, CB_REG_SQRTINVERSE = 2 };
+
+/*
+ * Hot-path subset of reg::RegOpt (include/RegOpt.hpp:475-635); defaults from
+ * RegOpt::Initialize (src/RegOpt.cpp:1032-1293).
+ */
+typedef struct claire_b200_opts {
+  int nx[3];            /* -nx */
+  int nt;               /* -nt (4) */
+  int regnorm;          /* -regnorm (CB_NORM_H1SN) */
+  int model;            /* registration model (CB_MODEL_COMPRESSIBLE when -regnorm given) */
+  double beta[3];       /* -beta sets beta[0] (1e-2); beta[1] = 1e-4; beta[2] = 1e-4 */
+  int maxit;            /* -maxit (50) */
+  double opttol;        /* -opttol: ||g|| < opttol*||g0|| (5e-2) */
+  double gatol;         /* ||g|| < gatol (1e-6) */
+  int krylovmaxit;      /* -krylovmaxit (50); PCG runs krylovmaxit-1 iterations */
+  double krylovtol[3];  /* rtol 1e-12, atol 1e-16, dtol 1e6 */
+  int krylovfseq;       /* -krylovfseq (CB_FSEQ_SUPERLINEAR) */
+  int precond;          /* 1: inverse regularisation (INVREG), 0: none */
+  int iporder;          /* -iporder: 3 (tricubic) is the only order on this path */
+  int verbosity;        /* -verbosity */
+  int bf16_images;      /* store transported images in bf16 (gathers accumulate in fp32) */
+} claire_b200_opts;
+
+typedef struct claire_b200_stats {
+  int gn_iterations;        /* outer iterations */
+  int pcg_iterations;       /* total inner iterations */
+  int obj_evals, grad_evals, hess_matvecs, pc_matvecs, pde_solves;
+  int converged_reason;     /* 1 gttol, 2 gatol, 3 maxit, 4 steptol, 5 lsfail, -1 nan */
+  double J, J0, D, D0, R;   /* objective, distance, regularisation (FP64) */
+  double gnorm, gnorm0;     /* ||g|| and ||g0|| (FP64) */
+  double rel_mismatch;      /* ||mR - m1|| / ||mR - mT|| */
+  double seconds;           /* wall time of claire_b200_run */
+} claire_b200_stats;
+
+typedef struct claire_b200_ctx claire_b200_ctx;
+
+/* ---- options (reg::RegOpt) ------------------------------------------------ */
+/* Fill with RegOpt::Initialize defaults (src/RegOpt.cpp:1032-1293). */
+int claire_b200_default_opts(claire_b200_opts* opts);
+/* Parse the hot-path flags of RegOpt::ParseArguments (src/RegOpt.cpp:260-834):
+ * -nx -nt -regnorm -beta -maxit -opttol -gabs -krylovmaxit -krylovtol
+ * -krylovfseq -precond -iporder -verbosity. */
+int claire_b200_parse_args(claire_b200_opts* opts, int argc, const char* const* argv);
+
+/* ---- registration context (reg::CLAIREInterface) -------------------------- */
+/* Create a context holding `nbatch` independent problems of one grid size;
+ * allocates all device state up front (include/CLAIREInterface.hpp:42-90). */
+int claire_b200_create(const claire_b200_opts* opts, int nbatch, claire_b200_ctx** ctx);
+int claire_b200_destroy(claire_b200_ctx* ctx);
+const char* claire_b200_last_error(const claire_b200_ctx* ctx);
+/* Bytes of device memory the context holds (admission accounting). */
+long long claire_b200_footprint_bytes(const claire_b200_ctx* ctx);
+long long claire_b200_estimate_bytes(const claire_b200_opts* opts, int nbatch);
+/* Per-problem options inside a batch (norm, beta, ...); nx and nt must match. */
+int claire_b200_set_problem_opts(claire_b200_ctx* ctx, int b, const claire_b200_opts* opts);
+/* SetReferenceImage / SetTemplateImage (src/CLAIREInterface.cpp:594-660). */
+int claire_b200_set_images(claire_b200_ctx* ctx, int b, const float* mR, const float* mT, int on_device);
+/* SetInitialGuess (src/CLAIREInterface.cpp: copy semantics). */
+int claire_b200_set_velocity(claire_b200_ctx* ctx, int b, const float* v, int on_device);
+int claire_b200_get_velocity(const claire_b200_ctx* ctx, int b, float* v, int on_device);
+/* Run: GN-Krylov solve of every problem in the context (RunSolver). */
+int claire_b200_run(claire_b200_ctx* ctx);
+/* Solve only the problems whose mask entry is nonzero. */
+int claire_b200_run_masked(claire_b200_ctx* ctx, const int* mask);
+/* GetFinalState: m(t=1) for the current velocity. */
+int claire_b200_get_final_state(claire_b200_ctx* ctx, int b, float* m1, int on_device);
+/* SolveForwardProblem(m1, m0) with the current velocity (src/CLAIREInterface.cpp:1890). */
+int claire_b200_forward(claire_b200_ctx* ctx, int b, const float* m0, float* m1, int on_device);
+int claire_b200_get_stats(const claire_b200_ctx* ctx, int b, claire_b200_stats* stats);
+/* Objective J(v), gradient g(v) and GN Hessian matvec H*vt at velocity v for
+ * problem b (OptimizationProblem::{EvaluateObjective, EvaluateGradient,
+ * HessianMatVec}, include/OptimizationProblem.hpp:51-121).  Host pointers. */
+int claire_b200_objective(claire_b200_ctx* ctx, int b, const float* v, double* J, double* D, double* R);
+int claire_b200_gradient(claire_b200_ctx* ctx, int b, const float* v, float* g);
+int claire_b200_hessian_matvec(claire_b200_ctx* ctx, int b, const float* v, const float* vt, float* hvt);
+/* Preconditioner::MatVec (INVREG): P x = (beta A)^-1 x (src/Preconditioner.cpp:549-580). */
+int claire_b200_precond(claire_b200_ctx* ctx, int b, const float* x, float* px);
+/* Adjoint state lambda(t=0) and body force b from the last gradient evaluation. */
+int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);
+int claire_b200_synchronize(claire_b200_ctx* ctx);
+/* Run the context's work on the caller's stream from now on (NULL: the
+ * context's own stream).  The caller keeps ownership of the stream. */
+int claire_b200_set_stream(claire_b200_ctx* ctx, void* stream);
+
+/* ---- operator seams on device buffers (one problem, explicit stream) ------ */
+/* SemiLagrangian::ComputeTrajectory (src/SemiLagrangian.cpp:192-289):
+ * flag 0 = "state" (+1), 1 = "adjoint" (-1).  v: 3n, disp: 3n. */
+int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt, int flag, void* stream);
+/* SemiLagrangian::Interpolate (src/SemiLagrangian.cpp:536-727): out[k] =
+ * f[k](i + disp) for k < dof (dof 1 or 3), tricubic (src/interp3.cpp:2492-2719). */
+int claire_b200_interp3(const float* f, const float* disp, float* out, const int nx[3], int dof, void* stream);
+/* accfft_grad_t: g (3n) = spectral gradient of f (n), Nyquist zeroed. */
+int claire_b200_fft_grad(const float* f, float* g, const int nx[3], void* stream);
+/* accfft_divergence_t: d (n) = spectral divergence of v (3n). */
+int claire_b200_fft_div(const float* v, float* d, const int nx[3], void* stream);
+/* Regularization::{EvaluateGradient, ApplyInverse} (src/Regularization*.cpp):
+ * out (3n) = op(v (3n)); kind = CB_REG_GRADIENT / CB_REG_INVERSE / CB_REG_SQRTINVERSE. */
+int claire_b200_reg_apply(const float* v, float* out, const int nx[3], int regnorm, const double beta[2],
+                          int kind, void* stream);
+/* Regularization::EvaluateFunctional: R(v) in FP64 (host result). */
+int claire_b200_reg_functional(const float* v, double* R, const int nx[3], int regnorm,
+                               const double beta[2], void* stream);
+/* CLAIREStokes / CLAIREDivReg ::ApplyProjection: b (3n) += Leray addend. */
+int claire_b200_leray(float* b, const int nx[3], int model, const double beta[3], void* stream);
+/* Preprocessing::GaussianSmoothing (src/Preprocessing.cpp:1956-2056): sigma in cells. */
+int claire_b200_smooth(const float* f, float* out, const int nx[3], const double sigma[3], void* stream);
+/* DistanceMeasureSL2::EvaluateFunctional: D = 1/2 hd sum (mR - m1)^2 (FP64 host result). */
+int claire_b200_distance(const float* mR, const float* m1, const int nx[3], double* D, void* stream);
+/* Number of CUDA kernel launches issued by this library since load (all threads). */
+long long claire_b200_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLAIRE_B200_H_ */

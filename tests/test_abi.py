@@ -1,0 +1,78 @@
+"""C ABI: the library loads and exports every symbol include/*.h declares, and
+the host-only entry points (options, argv parsing) behave like RegOpt.
+No compute calls: runs without a GPU."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(inc, fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(claire_b200_[a-z0-9_]+)\s*\(", src):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "claire_b200_run" in names and "claire_b200_interp3" in names
+    assert len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol():
+    import claire_b200
+    lib = ctypes.CDLL(claire_b200.LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_opts_match_regopt_initialize():
+    import claire_b200 as cb
+    o = cb.RegOpt().opts
+    # src/RegOpt.cpp:1032-1293
+    assert o.nt == 4 and tuple(o.nx) == (32, 32, 32)
+    assert o.regnorm == cb.NORMS["h1s"] and o.model == cb.MODELS["relaxedstokes"]
+    assert o.beta[0] == 1e-2 and o.beta[1] == 1e-4 and o.beta[2] == 1e-4
+    assert o.maxit == 50 and o.opttol == 5e-2 and o.gatol == 1e-6
+    assert o.krylovmaxit == 50 and o.krylovtol[0] == 1e-12 and o.krylovtol[1] == 1e-16
+    assert o.krylovtol[2] == 1e6 and o.precond == 1 and o.iporder == 3
+
+
+def test_parse_args():
+    import claire_b200 as cb
+    opt = cb.RegOpt(["-nx", "64x64x64", "-nt", "8", "-regnorm", "h2", "-beta", "1e-3", "-maxit", "10",
+                     "-opttol", "1e-2", "-krylovfseq", "quadratic", "-precond", "invreg"])
+    o = opt.opts
+    assert tuple(o.nx) == (64, 64, 64) and o.nt == 8
+    assert o.regnorm == cb.NORMS["h2"] and o.model == cb.MODELS["compressible"]
+    assert o.beta[0] == 1e-3 and o.maxit == 10 and o.opttol == 1e-2 and o.krylovfseq == 1
+    opt2 = cb.RegOpt(["-nx", "96", "-regnorm", "h1s-stokes"])
+    assert tuple(opt2.opts.nx) == (96, 96, 96) and opt2.opts.model == cb.MODELS["stokes"]
+
+
+def test_parse_args_rejects_bad_input():
+    import claire_b200 as cb
+    with pytest.raises(cb.ClaireError):
+        cb.RegOpt(["-regnorm", "h7"])
+    with pytest.raises(cb.ClaireError):
+        cb.RegOpt(["-iporder", "1"])
+    with pytest.raises(cb.ClaireError):
+        cb.RegOpt(["-nx"])
+
+
+def test_memory_estimate_scales():
+    import claire_b200 as cb
+    a = cb.RegOpt(["-nx", "64", "-nt", "4"]).estimate_bytes(1)
+    b = cb.RegOpt(["-nx", "128", "-nt", "4"]).estimate_bytes(1)
+    assert 7.5 < b / a < 8.5
+    assert cb.RegOpt(["-nx", "64"]).estimate_bytes(4) == 4 * a

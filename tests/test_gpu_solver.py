@@ -1,0 +1,147 @@
+"""Parity of the GN building blocks and of full registrations against the oracle.
+
+Tolerances: objective / distance / gradient / Hessian matvec within 1e-5
+relative (FP32 device arithmetic against the FP64 oracle on the same inputs);
+final velocity and mismatch within 1e-4 relative; GN / PCG iteration counts
+within +-1 of the oracle's restated loop.
+"""
+import numpy as np
+import pytest
+
+from oracle import claire_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    nb = np.linalg.norm(b.ravel())
+    return np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def cb(cuda):
+    import claire_b200
+    return claire_b200
+
+
+def make_opt(cb, n, nt, norm, beta, **kw):
+    opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", norm, "-beta", str(beta)])
+    for k, v in kw.items():
+        opt.set(k, v)
+    return opt
+
+
+def c1_problem(n, nt=4):
+    mR, mT, vstar = R.synthetic_c1(n, np.float64, nt)
+    return mR.astype(np.float32), mT.astype(np.float32), vstar.astype(np.float32)
+
+
+@pytest.mark.parametrize("norm,beta,nt", [("h1s", 1e-2, 4), ("h2", 1e-3, 8), ("h1", 1e-2, 4)])
+def test_objective_gradient_hessian(cb, norm, beta, nt):
+    n = 32
+    mR, mT, vstar = c1_problem(n, nt)
+    rng = np.random.default_rng(0)
+    v = (0.3 * vstar + 0.02 * rng.standard_normal(vstar.shape)).astype(np.float32)
+    vt = (0.1 * rng.standard_normal(vstar.shape)).astype(np.float32)
+    prob = R.Problem(mR, mT, nt, R.Regularization(norm, beta))
+    J = prob.objective(v.astype(np.float64))
+    g = prob.gradient(v.astype(np.float64))
+    H = prob.hessian_matvec(vt.astype(np.float64))
+    P = prob.precond(vt.astype(np.float64))
+    with cb.CLAIREInterface(make_opt(cb, n, nt, norm, beta)) as ci:
+        ci.set_images(mR, mT)
+        Jg, Dg, Rg = ci.EvaluateObjective(v)
+        assert abs(Dg - prob.last_D) <= 1e-5 * abs(prob.last_D)
+        assert abs(Rg - prob.last_R) <= 1e-5 * abs(prob.last_R) + 1e-14
+        assert abs(Jg - J) <= 1e-5 * abs(J)
+        gg = ci.EvaluateGradient(v)
+        assert rel(gg, g) < 1e-5
+        lam, bf = ci.GetAdjoint()
+        Hg = ci.HessianMatVec(v, vt)
+        assert rel(Hg, H) < 1e-5
+        Pg = ci.ApplyInvRegularizationOperator(vt)
+        assert rel(Pg, P) < 1e-5
+
+
+def test_forward_problem_and_round_trip(cb):
+    # apps/benchmark.cpp:297-380: transport forward with v, back with -v
+    n, nt = 64, 4
+    mT = R.template_sin2((n, n, n)).astype(np.float32)
+    v = R.velocity_trig((n, n, n), 0.5, reference_case=True).astype(np.float32)
+    ref1 = R.forward_transport(mT.astype(np.float64), v.astype(np.float64), nt)
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mT, mT)
+        ci.SetInitialGuess(v)
+        m1 = ci.SolveForwardProblem(mT)
+        assert rel(m1, ref1) < 1e-5
+        ci.SetInitialGuess(-v)
+        m0 = ci.SolveForwardProblem(m1)
+    ref0 = R.forward_transport(ref1, -v.astype(np.float64), nt)
+    assert rel(m0, ref0) < 1e-5
+    err = rel(m0, mT)
+    assert err < 2e-3  # the oracle's own round-trip error at this resolution is ~8e-4 at 32^3
+
+
+@pytest.mark.parametrize("n,norm,beta,nt,maxit", [(32, "h1s", 1e-2, 4, 10), (32, "h2s", 1e-3, 4, 4)])
+def test_full_registration_matches_oracle(cb, n, norm, beta, nt, maxit):
+    mR, mT, _ = c1_problem(n, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization(norm, beta))
+    res = R.gauss_newton(prob, R.GNOptions(maxit=maxit, gttol=1e-2))
+    opt = make_opt(cb, n, nt, norm, beta, maxit=maxit, opttol=1e-2)
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        ci.Run()
+        st = ci.stats()
+        vg = ci.GetSolution()
+    assert abs(st["gn_iterations"] - res["iters"]) <= 1
+    assert len(res["pcg_iters"]) == 0 or abs(st["pcg_iterations"] - sum(res["pcg_iters"])) <= len(res["pcg_iters"])
+    assert rel(vg, res["v"]) < 1e-4
+    mis = R.relative_mismatch(prob.mR, res["m1"], prob.mT)
+    assert abs(st["rel_mismatch"] - mis) <= 1e-4 * mis
+
+
+@pytest.mark.parametrize("norm,beta,nt", [("h1", 1e-2, 4), ("h2", 1e-3, 8)])
+def test_full_registration_fp32_conditioning(cb, norm, beta, nt):
+    # H1 / H2 keep the identity term beta1 = 1e-4, so their inverse symbol is
+    # 1/(beta0*beta1) (1e6 / 1e7) at k = 0 and PCG iteration counts react to
+    # FP32 roundoff (the oracle run in FP32 departs from the FP64 one in the
+    # same way).  GN counts and the objective still agree.
+    n = 32
+    mR, mT, _ = c1_problem(n, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization(norm, beta))
+    res = R.gauss_newton(prob, R.GNOptions(maxit=3, gttol=1e-2))
+    with cb.CLAIREInterface(make_opt(cb, n, nt, norm, beta, maxit=3, opttol=1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.Run()
+        st = ci.stats()
+    assert abs(st["gn_iterations"] - res["iters"]) <= 1
+    assert abs(st["J"] - res["J"]) <= 1e-3 * abs(res["J"])
+
+
+def test_batch_equals_single(cb):
+    # a problem gives the same result alone and inside a batch of different problems
+    n, nt = 32, 4
+    probs = [c1_problem(n, nt)]
+    rng = np.random.default_rng(11)
+    for k in range(2):
+        mR, mT, vs = c1_problem(n, nt)
+        shift = rng.integers(1, n, size=3)
+        probs.append((np.roll(mR, shift, axis=(0, 1, 2)).copy(), mT, vs))
+    opt = make_opt(cb, n, nt, "h1s", 1e-2, maxit=5, opttol=1e-2)
+    single = []
+    for (mR, mT, _) in probs:
+        with cb.CLAIREInterface(opt) as ci:
+            ci.set_images(mR, mT)
+            ci.Run()
+            single.append((ci.GetSolution(), ci.stats()))
+    with cb.CLAIREInterface(opt, nbatch=len(probs)) as ci:
+        for b, (mR, mT, _) in enumerate(probs):
+            ci.set_images(mR, mT, b)
+        ci.Run()
+        for b in range(len(probs)):
+            vb = ci.GetSolution(b)
+            st = ci.stats(b)
+            assert st["gn_iterations"] == single[b][1]["gn_iterations"]
+            assert rel(vb, single[b][0]) < 1e-6
