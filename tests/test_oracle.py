@@ -1,0 +1,192 @@
+"""Pin the oracle to the reference's own known-answer checks (CPU only).
+
+The reference ships no golden vectors; what it does check:
+tricubic Lagrange reproduction of cubics / node values, spectral operators
+exact on trig polynomials, the forward/backward transport round trip of
+apps/benchmark.cpp:297-380, the Taylor gradient test and the Hessian
+symmetry test of src/OptimizationProblem.cpp:157-496.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import claire_ref as R
+
+
+def test_lagrange_weights_partition_of_unity_and_nodes():
+    t = np.linspace(1.0, 2.0, 101)[:-1]
+    w = R.lagrange_weights(t)
+    assert np.allclose(sum(w), 1.0, atol=1e-14)
+    w1 = R.lagrange_weights(np.array([1.0]))
+    assert [float(x[0]) for x in w1] == [0.0, 1.0, 0.0, 0.0]
+
+
+def test_tricubic_reproduces_cubics():
+    n = 16
+    shape = (n, n, n)
+    rng = np.random.default_rng(0)
+    q = rng.uniform(2, n - 3, size=(3, 2000))
+    f = lambda a, b, c: 1 + 0.3 * a - 0.2 * b ** 2 + 0.01 * a * b * c + 0.001 * c ** 3 - 0.002 * a ** 2 * b
+    idx = R.index_grid(shape)
+    val = R.interp3(f(idx[0], idx[1], idx[2]), q)
+    assert np.max(np.abs(val - f(q[0], q[1], q[2]))) < 1e-11
+
+
+def test_tricubic_periodic_wrap_and_nodes():
+    n = 12
+    rng = np.random.default_rng(1)
+    F = rng.standard_normal((n, n, n))
+    idx = R.index_grid((n, n, n))
+    shift = rng.integers(-30, 30, size=(3, 1, 1, 1))
+    out = R.interp3(F, idx + shift)
+    ii = [(idx[d] + shift[d]).astype(int) % n for d in range(3)]
+    assert np.array_equal(out, F[ii[0], ii[1], ii[2]])
+
+
+def test_spectral_gradient_divergence_on_trig_polynomials():
+    n = 32
+    shape = (n, n, n)
+    x1, x2, x3 = R.grid_coords(shape)
+    m = np.sin(2 * x1) * np.cos(3 * x2) + np.sin(5 * x3)
+    g = R.grad(m)
+    assert np.max(np.abs(g[0] - 2 * np.cos(2 * x1) * np.cos(3 * x2))) < 1e-12
+    assert np.max(np.abs(g[1] + 3 * np.sin(2 * x1) * np.sin(3 * x2))) < 1e-12
+    assert np.max(np.abs(g[2] - 5 * np.cos(5 * x3))) < 1e-12
+    v = np.stack([np.sin(x1), np.cos(2 * x2), np.sin(3 * x3)])
+    d = R.div(v)
+    assert np.max(np.abs(d - (np.cos(x1) - 2 * np.sin(2 * x2) + 3 * np.cos(3 * x3)))) < 1e-12
+
+
+def test_nyquist_mode_has_zero_derivative():
+    n = 16
+    x1, _, _ = R.grid_coords((n, n, n))
+    m = np.cos(n / 2 * x1)   # pure Nyquist mode along x1
+    assert np.max(np.abs(R.grad(m))) < 1e-12
+
+
+@pytest.mark.parametrize("norm", ["h1s", "h1", "h2", "h2s", "h3", "h3s"])
+def test_regularization_symbols_on_a_single_mode(norm):
+    n = 16
+    shape = (n, n, n)
+    x1, x2, x3 = R.grid_coords(shape)
+    k = (1, 2, 3)
+    kap = float(sum(kk * kk for kk in k))
+    mode = np.cos(k[0] * x1 + k[1] * x2 + k[2] * x3)
+    v = np.stack([mode, 0.5 * mode, -mode])
+    reg = R.Regularization(norm, 1e-2, 1e-4)
+    hd = R.lebesgue_measure(shape)
+    b0, b1 = 1e-2, 1e-4
+    expect = {"h1s": hd * b0 * kap, "h1": hd * b0 * (kap + b1), "h2": b0 * (kap ** 2 + b1),
+              "h2s": hd * b0 * kap ** 2, "h3": b0 * (kap ** 3 + b1), "h3s": b0 * kap ** 3}[norm]
+    assert np.allclose(reg.gradient(v), expect * v, rtol=1e-12, atol=1e-12 * expect)
+    inv = {"h1s": b0 * kap, "h1": b0 * (kap + b1), "h2": b0 * (kap ** 2 + b1), "h2s": b0 * kap ** 2,
+           "h3": b0 * (kap ** 3 + b1), "h3s": b0 * kap ** 3}[norm]
+    # h1 / h2 amplify the roundoff mean of the mode by 1/(beta0*beta1) at k = 0
+    assert np.allclose(reg.apply_inverse(v), v / inv, rtol=1e-12, atol=1e-9)
+
+
+def test_h2_functional_matches_its_symbol():
+    # src/RegularizationH2.cpp:118-164: R = 1/2 hd ||sqrt(b0)(-kappa + sqrt(b1)) v||^2
+    n = 16
+    shape = (n, n, n)
+    x1, x2, x3 = R.grid_coords(shape)
+    mode = np.cos(x1 + 2 * x2)
+    v = np.stack([mode, mode, mode])
+    reg = R.Regularization("h2", 1e-3, 1e-4)
+    kap = 5.0
+    sym = math.sqrt(1e-3) * (-kap + math.sqrt(1e-4))
+    expect = 0.5 * R.lebesgue_measure(shape) * sym ** 2 * 3 * np.sum(mode ** 2)
+    assert abs(reg.functional(v) - expect) < 1e-12 * abs(expect)
+
+
+def test_leray_projection_is_divergence_free():
+    n = 16
+    rng = np.random.default_rng(2)
+    b = rng.standard_normal((3, n, n, n))
+    p = R.leray_projection(b, "stokes")
+    # away from the Nyquist planes (where the two wavenumber conventions differ)
+    k = R.spectral_k((n, n, n))
+    dh = sum(1j * k[d] * np.fft.rfftn(p[d]) for d in range(3))
+    keep = np.ones(dh.shape, bool)
+    keep[n // 2, :, :] = False
+    keep[:, n // 2, :] = False
+    keep[:, :, n // 2] = False
+    assert np.max(np.abs(dh[keep])) < 1e-9 * np.max(np.abs(np.fft.rfftn(b[0])))
+
+
+def test_forward_backward_round_trip_converges():
+    # apps/benchmark.cpp:297-380: transport m0 with v, then with -v
+    errs = []
+    for n in (16, 32):
+        mT = R.template_sin2((n, n, n))
+        v = R.velocity_trig((n, n, n), 0.5, reference_case=True)
+        m1 = R.forward_transport(mT, v, 4)
+        m0 = R.forward_transport(m1, -v, 4)
+        errs.append(np.linalg.norm(m0 - mT) / np.linalg.norm(mT))
+    assert errs[0] < 2e-2 and errs[1] < 2e-3 and errs[1] < errs[0] / 4
+
+
+@pytest.mark.parametrize("norm", ["h1s", "h2s"])
+def test_taylor_gradient(norm):
+    # src/OptimizationProblem.cpp:157-243; the SL gradient is the discretised
+    # continuous adjoint, so FD and g.w agree to discretisation accuracy.
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization(norm, 1e-2))
+    v = 0.3 * vs
+    J0 = prob.objective(v)
+    gw = R.dot(prob.gradient(v), vs)
+    for h in (1e-3, 1e-4):
+        fd = (prob.objective(v + h * vs) - J0) / h
+        assert abs(fd - gw) < 1e-2 * abs(gw)
+
+
+def test_hessian_symmetry():
+    # src/OptimizationProblem.cpp:439-496
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2))
+    v = 0.3 * vs
+    prob.objective(v)
+    prob.gradient(v)
+    w1 = vs
+    w2 = np.roll(vs, 3, axis=1)
+    a = prob.hessian_matvec(w1)
+    b = prob.hessian_matvec(w2)
+    assert abs(R.dot(a, w2) - R.dot(w1, b)) <= 1e-10 * np.linalg.norm(a) * np.linalg.norm(w2)
+
+
+def test_pcg_on_spd_diagonal_system():
+    rng = np.random.default_rng(3)
+    d = rng.uniform(1.0, 100.0, size=(3, 4, 4, 4))
+    b = rng.standard_normal((3, 4, 4, 4))
+    x, it, reason = R.pcg(lambda p: d * p, lambda r: r / d, b, rtol=1e-10, maxit=50)
+    assert reason == "converged" and it == 1
+    x, it, reason = R.pcg(lambda p: d * p, lambda r: r, b, rtol=1e-10, maxit=200)
+    assert reason == "converged" and np.allclose(d * x, b, atol=1e-8)
+
+
+def test_forcing_sequence():
+    # src/KrylovInterface.cpp:134-165
+    assert R.forcing_tolerance(1.0, 1.0) == 0.5
+    assert R.forcing_tolerance(0.01, 1.0) == pytest.approx(0.1)
+    assert R.forcing_tolerance(0.01, 1.0, "qdfs") == pytest.approx(0.01)
+
+
+def test_rescale_only_shifts_negative_minimum():
+    # src/CLAIREUtils.cpp:691-725
+    x = np.array([0.1, 0.5, 0.9])
+    assert np.allclose(R.rescale(x), x / 0.8)        # no shift for min >= -1e-6
+    y = np.array([-1.0, 0.0, 1.0])
+    assert np.allclose(R.rescale(y), [0.0, 0.5, 1.0])
+
+
+def test_gauss_newton_reduces_gradient_on_reference_problem():
+    # CLAIRE's own -synthetic 0 problem, h1s beta 1e-2, nt 4 (small grid)
+    n, nt = 16, 4
+    mR, mT, _ = R.synthetic_reference(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2))
+    res = R.gauss_newton(prob, R.GNOptions(maxit=10, gttol=1e-2))
+    assert res["reason"] == "gttol"
+    assert R.relative_mismatch(mR, res["m1"], mT) < 0.5
