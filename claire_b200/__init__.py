@@ -119,6 +119,7 @@ _signatures = {
     "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
     "claire_b200_reg_apply": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
     "claire_b200_reg_functional": (_I, [_P, _DA, _IA, _I, _DA, _P]),
+    "claire_b200_reg_apply_noalloc": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
     "claire_b200_leray": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_smooth": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),

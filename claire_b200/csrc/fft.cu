@@ -740,4 +740,42 @@ int launch_deriv(const float* in, long long ip, long long ifs, float* out, long 
   return e;
 }
 
+// 3-field spectral operator (r2c, x1 op, c2r store) on caller-provided
+// spectrum workspace and twiddle table: the launches allocate nothing.
+template <int N>
+static int spectral3_explicit_impl(const float* in, float* out, float2* spec, const SpecParams* params,
+                                   const Dims& d, int op, const float2* tw, cudaStream_t s) {
+  const long long n = d.n(), nc = d.nc();
+  const int n3h = N / 2 + 1;
+  const int nrows = d.n1 * d.n2;
+  int e = set_smem(k_r2c_rows<N>, row_smem<N>(false));
+  if (!e) e = set_smem(k_cols<N, false>, col_smem<N>(2));
+  if (!e) e = set_smem(k_cols<N, true>, col_smem<N>(2));
+  if (!e) e = set_smem(k_pencil<N>, col_smem<N>(4));
+  if (!e) e = set_smem(k_c2r_rows<N>, row_smem<N>(true));
+  if (e) return e;
+  const dim3 rows((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), 3, 1);
+  const int ncx2 = d.n1 * n3h;
+  const dim3 cols((ncx2 + ColCfg<N>::C - 1) / ColCfg<N>::C, 3, 1);
+  const int ncx1 = d.n2 * n3h;
+  const dim3 pen((ncx1 + ColCfg<N>::C - 1) / ColCfg<N>::C, 1, 1);
+  k_r2c_rows<N><<<rows, kThreads, row_smem<N>(false), s>>>(in, 0, n, spec, 0, nc, nrows, tw, nullptr);
+  k_cols<N, false><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+                                                          nullptr);
+  k_pencil<N><<<pen, kThreads, col_smem<N>(4), s>>>(spec, 0, nc, d, op, params, 3, 3, tw, nullptr);
+  k_cols<N, true><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+                                                         nullptr);
+  k_c2r_rows<N><<<rows, kThreads, row_smem<N>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
+                                                           nullptr, 0, nullptr);
+  return (int)cudaGetLastError();
+}
+
+int launch_spectral3_explicit(const float* in, float* out, float2* spec, const SpecParams* params, const Dims& d,
+                              int op, const float2* tw, cudaStream_t s) {
+  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  int e = 0;
+  CB_DISPATCH_N(d.n1, e = spectral3_explicit_impl<NN>(in, out, spec, params, d, op, tw, s));
+  return e;
+}
+
 }  // namespace cb

@@ -64,4 +64,10 @@ int c2r_partials(const Dims& d, int nf);
 
 bool fft_size_supported(int n);
 
+// 3-field op (forward r2c, op in the x1 pass, inverse c2r stored to out) using
+// a caller-provided spectrum workspace (3 * nc float2) and twiddle table
+// (W_N^m, m < N); allocates nothing.
+int launch_spectral3_explicit(const float* in, float* out, float2* spec, const SpecParams* params, const Dims& d,
+                              int op, const float2* tw, cudaStream_t s);
+
 }  // namespace cb

@@ -26,6 +26,7 @@ extern "C" {
 #define CB_ERR_NUMERIC (-4)   /* NaN / Inf in objective or gradient */
 #define CB_ERR_STATE (-5)     /* call out of order (e.g. run before images) */
 #define CB_ERR_UNSUPPORTED (-6) /* grid size without an FFT plan */
+#define CB_ERR_TOO_LARGE (-7)   /* grid exceeds a fixed-size workspace */
 
 /* Regularisation norms (-regnorm): l2 h1 h1s h2 h2s h3 h3s. */
 enum {
@@ -137,6 +138,18 @@ int claire_b200_fft_div(const float* v, float* d, const int nx[3], void* stream)
  * out (3n) = op(v (3n)); kind = CB_REG_GRADIENT / CB_REG_INVERSE / CB_REG_SQRTINVERSE. */
 int claire_b200_reg_apply(const float* v, float* out, const int nx[3], int regnorm, const double beta[2],
                           int kind, void* stream);
+/* Same operator as claire_b200_reg_apply, for callers that cannot allocate
+ * device memory while it runs (their allocator owns the whole GPU budget, or
+ * an allocation would synchronise or may fail mid-run).  No counterpart in the
+ * reference.  The FFT workspace, parameter block and twiddle tables are fixed
+ * device arrays inside the library (3.3 MB on every GPU that loads it, held
+ * until exit); nothing is allocated per call.  Grids up to 64^3 only (N in
+ * 16, 32, 48, 64): larger grids return CB_ERR_TOO_LARGE.  All calls share the
+ * workspace, so calls that overlap on the GPU race; serialise them.  The first
+ * call on a device sets it up (symbol lookup and twiddle upload with that
+ * device current): make it before any stream capture. */
+int claire_b200_reg_apply_noalloc(const float* v, float* out, const int nx[3], int regnorm, const double beta[2],
+                                  int kind, void* stream);
 /* Regularization::EvaluateFunctional: R(v) in FP64 (host result). */
 int claire_b200_reg_functional(const float* v, double* R, const int nx[3], int regnorm,
                                const double beta[2], void* stream);
