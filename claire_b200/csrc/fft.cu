@@ -15,6 +15,10 @@
 // Spectral derivatives are separable: d/dx_k of a periodic field only needs
 // the 1D transform along axis k, so gradient and divergence are one pass per
 // axis over real data.
+//
+// Every global->shared load is two-phase: a thread issues all of its loads
+// into registers (compile-time count) before it stores any of them, so each
+// thread keeps 8-32 independent loads in flight.
 #include <cstdio>
 #include <mutex>
 #include <vector>
@@ -67,7 +71,68 @@ template <int N> struct ColCfg {
   static constexpr int PITCH = C + 1;
 };
 
-constexpr int kThreads = 128;
+constexpr int kThreads = kFftThreads;
+
+// ---------------------------------------------------------------------------
+// load helpers
+// ---------------------------------------------------------------------------
+// Column tile: N elements (es apart) of the thread's column into split
+// re/im shared arrays.  The thread owns column c = tid % C and rows
+// e = tid / C + k * (kThreads / C).  colp == nullptr loads zeros.
+template <int N, int C, int PITCH>
+CB_DEVICE void load_col_tile(float* re, float* im, const float2* __restrict__ colp, long long es) {
+  constexpr int RSTEP = kThreads / C;
+  constexpr int K = N / RSTEP;
+  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
+  float2 v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = colp ? __ldg(colp + (long long)(e0 + k * RSTEP) * es) : make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = e0 + k * RSTEP;
+    re[e * PITCH + c] = v[k].x;
+    im[e * PITCH + c] = v[k].y;
+  }
+}
+
+template <int N, int C, int PITCH>
+CB_DEVICE void store_col_tile(const float* re, const float* im, float2* __restrict__ colp, long long es) {
+  constexpr int RSTEP = kThreads / C;
+  constexpr int K = N / RSTEP;
+  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
+  if (!colp) return;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = e0 + k * RSTEP;
+    colp[(long long)(e0 + k * RSTEP) * es] = make_float2(re[e * PITCH + c], im[e * PITCH + c]);
+  }
+}
+
+// Row chunk: 2P contiguous real rows of N floats -> pair-packed complex lines
+// (row 2p -> real part, row 2p+1 -> imaginary part of line p).  float4 loads.
+template <int N, int P, int PITCH>
+CB_DEVICE void load_row_chunk(float* re, float* im, const float* __restrict__ src, int nr) {
+  constexpr int Q = 2 * P * N / 4;          // float4s in the chunk
+  constexpr int K = Q / kThreads;           // per thread (exact for all plans)
+  static_assert(Q % kThreads == 0, "row chunk must split evenly");
+  float4 v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int q = threadIdx.x + k * kThreads;
+    const int r = (4 * q) / N;
+    v[k] = (r < nr) ? __ldg(reinterpret_cast<const float4*>(src) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int q = threadIdx.x + k * kThreads;
+    const int r = (4 * q) / N, e = 4 * q - r * N;
+    float* dst = ((r & 1) ? im : re) + (r >> 1);
+    dst[(e + 0) * PITCH] = v[k].x;
+    dst[(e + 1) * PITCH] = v[k].y;
+    dst[(e + 2) * PITCH] = v[k].z;
+    dst[(e + 3) * PITCH] = v[k].w;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // rows: r2c along x3.  Two real rows a, b are packed as z = a + i b; after
@@ -92,14 +157,10 @@ __global__ void __launch_bounds__(kThreads) k_r2c_rows(const float* __restrict__
   const int row0 = blockIdx.x * 2 * P;
   const int nr = min(2 * P, nrows - row0);
   load_twiddles<N>(tw, twg);
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += blockDim.x) {
-    const int r = idx / N, e = idx - r * N;
-    const float val = (r < nr) ? src[(long long)(row0 + r) * N + e] : 0.f;
-    ((r & 1) ? im : re)[e * PITCH + (r >> 1)] = val;
-  }
+  load_row_chunk<N, P, PITCH>(re, im, src + (long long)row0 * N, nr);
   __syncthreads();
-  fft_lines<N, false>(re, im, sre, sim, P, PITCH, tw);
-  for (int idx = threadIdx.x; idx < 2 * P * NH; idx += blockDim.x) {
+  fft_lines<N, false, P, PITCH>(re, im, sre, sim, tw);
+  for (int idx = threadIdx.x; idx < 2 * P * NH; idx += kThreads) {
     const int r = idx / NH, k = idx - r * NH;
     if (r >= nr) continue;
     const int line = r >> 1;
@@ -134,23 +195,37 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
   float* im = re + N * PITCH;
   float* sre = im + N * PITCH;
   float* sim = sre + N * PITCH;
-  float* str = sim + N * PITCH;          // staging: 2P rows x NH
+  float* str = sim + N * PITCH;  // staging: 2P rows x NH
   float* sti = str + 2 * P * NH;
   const float2* src = in + blockIdx.z * ip + blockIdx.y * ifs;
-  float* dst = out + blockIdx.z * op + blockIdx.y * ofs;
+  float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
   const int row0 = blockIdx.x * 2 * P;
   const int nr = min(2 * P, nrows - row0);
   load_twiddles<N>(tw, twg);
-  for (int idx = threadIdx.x; idx < 2 * P * NH; idx += blockDim.x) {
-    const int r = idx / NH, k = idx - r * NH;
-    float2 v = make_float2(0.f, 0.f);
-    if (r < nr) v = src[(long long)(row0 + r) * NH + k];
-    if (k == 0 || k == N / 2) v.y = 0.f;
-    str[idx] = v.x;
-    sti[idx] = v.y;
+  {
+    // two-phase load of the 2P x NH complex chunk (contiguous)
+    constexpr int TOT = 2 * P * NH;
+    constexpr int K = (TOT + kThreads - 1) / kThreads;
+    const float2* s0 = src + (long long)row0 * NH;
+    float2 v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int idx = threadIdx.x + k * kThreads;
+      v[k] = (idx < TOT && idx / NH < nr) ? __ldg(s0 + idx) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int idx = threadIdx.x + k * kThreads;
+      if (idx >= TOT) continue;
+      const int kk = idx % NH;
+      float2 w = v[k];
+      if (kk == 0 || kk == N / 2) w.y = 0.f;
+      str[idx] = w.x;
+      sti[idx] = w.y;
+    }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < P * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < P * N; idx += kThreads) {
     const int line = idx / N, e = idx - line * N;
     const int a = 2 * line, b = 2 * line + 1;
     float zr, zi;
@@ -170,10 +245,10 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
     im[e * PITCH + line] = zi;
   }
   __syncthreads();
-  fft_lines<N, true>(re, im, sre, sim, P, PITCH, tw);
+  fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
   const float al = alpha ? alpha[blockIdx.z] : 1.f;
   double acc = 0.0;
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 2 * P * N; idx += kThreads) {
     const int r = idx / N, e = idx - r * N;
     if (r >= nr) continue;
     const float val = al * ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
@@ -183,8 +258,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
     else acc += (double)val * (double)val;
   }
   if (epi == EPI_SUMSQ) {
-    block_reduce_store(acc, partials + (long long)blockIdx.z * nparts,
-                       blockIdx.x + gridDim.x * blockIdx.y);
+    block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
   }
 }
 
@@ -206,23 +280,13 @@ __global__ void __launch_bounds__(kThreads) k_cols(float2* __restrict__ data, lo
   float* sre = im + N * PITCH;
   float* sim = sre + N * PITCH;
   float2* base = data + blockIdx.z * pstr + blockIdx.y * fstr;
-  const int g0 = blockIdx.x * C;
+  const int g = blockIdx.x * C + threadIdx.x % C;
+  float2* colp = (g < ncols) ? base + (long long)(g / cpg) * gs + (g % cpg) : nullptr;
   load_twiddles<N>(tw, twg);
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int e = idx / C, c = idx - e * C;
-    const int g = g0 + c;
-    float2 v = make_float2(0.f, 0.f);
-    if (g < ncols) v = base[(long long)(g / cpg) * gs + (g % cpg) + e * es];
-    re[e * PITCH + c] = v.x;
-    im[e * PITCH + c] = v.y;
-  }
+  load_col_tile<N, C, PITCH>(re, im, colp, es);
   __syncthreads();
-  fft_lines<N, INV>(re, im, sre, sim, C, PITCH, tw);
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int e = idx / C, c = idx - e * C;
-    const int g = g0 + c;
-    if (g < ncols) base[(long long)(g / cpg) * gs + (g % cpg) + e * es] = make_float2(re[e * PITCH + c], im[e * PITCH + c]);
-  }
+  fft_lines<N, INV, C, PITCH>(re, im, sre, sim, tw);
+  store_col_tile<N, C, PITCH>(re, im, colp, es);
 }
 
 // ---------------------------------------------------------------------------
@@ -255,102 +319,151 @@ CB_DEVICE float reg_inv_operator(const SpecParams& q, float kap) {
   }
 }
 
-// Apply op at wavenumber index (i1, i2, i3) to the field values x[0..nin).
-CB_DEVICE void apply_op(int op, const SpecParams& q, const Dims& d, int i1, int i2, int i3,
-                        float2 (&x)[3], int nin) {
-  const float s = 1.f / (float)((double)d.n1 * d.n2 * d.n3);
-  const float k1 = (float)wavenumber(i1, d.n1), k2 = (float)wavenumber(i2, d.n2),
-              k3 = (float)wavenumber(i3, d.n3);
-  const float kap = k1 * k1 + k2 * k2 + k3 * k3;
+// Wavenumber data of one spectral column (x2 index i2, x3 index i3) and a
+// spectral element of it along x1 (index i1).
+struct ColumnK {
+  float k2, k3, l2, l3;   // Nyquist-zeroed and Nyquist-kept wavenumbers
+};
+
+CB_DEVICE ColumnK column_k(int i2, int i3, const Dims& d) {
+  ColumnK c;
+  c.k2 = (float)wavenumber(i2, d.n2);
+  c.k3 = (float)wavenumber(i3, d.n3);
+  c.l2 = (float)wavenumber_keep_nyquist(i2, d.n2);
+  c.l3 = (float)wavenumber_keep_nyquist(i3, d.n3);
+  return c;
+}
+
+// Per-field diagonal operators (one field, component index comp for H3/H3SN).
+CB_DEVICE float2 apply_op1(int op, const SpecParams& q, const Dims& d, int i1, const ColumnK& ck, int comp,
+                           float2 x, float s) {
+  const float k1 = (float)wavenumber(i1, d.n1);
+  const float kap = k1 * k1 + ck.k2 * ck.k2 + ck.k3 * ck.k3;
   switch (op) {
     case OP_REG_GRAD: {
       const float sig = s * reg_grad_symbol(q, kap);
-      for (int f = 0; f < 3; ++f) x[f] = make_float2(x[f].x * sig, x[f].y * sig);
-      break;
+      return make_float2(x.x * sig, x.y * sig);
     }
     case OP_REG_INV:
     case OP_REG_SQRTINV: {
       float o = reg_inv_operator(q, kap);
       if (op == OP_REG_SQRTINV) o = sqrtf(o);
       const float sig = s / o;
-      for (int f = 0; f < 3; ++f) x[f] = make_float2(x[f].x * sig, x[f].y * sig);
-      break;
+      return make_float2(x.x * sig, x.y * sig);
     }
     case OP_REG_FUNC: {
       if (q.norm == NORM_L2) {
         const float sig = s * sqrtf(q.beta0);
-        for (int f = 0; f < 3; ++f) x[f] = make_float2(x[f].x * sig, x[f].y * sig);
-      } else if (q.norm == NORM_H2) {
+        return make_float2(x.x * sig, x.y * sig);
+      }
+      if (q.norm == NORM_H2) {
         const float sig = s * sqrtf(q.beta0) * (-kap + sqrtf(q.beta1));
-        for (int f = 0; f < 3; ++f) x[f] = make_float2(x[f].x * sig, x[f].y * sig);
-      } else if (q.norm == NORM_H2SN) {
+        return make_float2(x.x * sig, x.y * sig);
+      }
+      if (q.norm == NORM_H2SN) {
         const float sig = -s * kap;
-        for (int f = 0; f < 3; ++f) x[f] = make_float2(x[f].x * sig, x[f].y * sig);
-      } else {  // H3 / H3SN: separate multipliers on real and imaginary parts
-        const float kk[3] = {k1, k2, k3};
-        for (int f = 0; f < 3; ++f) {
-          const float a = kk[f] * (-kap);
-          float mre, mim;
-          if (q.norm == NORM_H3) {
-            const float sb0 = sqrtf(q.beta0), sb1 = sqrtf(q.beta1);
-            mre = s * sb0 * (a + sb1);
-            mim = s * sb0 * (-a + sb1);
-          } else {
-            mre = s * a;
-            mim = -s * a;
-          }
-          x[f] = make_float2(x[f].x * mre, x[f].y * mim);
-        }
+        return make_float2(x.x * sig, x.y * sig);
       }
-      break;
-    }
-    case OP_LERAY:
-    case OP_LERAY_RELAXED: {
-      float kl;
-      float c = 1.f;
-      if (op == OP_LERAY) {
-        const float l1 = (float)wavenumber_keep_nyquist(i1, d.n1);
-        const float l2 = (float)wavenumber_keep_nyquist(i2, d.n2);
-        const float l3 = (float)wavenumber_keep_nyquist(i3, d.n3);
-        kl = l1 * l1 + l2 * l2 + l3 * l3;
+      // H3 / H3SN: separate multipliers on real and imaginary parts
+      const float kc = comp == 0 ? k1 : (comp == 1 ? ck.k2 : ck.k3);
+      const float a = kc * (-kap);
+      float mre, mim;
+      if (q.norm == NORM_H3) {
+        const float sb0 = sqrtf(q.beta0), sb1 = sqrtf(q.beta1);
+        mre = s * sb0 * (a + sb1);
+        mim = s * sb0 * (-a + sb1);
       } else {
-        kl = kap;
-        float opik = 1.f / (q.beta2 * (kap + 1.f));
-        c = 1.f / (q.beta0 * opik + 1.f);
+        mre = s * a;
+        mim = -s * a;
       }
-      const float L = (kl == 0.f) ? -1.f : -1.f / kl;
-      const float2 kd = make_float2(k1 * x[0].x + k2 * x[1].x + k3 * x[2].x,
-                                    k1 * x[0].y + k2 * x[1].y + k3 * x[2].y);
-      const float g = s * c * L;
-      x[0] = make_float2(g * k1 * kd.x, g * k1 * kd.y);
-      x[1] = make_float2(g * k2 * kd.x, g * k2 * kd.y);
-      x[2] = make_float2(g * k3 * kd.x, g * k3 * kd.y);
-      break;
+      return make_float2(x.x * mre, x.y * mim);
     }
     case OP_GAUSS: {
       const float l1 = (float)wavenumber_keep_nyquist(i1, d.n1);
-      const float l2 = (float)wavenumber_keep_nyquist(i2, d.n2);
-      const float l3 = (float)wavenumber_keep_nyquist(i3, d.n3);
       const float c1 = q.sigma[0] * (float)(kTwoPi / d.n1), c2 = q.sigma[1] * (float)(kTwoPi / d.n2),
                   c3 = q.sigma[2] * (float)(kTwoPi / d.n3);
-      const float sik = expf(-0.5f * (l1 * l1 * c1 * c1 + l2 * l2 * c2 * c2 + l3 * l3 * c3 * c3));
-      for (int f = 0; f < nin; ++f) x[f] = make_float2(x[f].x * s * sik, x[f].y * s * sik);
-      break;
+      const float sik = expf(-0.5f * (l1 * l1 * c1 * c1 + ck.l2 * ck.l2 * c2 * c2 + ck.l3 * ck.l3 * c3 * c3));
+      return make_float2(x.x * s * sik, x.y * s * sik);
     }
-    default: {
-      for (int f = 0; f < nin; ++f) x[f] = make_float2(x[f].x * s, x[f].y * s);
-    }
+    default:
+      return make_float2(x.x * s, x.y * s);
   }
 }
 
-// x1 pencil: forward FFT along x1 of nin fields, op, inverse FFT of nout fields.
+// Coupled 3-field projections b -> F^-1(-c k (k . b^)/kappa): Stokes keeps the
+// Nyquist index in kappa, the relaxed model zeroes it and scales by
+// c = (beta_v (beta_w (kappa + 1))^-1 + 1)^-1.
+CB_DEVICE void apply_op3(int op, const SpecParams& q, const Dims& d, int i1, const ColumnK& ck, float2 (&x)[3],
+                         float s) {
+  const float k1 = (float)wavenumber(i1, d.n1);
+  const float kap = k1 * k1 + ck.k2 * ck.k2 + ck.k3 * ck.k3;
+  float kl, c = 1.f;
+  if (op == OP_LERAY) {
+    const float l1 = (float)wavenumber_keep_nyquist(i1, d.n1);
+    kl = l1 * l1 + ck.l2 * ck.l2 + ck.l3 * ck.l3;
+  } else {
+    kl = kap;
+    const float opik = 1.f / (q.beta2 * (kap + 1.f));
+    c = 1.f / (q.beta0 * opik + 1.f);
+  }
+  const float L = (kl == 0.f) ? -1.f : -1.f / kl;
+  const float2 kd = make_float2(k1 * x[0].x + ck.k2 * x[1].x + ck.k3 * x[2].x,
+                                k1 * x[0].y + ck.k2 * x[1].y + ck.k3 * x[2].y);
+  const float g = s * c * L;
+  x[0] = make_float2(g * k1 * kd.x, g * k1 * kd.y);
+  x[1] = make_float2(g * ck.k2 * kd.x, g * ck.k2 * kd.y);
+  x[2] = make_float2(g * ck.k3 * kd.x, g * ck.k3 * kd.y);
+}
+
+// x1 pencil, one field per CTA (grid.y = field): forward FFT along x1, the
+// diagonal symbol, inverse FFT.
 template <int N>
-__global__ void __launch_bounds__(kThreads) k_pencil(float2* __restrict__ spec, long long pstr,
-                                                      long long fstr, Dims d, int op,
-                                                      const SpecParams* __restrict__ params, int nin,
-                                                      int nout, const float2* __restrict__ twg,
-                                                      const int* __restrict__ active) {
+__global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec, long long pstr, long long fstr,
+                                                       Dims d, int op, const SpecParams* __restrict__ params,
+                                                       const float2* __restrict__ twg,
+                                                       const int* __restrict__ active) {
   constexpr int C = ColCfg<N>::C, PITCH = ColCfg<N>::PITCH;
+  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
+  if (active && !active[blockIdx.z]) return;
+  extern __shared__ float smem[];
+  float2* tw = reinterpret_cast<float2*>(smem);
+  float* re = smem + 2 * N;
+  float* im = re + N * PITCH;
+  float* sre = im + N * PITCH;
+  float* sim = sre + N * PITCH;
+  const int n3h = d.n3 / 2 + 1;
+  const int ncols = d.n2 * n3h;
+  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
+  const int g = blockIdx.x * C + c;
+  float2* colp = (g < ncols) ? spec + blockIdx.z * pstr + blockIdx.y * fstr + g : nullptr;
+  const SpecParams q = params[blockIdx.z];
+  const ColumnK ck = column_k(g / n3h, g % n3h, d);
+  const float s = 1.f / (float)((double)d.n1 * d.n2 * d.n3);
+  load_twiddles<N>(tw, twg);
+  load_col_tile<N, C, PITCH>(re, im, colp, ncols);
+  __syncthreads();
+  fft_lines<N, false, C, PITCH>(re, im, sre, sim, tw);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = e0 + k * RSTEP;
+    const int a = e * PITCH + c;
+    const float2 y = apply_op1(op, q, d, e, ck, blockIdx.y, make_float2(re[a], im[a]), s);
+    re[a] = y.x;
+    im[a] = y.y;
+  }
+  __syncthreads();
+  fft_lines<N, true, C, PITCH>(re, im, sre, sim, tw);
+  store_col_tile<N, C, PITCH>(re, im, colp, ncols);
+}
+
+// x1 pencil with the three fields in one CTA (coupled projections).
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec, long long pstr, long long fstr,
+                                                       Dims d, int op, const SpecParams* __restrict__ params,
+                                                       const float2* __restrict__ twg,
+                                                       const int* __restrict__ active) {
+  constexpr int C = ColCfg<N>::C, PITCH = ColCfg<N>::PITCH;
+  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -358,51 +471,44 @@ __global__ void __launch_bounds__(kThreads) k_pencil(float2* __restrict__ spec, 
   float* sim = sre + N * PITCH;
   float* fre[3];
   float* fim[3];
+#pragma unroll
   for (int f = 0; f < 3; ++f) {
     fre[f] = sim + N * PITCH + 2 * f * N * PITCH;
     fim[f] = fre[f] + N * PITCH;
   }
   const int n3h = d.n3 / 2 + 1;
   const int ncols = d.n2 * n3h;
-  const long long es = ncols;
-  float2* base = spec + blockIdx.z * pstr;
-  const int g0 = blockIdx.x * C;
+  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
+  const int g = blockIdx.x * C + c;
+  float2* colp = (g < ncols) ? spec + blockIdx.z * pstr + g : nullptr;
   const SpecParams q = params[blockIdx.z];
+  const ColumnK ck = column_k(g / n3h, g % n3h, d);
+  const float s = 1.f / (float)((double)d.n1 * d.n2 * d.n3);
   load_twiddles<N>(tw, twg);
-  for (int f = 0; f < nin; ++f) {
-    for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-      const int e = idx / C, c = idx - e * C;
-      const int g = g0 + c;
-      float2 v = make_float2(0.f, 0.f);
-      if (g < ncols) v = base[f * fstr + g + e * es];
-      fre[f][e * PITCH + c] = v.x;
-      fim[f][e * PITCH + c] = v.y;
-    }
-  }
+#pragma unroll
+  for (int f = 0; f < 3; ++f) load_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
   __syncthreads();
-  for (int f = 0; f < nin; ++f) fft_lines<N, false>(fre[f], fim[f], sre, sim, C, PITCH, tw);
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int e = idx / C, c = idx - e * C;
-    const int g = g0 + c;
-    if (g >= ncols) continue;
+#pragma unroll 1
+  for (int f = 0; f < 3; ++f) fft_lines<N, false, C, PITCH>(fre[f], fim[f], sre, sim, tw);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = e0 + k * RSTEP;
+    const int a = e * PITCH + c;
     float2 x[3];
-    for (int f = 0; f < 3; ++f)
-      x[f] = (f < nin) ? make_float2(fre[f][e * PITCH + c], fim[f][e * PITCH + c]) : make_float2(0.f, 0.f);
-    apply_op(op, q, d, e, g / n3h, g % n3h, x, nin);
-    for (int f = 0; f < nout; ++f) {
-      fre[f][e * PITCH + c] = x[f].x;
-      fim[f][e * PITCH + c] = x[f].y;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) x[f] = make_float2(fre[f][a], fim[f][a]);
+    apply_op3(op, q, d, e, ck, x, s);
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      fre[f][a] = x[f].x;
+      fim[f][a] = x[f].y;
     }
   }
   __syncthreads();
-  for (int f = 0; f < nout; ++f) fft_lines<N, true>(fre[f], fim[f], sre, sim, C, PITCH, tw);
-  for (int f = 0; f < nout; ++f) {
-    for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-      const int e = idx / C, c = idx - e * C;
-      const int g = g0 + c;
-      if (g < ncols) base[f * fstr + g + e * es] = make_float2(fre[f][e * PITCH + c], fim[f][e * PITCH + c]);
-    }
-  }
+#pragma unroll 1
+  for (int f = 0; f < 3; ++f) fft_lines<N, true, C, PITCH>(fre[f], fim[f], sre, sim, tw);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) store_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
 }
 
 // ---------------------------------------------------------------------------
@@ -411,12 +517,12 @@ __global__ void __launch_bounds__(kThreads) k_pencil(float2* __restrict__ spec, 
 // and imaginary parts of the result are the derivatives of a and b.
 // AXIS 2: rows (x3, contiguous).  AXIS 0/1: columns along x1 / x2.
 // ---------------------------------------------------------------------------
-template <int N>
-CB_DEVICE void mul_ik(float* re, float* im, int nlines, int pitch, float hscale) {
-  for (int idx = threadIdx.x; idx < nlines * N; idx += blockDim.x) {
-    const int e = idx / nlines, p = idx - e * nlines;
+template <int N, int NL, int PITCH>
+CB_DEVICE void mul_ik(float* re, float* im, float hscale) {
+  for (int idx = threadIdx.x; idx < NL * N; idx += kThreads) {
+    const int e = idx / NL, p = idx - e * NL;
     const float k = (float)wavenumber(e, N) * hscale;
-    const int a = e * pitch + p;
+    const int a = e * PITCH + p;
     const float xr = re[a], xi = im[a];
     re[a] = -k * xi;
     im[a] = k * xr;
@@ -439,22 +545,18 @@ __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict
   float* sre = im + N * PITCH;
   float* sim = sre + N * PITCH;
   const float* src = in + blockIdx.z * ip + blockIdx.y * ifs;
-  float* dst = out + blockIdx.z * op + blockIdx.y * ofs;
+  float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
   const int row0 = blockIdx.x * 2 * P;
   const int nr = min(2 * P, nrows - row0);
   load_twiddles<N>(tw, twg);
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += blockDim.x) {
-    const int r = idx / N, e = idx - r * N;
-    const float val = (r < nr) ? src[(long long)(row0 + r) * N + e] : 0.f;
-    ((r & 1) ? im : re)[e * PITCH + (r >> 1)] = val;
-  }
+  load_row_chunk<N, P, PITCH>(re, im, src + (long long)row0 * N, nr);
   __syncthreads();
-  fft_lines<N, false>(re, im, sre, sim, P, PITCH, tw);
-  mul_ik<N>(re, im, P, PITCH, 1.f / (float)N);
+  fft_lines<N, false, P, PITCH>(re, im, sre, sim, tw);
+  mul_ik<N, P, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
-  fft_lines<N, true>(re, im, sre, sim, P, PITCH, tw);
+  fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
   double acc = 0.0;
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 2 * P * N; idx += kThreads) {
     const int r = idx / N, e = idx - r * N;
     if (r >= nr) continue;
     const float val = ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
@@ -475,10 +577,11 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
                                                           const float2* __restrict__ twg, int epi,
                                                           double* __restrict__ partials, int nparts,
                                                           const int* __restrict__ active) {
-  constexpr int C = 2 * ColCfg<N>::C;   // real columns per CTA
-  if (active && !active[blockIdx.z]) return;
-  constexpr int L = ColCfg<N>::C;       // packed complex lines
+  constexpr int L = ColCfg<N>::C;       // packed complex lines per CTA
+  constexpr int C = 2 * L;              // real columns per CTA
   constexpr int PITCH = ColCfg<N>::PITCH;
+  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
+  if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
   float* re = smem + 2 * N;
@@ -486,30 +589,36 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   float* sre = im + N * PITCH;
   float* sim = sre + N * PITCH;
   const float* src = in + blockIdx.z * ip + blockIdx.y * ifs;
-  float* dst = out + blockIdx.z * op + blockIdx.y * ofs;
-  const int g0 = blockIdx.x * C;
+  float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
+  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
+  const int g = blockIdx.x * C + c;
+  const bool ok = g < ncols;
+  const long long cbase = ok ? (long long)(g / cpg) * gs + (g % cpg) : 0;
+  float* lane = ((c & 1) ? im : re) + (c >> 1);
   load_twiddles<N>(tw, twg);
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int e = idx / C, c = idx - e * C;
-    const int g = g0 + c;
-    const float val = (g < ncols) ? src[(long long)(g / cpg) * gs + (g % cpg) + e * es] : 0.f;
-    ((c & 1) ? im : re)[e * PITCH + (c >> 1)] = val;
+  {
+    float v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = ok ? __ldg(src + cbase + (long long)(e0 + k * RSTEP) * es) : 0.f;
+#pragma unroll
+    for (int k = 0; k < K; ++k) lane[(e0 + k * RSTEP) * PITCH] = v[k];
   }
   __syncthreads();
-  fft_lines<N, false>(re, im, sre, sim, L, PITCH, tw);
-  mul_ik<N>(re, im, L, PITCH, 1.f / (float)N);
+  fft_lines<N, false, L, PITCH>(re, im, sre, sim, tw);
+  mul_ik<N, L, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
-  fft_lines<N, true>(re, im, sre, sim, L, PITCH, tw);
+  fft_lines<N, true, L, PITCH>(re, im, sre, sim, tw);
   double acc = 0.0;
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int e = idx / C, c = idx - e * C;
-    const int g = g0 + c;
-    if (g >= ncols) continue;
-    const float val = ((c & 1) ? im : re)[e * PITCH + (c >> 1)];
-    const long long gi = (long long)(g / cpg) * gs + (g % cpg) + e * es;
-    if (epi == EPI_STORE) dst[gi] = val;
-    else if (epi == EPI_ADD) dst[gi] += val;
-    else acc += (double)val * (double)val;
+  if (ok) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int e = e0 + k * RSTEP;
+      const float val = lane[e * PITCH];
+      const long long gi = cbase + (long long)e * es;
+      if (epi == EPI_STORE) dst[gi] = val;
+      else if (epi == EPI_ADD) dst[gi] += val;
+      else acc += (double)val * (double)val;
+    }
   }
   if (epi == EPI_SUMSQ)
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
@@ -534,6 +643,8 @@ template <typename K> static int set_smem(K kernel, size_t bytes) {
   }
   return 0;
 }
+
+static bool aligned16(const void* p) { return (reinterpret_cast<unsigned long long>(p) & 15) == 0; }
 
 #define CB_DISPATCH_N(n, CALL)                         \
   switch (n) {                                         \
@@ -592,16 +703,25 @@ static int cols_impl(float2* data, long long pstr, long long fstr, int ncols, in
 
 template <int N>
 static int pencil_impl(float2* spec, long long sp, long long fstr, int nprob, const Dims& d, int op,
-                       const SpecParams* params, int nin, int nout, const int* active,
-                       cudaStream_t s) {
+                       const SpecParams* params, int nin, int nout, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  size_t sm = col_smem<N>(4);
-  int e = set_smem(k_pencil<N>, sm);
-  if (e) return e;
   const int ncols = d.n2 * (d.n3 / 2 + 1);
-  dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, 1, nprob);
-  k_pencil<N><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, nin, nout, tw, active);
+  if (op == OP_LERAY || op == OP_LERAY_RELAXED) {
+    if (nin != 3 || nout != 3) return (int)cudaErrorInvalidValue;
+    size_t sm = col_smem<N>(4);
+    int e = set_smem(k_pencil3<N>, sm);
+    if (e) return e;
+    dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, 1, nprob);
+    k_pencil3<N><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
+  } else {
+    if (nin != nout) return (int)cudaErrorInvalidValue;
+    size_t sm = col_smem<N>(2);
+    int e = set_smem(k_pencil1<N>, sm);
+    if (e) return e;
+    dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, nin, nprob);
+    k_pencil1<N><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
+  }
   return (int)cudaGetLastError();
 }
 
@@ -611,7 +731,7 @@ static bool cubic_supported(const Dims& d) {
 
 int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, long long sp, int nf,
                  int nprob, const Dims& d, const int* active, cudaStream_t s) {
-  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (!cubic_supported(d) || !aligned16(in) || ((ip | ifs) & 3)) return (int)cudaErrorInvalidValue;
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
@@ -632,19 +752,17 @@ int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
 }
 
 static int row_lines(int n) {
-  int P = 0;
   switch (n) {
-    case 16: P = RowCfg<16>::P; break;
-    case 32: P = RowCfg<32>::P; break;
-    case 48: P = RowCfg<48>::P; break;
-    case 64: P = RowCfg<64>::P; break;
-    case 96: P = RowCfg<96>::P; break;
-    case 128: P = RowCfg<128>::P; break;
-    case 192: P = RowCfg<192>::P; break;
-    case 256: P = RowCfg<256>::P; break;
-    default: P = 0;
+    case 16: return RowCfg<16>::P;
+    case 32: return RowCfg<32>::P;
+    case 48: return RowCfg<48>::P;
+    case 64: return RowCfg<64>::P;
+    case 96: return RowCfg<96>::P;
+    case 128: return RowCfg<128>::P;
+    case 192: return RowCfg<192>::P;
+    case 256: return RowCfg<256>::P;
+    default: return 0;
   }
-  return P;
 }
 
 static int col_lines(int n) {
@@ -733,6 +851,7 @@ int launch_deriv(const float* in, long long ip, long long ifs, float* out, long 
                  long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
                  double* partials, int nparts, const int* active, cudaStream_t s) {
   if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (axis == 2 && (!aligned16(in) || ((ip | ifs) & 3))) return (int)cudaErrorInvalidValue;
   const int n = (axis == 0) ? d.n1 : (axis == 1 ? d.n2 : d.n3);
   int e = 0;
   CB_DISPATCH_N(n, e = deriv_impl<NN>(in, ip, ifs, out, op_, ofs, nf, nprob, d, axis, epi, partials, nparts,
@@ -751,18 +870,18 @@ static int spectral3_explicit_impl(const float* in, float* out, float2* spec, co
   int e = set_smem(k_r2c_rows<N>, row_smem<N>(false));
   if (!e) e = set_smem(k_cols<N, false>, col_smem<N>(2));
   if (!e) e = set_smem(k_cols<N, true>, col_smem<N>(2));
-  if (!e) e = set_smem(k_pencil<N>, col_smem<N>(4));
+  if (!e) e = set_smem(k_pencil1<N>, col_smem<N>(2));
   if (!e) e = set_smem(k_c2r_rows<N>, row_smem<N>(true));
   if (e) return e;
   const dim3 rows((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), 3, 1);
   const int ncx2 = d.n1 * n3h;
   const dim3 cols((ncx2 + ColCfg<N>::C - 1) / ColCfg<N>::C, 3, 1);
   const int ncx1 = d.n2 * n3h;
-  const dim3 pen((ncx1 + ColCfg<N>::C - 1) / ColCfg<N>::C, 1, 1);
+  const dim3 pen((ncx1 + ColCfg<N>::C - 1) / ColCfg<N>::C, 3, 1);
   k_r2c_rows<N><<<rows, kThreads, row_smem<N>(false), s>>>(in, 0, n, spec, 0, nc, nrows, tw, nullptr);
   k_cols<N, false><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                           nullptr);
-  k_pencil<N><<<pen, kThreads, col_smem<N>(4), s>>>(spec, 0, nc, d, op, params, 3, 3, tw, nullptr);
+  k_pencil1<N><<<pen, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, d, op, params, tw, nullptr);
   k_cols<N, true><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                          nullptr);
   k_c2r_rows<N><<<rows, kThreads, row_smem<N>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
@@ -772,7 +891,7 @@ static int spectral3_explicit_impl(const float* in, float* out, float2* spec, co
 
 int launch_spectral3_explicit(const float* in, float* out, float2* spec, const SpecParams* params, const Dims& d,
                               int op, const float2* tw, cudaStream_t s) {
-  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (!cubic_supported(d) || !aligned16(in)) return (int)cudaErrorInvalidValue;
   int e = 0;
   CB_DISPATCH_N(d.n1, e = spectral3_explicit_impl<NN>(in, out, spec, params, d, op, tw, s));
   return e;

@@ -2,8 +2,9 @@
 //
 // A CTA transforms `nlines` complex lines of length N that live in shared
 // memory as split real/imaginary arrays: element e of line p sits at
-// re[e*pitch + p], im[e*pitch + p] (line index fastest, pitch odd so that
-// consecutive lines hit distinct banks).  Every plan has exactly two radix
+// re[e*PITCH + p], im[e*PITCH + p] (line index fastest, PITCH odd so that
+// consecutive lines hit distinct banks).  Line count and pitch are
+// compile-time so every loop has a known trip count.  Every plan has exactly two radix
 // stages (N = R0*R1, R0, R1 in {4, 8, 12, 16}), each an in-register DFT
 // followed by one shared-memory exchange, so the result lands back in the
 // source buffer after one ping-pong through the scratch buffer.
@@ -133,20 +134,22 @@ template <> struct Plan<128> { static constexpr int R0 = 16, R1 = 8; };
 template <> struct Plan<192> { static constexpr int R0 = 12, R1 = 16; };
 template <> struct Plan<256> { static constexpr int R0 = 16, R1 = 16; };
 
-template <int N, int R, int NS, bool INV>
+constexpr int kFftThreads = 128;  // threads per CTA of every FFT kernel
+
+template <int N, int R, int NS, bool INV, int NL, int PITCH>
 CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict__ sim,
-                         float* __restrict__ dre, float* __restrict__ dim, int nlines,
-                         int pitch, const float2* __restrict__ tw) {
+                         float* __restrict__ dre, float* __restrict__ dim, const float2* __restrict__ tw) {
   constexpr int J = N / R;
-  const int total = nlines * J;
-  for (int u = threadIdx.x; u < total; u += blockDim.x) {
-    const int p = u % nlines;
-    const int j = u / nlines;
+  constexpr int total = NL * J;
+#pragma unroll 2
+  for (int u = threadIdx.x; u < total; u += kFftThreads) {
+    const int p = u % NL;
+    const int j = u / NL;
     const int k = j % NS;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int idx = (j + r * J) * pitch + p;
+      const int idx = (j + r * J) * PITCH + p;
       v[r] = make_float2(sre[idx], sim[idx]);
     }
     if (NS > 1) {
@@ -161,7 +164,7 @@ CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict_
     const int o = (j - k) * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int idx = (o + r * NS) * pitch + p;
+      const int idx = (o + r * NS) * PITCH + p;
       dre[idx] = v[r].x;
       dim[idx] = v[r].y;
     }
@@ -171,20 +174,19 @@ CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict_
 // Transform nlines lines held in (re, im); (sre, sim) is scratch of the same
 // size.  The result is back in (re, im).  Caller synchronises before; this
 // function synchronises after each stage.
-template <int N, bool INV>
-CB_DEVICE void fft_lines(float* re, float* im, float* sre, float* sim, int nlines, int pitch,
-                         const float2* tw) {
+template <int N, bool INV, int NL, int PITCH>
+CB_DEVICE void fft_lines(float* re, float* im, float* sre, float* sim, const float2* tw) {
   using P = Plan<N>;
-  fft_stage<N, P::R0, 1, INV>(re, im, sre, sim, nlines, pitch, tw);
+  fft_stage<N, P::R0, 1, INV, NL, PITCH>(re, im, sre, sim, tw);
   __syncthreads();
-  fft_stage<N, P::R1, P::R0, INV>(sre, sim, re, im, nlines, pitch, tw);
+  fft_stage<N, P::R1, P::R0, INV, NL, PITCH>(sre, sim, re, im, tw);
   __syncthreads();
 }
 
 // Stage the N-entry twiddle table into shared memory.
 template <int N>
 CB_DEVICE void load_twiddles(float2* dst, const float2* __restrict__ src) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) dst[i] = src[i];
+  for (int i = threadIdx.x; i < N; i += kFftThreads) dst[i] = src[i];
 }
 
 }  // namespace cb
