@@ -91,9 +91,12 @@ def draw_ellipsoid_params(rng, count=40):
 
 
 def draw_velocity_coeffs(rng, n, kmax=6, amp=0.3):
-    k = _wavenumbers(n).astype(np.float64)
+    # Nyquist indices keep their magnitude n/2 > kmax: no Nyquist mode (a +-1
+    # checkerboard on the grid) enters the field
+    k = np.arange(n, dtype=np.float64)
+    k[k > n // 2] -= n
     k3 = k[: n // 2 + 1].copy()
-    k3[n // 2] = 0
+    k3[n // 2] = n // 2
     kk = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k3[None, None, :] ** 2)
     mask = (kk >= 1.0) & (kk <= kmax)
     coeffs = []

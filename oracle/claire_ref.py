@@ -827,7 +827,9 @@ def velocity_random(shape, rng, kmax=6, amp=0.3, dtype=np.float64):
     coefficients N(0, amp)/|k|^2 on 1 <= |k| <= kmax, Hermitian through the
     real inverse FFT, Nyquist zero; coefficient c gives c*e^{ik.x} + c.c."""
     n1, n2, n3 = shape
-    k1, k2, k3 = spectral_k(shape, nyquist_zero=True)
+    # Nyquist indices keep their magnitude n/2 > kmax, so no Nyquist mode
+    # (a +-1 checkerboard on the grid) enters the field
+    k1, k2, k3 = spectral_k(shape, nyquist_zero=False)
     kk = np.sqrt(k1 * k1 + k2 * k2 + k3 * k3)
     mask = (kk >= 1.0) & (kk <= kmax)
     out = []
