@@ -337,8 +337,17 @@ int claire_b200_get_adjoint(claire_b200_ctx* c, int b, float* lambda0, float* bo
   if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;
   int e = CB_OK;
-  if (lambda0) e = copy_out(s, lambda0, s.lam + b * s.n, s.n, 0);
-  if (!e && body_force) e = copy_out(s, body_force, s.bf + b * 3 * s.n, 3 * s.n, 0);
+  if (lambda0) e = copy_out(s, lambda0, s.lamh + b * (s.nt + 1) * s.n, s.n, 0);
+  if (!e && body_force) {
+    if (s.opts.model == CB_MODEL_COMPRESSIBLE) {
+      // without a projection the sweep writes its body force straight into the
+      // gradient / matvec output; re-form it from the stored adjoint levels
+      e = cuda_status(launch_body_force(s.lamh + b * (s.nt + 1) * s.n, 0, s.gm + b * (s.nt + 1) * 3 * s.n, 0,
+                                        s.bf + b * 3 * s.n, 0, s.nt, s.ht, s.hd, 1, s.n, nullptr, s.stream));
+      note_launches(1);
+    }
+    if (!e) e = copy_out(s, body_force, s.bf + b * 3 * s.n, 3 * s.n, 0);
+  }
   return e;
 }
 

@@ -73,6 +73,41 @@ template <int N> struct ColCfg {
 
 constexpr int kThreads = kFftThreads;
 
+// Epilogue of the row kernels: value of row r, element e sits at
+// ((r & 1) ? im : re)[e * PITCH + r / 2]; store it, add it to dst, or
+// accumulate its square.  For EPI_ADD the old values of a group of 8 elements
+// are loaded before any of them is stored, so the loads overlap.
+template <int N, int P, int PITCH>
+CB_DEVICE double rows_epilogue(const float* re, const float* im, float* __restrict__ dst, int row0, int nr,
+                               int epi, float al) {
+  constexpr int TOTAL = 2 * P * N;
+  constexpr int G = 8;
+  double acc = 0.0;
+  for (int i0 = threadIdx.x; i0 < TOTAL; i0 += G * kThreads) {
+    float old[G];
+    if (epi == EPI_ADD) {
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        const int idx = i0 + u * kThreads;
+        const int r = idx / N, e = idx - r * N;
+        old[u] = (idx < TOTAL && r < nr) ? dst[(long long)(row0 + r) * N + e] : 0.f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+      const int idx = i0 + u * kThreads;
+      const int r = idx / N, e = idx - r * N;
+      if (idx >= TOTAL || r >= nr) continue;
+      const float val = al * ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
+      const long long gi = (long long)(row0 + r) * N + e;
+      if (epi == EPI_STORE) dst[gi] = val;
+      else if (epi == EPI_ADD) dst[gi] = old[u] + val;
+      else acc += (double)val * (double)val;
+    }
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------
 // load helpers
 // ---------------------------------------------------------------------------
@@ -247,16 +282,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
   __syncthreads();
   fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
   const float al = alpha ? alpha[blockIdx.z] : 1.f;
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += kThreads) {
-    const int r = idx / N, e = idx - r * N;
-    if (r >= nr) continue;
-    const float val = al * ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
-    const long long gi = (long long)(row0 + r) * N + e;
-    if (epi == EPI_STORE) dst[gi] = val;
-    else if (epi == EPI_ADD) dst[gi] += val;
-    else acc += (double)val * (double)val;
-  }
+  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, row0, nr, epi, al);
   if (epi == EPI_SUMSQ) {
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
   }
@@ -555,16 +581,7 @@ __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict
   mul_ik<N, P, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
   fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < 2 * P * N; idx += kThreads) {
-    const int r = idx / N, e = idx - r * N;
-    if (r >= nr) continue;
-    const float val = ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
-    const long long gi = (long long)(row0 + r) * N + e;
-    if (epi == EPI_STORE) dst[gi] = val;
-    else if (epi == EPI_ADD) dst[gi] += val;
-    else acc += (double)val * (double)val;
-  }
+  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, row0, nr, epi, 1.f);
   if (epi == EPI_SUMSQ)
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
 }
@@ -610,13 +627,16 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   fft_lines<N, true, L, PITCH>(re, im, sre, sim, tw);
   double acc = 0.0;
   if (ok) {
+    float old[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) old[k] = (epi == EPI_ADD) ? dst[cbase + (long long)(e0 + k * RSTEP) * es] : 0.f;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int e = e0 + k * RSTEP;
       const float val = lane[e * PITCH];
       const long long gi = cbase + (long long)e * es;
       if (epi == EPI_STORE) dst[gi] = val;
-      else if (epi == EPI_ADD) dst[gi] += val;
+      else if (epi == EPI_ADD) dst[gi] = old[k] + val;
       else acc += (double)val * (double)val;
     }
   }

@@ -1,5 +1,5 @@
 // Semi-Lagrangian kernels: RK2 characteristics, tricubic gathers and the
-// fused state / adjoint / incremental time steps.
+// state / adjoint / incremental time steps built on them.
 //
 // Reference loops: SemiLagrangian::ComputeTrajectoryRK2
 // (src/SemiLagrangian.cpp:192-289), Interp3_Plan::interpolate +
@@ -10,35 +10,22 @@
 // scatter, ghost exchange and owner lookup of the reference are not needed on
 // one GPU: the periodic wrap is applied while each CTA stages its footprint
 // box in shared memory (sl_tile.cuh).
-#include <mutex>
-
+//
+// Every time step is one gather with a pointwise epilogue: the adjoint step's
+// right-hand side collapses to a per-point factor (launch_adjoint_coef), the
+// incremental state's sources are formed for all steps in one streaming pass
+// (launch_incstate_source), and the body force is summed once over the stored
+// adjoint levels (launch_body_force) instead of being accumulated step by step.
 #include "sl_tile.cuh"
 
 namespace cb {
 
 constexpr int kSlThreads = 256;
 
-static dim3 point_grid(long long n, int nprob) {
-  return dim3((unsigned)((n + kSlThreads - 1) / kSlThreads), nprob);
-}
-
-// Persistent grid: two CTAs per SM (each holds two 48 KB boxes), capped by
-// the number of tiles.
-static dim3 persist_grid(const Dims& d, int nprob, int nz) {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  const unsigned nt = tile_count(d);
-  const unsigned cap = (unsigned)(kPersistCtasPerSm * sms);
-  return dim3(nt < cap ? nt : cap, nprob, nz);
-}
+static dim3 tile_grid(const Dims& d, int nprob, int nz) { return dim3(tile_count(d), nprob, nz); }
 
 template <typename K>
-static int allow_gather_smem(K kernel) {
+static int allow_smem(K kernel) {
   return (int)cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGatherSmemBytes);
 }
 
@@ -48,227 +35,266 @@ static int allow_gather_smem(K kernel) {
 struct VelocitySource {
   const float* v;
   float c0, c1, c2;  // -sign*ht*N_k/(2 pi)
-  CB_DEVICE void points(TilePoint (&pts)[kTX1], const TileRow& row, const Dims& d) const {
-    const long long n = d.n();
+  CB_DEVICE void load(float (&dd)[kTilePts][3], const TileThread& tt, const Dims& d) const {
+    const float* v2 = v + d.n();
+    const float* v3 = v2 + d.n();
 #pragma unroll
-    for (int a = 0; a < kTX1; ++a) {
-      if (!row.valid(a, d)) {
-        pts[a] = TilePoint{{0, 0, 0}, {0.f, 0.f, 0.f}};
-        continue;
-      }
-      const long long i = row.idx(a);
-      set_point(pts[a], row.t1 + a, row.i2, row.i3, c0 * __ldg(v + i), c1 * __ldg(v + n + i),
-                c2 * __ldg(v + 2 * n + i));
+    for (int a = 0; a < kTilePts; ++a) {
+      const bool ok = tt.valid_idx(a);
+      const unsigned i = tt.idx(a);
+      dd[a][0] = ok ? c0 * __ldg(v + i) : 0.f;
+      dd[a][1] = ok ? c1 * __ldg(v2 + i) : 0.f;
+      dd[a][2] = ok ? c2 * __ldg(v3 + i) : 0.f;
     }
   }
 };
 
-// X = x - sign*(ht/2)*(v + v(Xt)) as a displacement.
+// Component k of X = x - sign*(ht/2)*(v + v(X~)) as a displacement:
+// disp_k = h_k (v_k + v_k(X~)), h_k = -sign*(ht/2)*N_k/(2 pi).
 struct TrajectoryEpi {
-  const float* v;
-  float* disp;
-  float h0, h1, h2;  // -sign*(ht/2)*N_k/(2 pi)
-  Dims d;
-  CB_DEVICE void operator()(const TileRow& row, const float (&vx)[3][kTX1]) const {
-    const long long n = d.n();
-#pragma unroll
-    for (int a = 0; a < kTX1; ++a) {
-      if (!row.valid(a, d)) continue;
-      const long long i = row.idx(a);
-      disp[i] = h0 * (__ldg(v + i) + vx[0][a]);
-      disp[n + i] = h1 * (__ldg(v + n + i) + vx[1][a]);
-      disp[2 * n + i] = h2 * (__ldg(v + 2 * n + i) + vx[2][a]);
-    }
+  const float* vk;
+  float* dk;
+  float h;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float vx) const {
+    if (tt.valid_idx(a)) dk[tt.idx(a)] = h * (__ldg(vk + tt.idx(a)) + vx);
   }
 };
 
-template <int NF>
 struct StoreEpi {
   float* dst;
-  long long of;
-  Dims d;
-  CB_DEVICE void operator()(const TileRow& row, const float (&vals)[NF][kTX1]) const {
-#pragma unroll
-    for (int k = 0; k < NF; ++k)
-#pragma unroll
-      for (int a = 0; a < kTX1; ++a)
-        if (row.valid(a, d)) dst[k * of + row.idx(a)] = vals[k][a];
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
+    if (tt.valid_idx(a)) dst[tt.idx(a)] = val;
   }
 };
 
-// lam_out = lx + ht/2 (rhs0 + rhs1), rhs0 = lx*divvx, rhs1 = (lx + ht*rhs0)*divv;
-// b += w * g * lam_in  (src/CLAIRE.cpp:2646-2686, 3940-3971)
-struct AdjointEpi {
-  const float *lam_in, *divv, *divvx, *g;
-  float *lam_out, *b;
-  float ht, w;
-  Dims d;
-  CB_DEVICE void operator()(const TileRow& row, const float (&lx)[1][kTX1]) const {
-    const long long n = d.n();
-#pragma unroll
-    for (int a = 0; a < kTX1; ++a) {
-      if (!row.valid(a, d)) continue;
-      const long long i = row.idx(a);
-      const float lam = __ldg(lam_in + i);
-      const float rhs0 = lx[0][a] * __ldg(divvx + i);
-      const float rhs1 = (lx[0][a] + ht * rhs0) * __ldg(divv + i);
-      b[i] += w * __ldg(g + i) * lam;
-      b[n + i] += w * __ldg(g + n + i) * lam;
-      b[2 * n + i] += w * __ldg(g + 2 * n + i) * lam;
-      lam_out[i] = lx[0][a] + 0.5f * ht * (rhs0 + rhs1);
-    }
+// out = c * val
+struct ScaleEpi {
+  const float* c;
+  float* out;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
+    if (tt.valid_idx(a)) out[tt.idx(a)] = __ldg(c + tt.idx(a)) * val;
   }
 };
 
-// mt_out = mt_in(X) - ht/2 (gx . vtx) - ht/2 (g1 . vt)  (src/CLAIRE.cpp:3220-3276)
-struct IncStateEpi {
-  const float *gx, *vtx, *g1, *vt;
-  float* mt_out;
+// out = sign * (val + src)
+struct AddEpi {
+  const float* src;
+  float* out;
+  float sign;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
+    if (tt.valid_idx(a)) out[tt.idx(a)] = sign * (val + __ldg(src + tt.idx(a)));
+  }
+};
+
+// out = 1 + ht/2 (dx + dv + ht dx dv), dx = divv(X) (the gathered value), dv = divv
+struct AdjCoefEpi {
+  const float* divv;
+  float* out;
   float ht;
-  Dims d;
-  CB_DEVICE void operator()(const TileRow& row, const float (&mx)[1][kTX1]) const {
-    const long long n = d.n();
-    const float hh = 0.5f * ht;
-#pragma unroll
-    for (int a = 0; a < kTX1; ++a) {
-      if (!row.valid(a, d)) continue;
-      const long long i = row.idx(a);
-      float m = mx[0][a];
-      m -= hh * (__ldg(gx + i) * __ldg(vtx + i) + __ldg(gx + n + i) * __ldg(vtx + n + i) +
-                 __ldg(gx + 2 * n + i) * __ldg(vtx + 2 * n + i));
-      m -= hh * (__ldg(g1 + i) * __ldg(vt + i) + __ldg(g1 + n + i) * __ldg(vt + n + i) +
-                 __ldg(g1 + 2 * n + i) * __ldg(vt + 2 * n + i));
-      mt_out[i] = m;
-    }
+  CB_DEVICE void operator()(const TileThread& tt, int a, float dx) const {
+    if (!tt.valid_idx(a)) return;
+    const float dv = __ldg(divv + tt.idx(a));
+    out[tt.idx(a)] = 1.f + 0.5f * ht * (dx + dv + ht * dx * dv);
   }
 };
 
-// ---- kernels ----------------------------------------------------------------
+// ---- gather kernels (grid: tiles x problems x fields) -------------------------
 
-__global__ void __launch_bounds__(kTileThreads, kPersistCtasPerSm)
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_trajectory(const float* __restrict__ v, long long vp, float* __restrict__ disp, long long dp, Dims d,
                  float ht, float sign, const int* __restrict__ active) {
-  const int p = blockIdx.y;
+  const int p = blockIdx.y, k = blockIdx.z;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
   const float* v1 = v + p * vp;
   const float c0 = (float)(d.n1 / kTwoPi), c1 = (float)(d.n2 / kTwoPi), c2 = (float)(d.n3 / kTwoPi);
   VelocitySource src{v1, -sign * ht * c0, -sign * ht * c1, -sign * ht * c2};
-  const float hh = 0.5f * ht;
-  TrajectoryEpi epi{v1, disp + p * dp, -sign * hh * c0, -sign * hh * c1, -sign * hh * c2, d};
-  pipelined_gather<3>(sbuf, src, v1, d.n(), d, epi);
+  const float ck = k == 0 ? c0 : (k == 1 ? c1 : c2);
+  const float* vk = v1 + k * d.n();
+  TrajectoryEpi epi{vk, disp + p * dp + k * d.n(), -sign * 0.5f * ht * ck};
+  tile_gather(sbuf, src, vk, d, epi);
 }
 
-// NF fields (1 or 3) gathered at one characteristic; grid.z runs over groups
-// of NF fields (group g: fields g*NF .. g*NF+NF-1).
-template <int NF>
-__global__ void __launch_bounds__(kTileThreads, kPersistCtasPerSm)
+// field z of f (ff apart) -> field z of out (of apart)
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_interp(const float* __restrict__ f, long long fp, long long ff, const float* __restrict__ disp, long long dp,
              float* __restrict__ out, long long op, long long of, Dims d, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
   DispSource src{disp + p * dp};
-  StoreEpi<NF> epi{out + p * op + (long long)blockIdx.z * NF * of, of, d};
-  pipelined_gather<NF>(sbuf, src, f + p * fp + (long long)blockIdx.z * NF * ff, ff, d, epi);
+  StoreEpi epi{out + p * op + (long long)blockIdx.z * of};
+  tile_gather(sbuf, src, f + p * fp + (long long)blockIdx.z * ff, d, epi);
 }
 
-__global__ void __launch_bounds__(kTileThreads, kPersistCtasPerSm) k_adjoint_step(
-    const float* __restrict__ lam_in, float* __restrict__ lam_out, long long lp,
-    const float* __restrict__ disp, long long dp, const float* __restrict__ divv,
-    const float* __restrict__ divvx, long long vp, const float* __restrict__ g, long long gp,
-    float* __restrict__ b, long long bp, float ht, float w, Dims d, const int* __restrict__ active) {
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
+    k_gather_scale(const float* __restrict__ f, long long fp, const float* __restrict__ disp, long long dp,
+                   const float* __restrict__ c, long long cp, float* __restrict__ out, long long op, Dims d,
+                   const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
   DispSource src{disp + p * dp};
-  AdjointEpi epi{lam_in + p * lp, divv + p * vp, divvx + p * vp, g + p * gp, lam_out + p * lp, b + p * bp, ht, w, d};
-  pipelined_gather<1>(sbuf, src, lam_in + p * lp, 0, d, epi);
+  ScaleEpi epi{c + p * cp, out + p * op};
+  tile_gather(sbuf, src, f + p * fp, d, epi);
 }
 
-__global__ void k_body_force_final(float* __restrict__ b, long long bp, const float* __restrict__ g,
-                                   long long gp, const float* __restrict__ lam, long long lp, float w,
-                                   float hd, long long n, const int* __restrict__ active) {
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
+    k_gather_add(const float* __restrict__ f, long long fp, const float* __restrict__ disp, long long dp,
+                 const float* __restrict__ s, long long sp, float* __restrict__ out, long long op, float sign,
+                 Dims d, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  extern __shared__ __align__(16) float sbuf[];
+  DispSource src{disp + p * dp};
+  AddEpi epi{s + p * sp, out + p * op, sign};
+  tile_gather(sbuf, src, f + p * fp, d, epi);
+}
+
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
+    k_adjoint_coef(const float* __restrict__ divv, long long vp, const float* __restrict__ disp, long long dp,
+                   float* __restrict__ out, long long op, float ht, Dims d, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  extern __shared__ __align__(16) float sbuf[];
+  DispSource src{disp + p * dp};
+  AdjCoefEpi epi{divv + p * vp, out + p * op, ht};
+  tile_gather(sbuf, src, divv + p * vp, d, epi);
+}
+
+// ---- pointwise kernels (4 consecutive points per thread, float4) ---------------
+
+__global__ void k_body_force(const float* __restrict__ lam, long long lp, const float* __restrict__ gm, long long gp,
+                             float* __restrict__ b, long long bp, int nt, float ht, float scale, long long n,
+                             const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const long long i = 4 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
   if (i >= n) return;
-  const float l = lam[p * lp + i];
+  const float* L = lam + p * lp;
+  const float* G = gm + p * gp;
+  float4 acc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int l = 0; l <= nt; ++l) {
+    const float w = (l == 0 || l == nt) ? 0.5f * ht : ht;
+    const float4 lv = __ldg(reinterpret_cast<const float4*>(L + l * n + i));
+    const float4 wl = make_float4(w * lv.x, w * lv.y, w * lv.z, w * lv.w);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 g = __ldg(reinterpret_cast<const float4*>(G + (3 * l + k) * n + i));
+      acc[k].x += wl.x * g.x;
+      acc[k].y += wl.y * g.y;
+      acc[k].z += wl.z * g.z;
+      acc[k].w += wl.w * g.w;
+    }
+  }
   float* bb = b + p * bp;
-  const float* gg = g + p * gp;
-  bb[i] = hd * (bb[i] + w * gg[i] * l);
-  bb[n + i] = hd * (bb[n + i] + w * gg[n + i] * l);
-  bb[2 * n + i] = hd * (bb[2 * n + i] + w * gg[2 * n + i] * l);
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    *reinterpret_cast<float4*>(bb + k * n + i) =
+        make_float4(scale * acc[k].x, scale * acc[k].y, scale * acc[k].z, scale * acc[k].w);
 }
 
-__global__ void __launch_bounds__(kTileThreads, kPersistCtasPerSm) k_incstate_step(
-    const float* __restrict__ mt_in, float* __restrict__ mt_out, long long mp,
-    const float* __restrict__ disp, long long dp, const float* __restrict__ gx, long long gxp,
-    const float* __restrict__ vtx, const float* __restrict__ g1, long long g1p,
-    const float* __restrict__ vt, long long vtp, float ht, Dims d, const int* __restrict__ active) {
+__global__ void k_incstate_source(const float* __restrict__ gx, long long gxp, const float* __restrict__ vtx,
+                                  long long vtxp, const float* __restrict__ gm, long long gmp,
+                                  const float* __restrict__ vt, long long vtp, float* __restrict__ s, long long sp,
+                                  int nt, float ht, long long n, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
-  extern __shared__ __align__(16) float sbuf[];
-  DispSource src{disp + p * dp};
-  IncStateEpi epi{gx + p * gxp, vtx + p * vtp, g1 + p * g1p, vt + p * vtp, mt_out + p * mp, ht, d};
-  pipelined_gather<1>(sbuf, src, mt_in + p * mp, 0, d, epi);
+  const long long i = 4 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  if (i >= n) return;
+  float4 a[3], c[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    a[k] = __ldg(reinterpret_cast<const float4*>(vtx + p * vtxp + k * n + i));
+    c[k] = __ldg(reinterpret_cast<const float4*>(vt + p * vtp + k * n + i));
+  }
+  const float hh = -0.5f * ht;
+  const float* GX = gx + p * gxp;
+  const float* GM = gm + p * gmp;
+  float* S = s + p * sp;
+  for (int j = 0; j < nt; ++j) {
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f), u = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float4 x = __ldg(reinterpret_cast<const float4*>(GX + (3 * j + k) * n + i));
+      const float4 y = __ldg(reinterpret_cast<const float4*>(GM + (3 * (j + 1) + k) * n + i));
+      t.x += x.x * a[k].x; t.y += x.y * a[k].y; t.z += x.z * a[k].z; t.w += x.w * a[k].w;
+      u.x += y.x * c[k].x; u.y += y.y * c[k].y; u.z += y.z * c[k].z; u.w += y.w * c[k].w;
+    }
+    *reinterpret_cast<float4*>(S + j * n + i) =
+        make_float4(hh * (t.x + u.x), hh * (t.y + u.y), hh * (t.z + u.z), hh * (t.w + u.w));
+  }
 }
 
 // ---- launchers ---------------------------------------------------------------
 
 int launch_trajectory(const float* v, long long vp, float* disp, long long dp, int nprob,
                       const Dims& d, float ht, float sign, const int* active, cudaStream_t s) {
-  int e = allow_gather_smem(k_trajectory);
+  int e = allow_smem(k_trajectory);
   if (e) return e;
-  k_trajectory<<<persist_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(v, vp, disp, dp, d, ht, sign,
-                                                                                  active);
+  k_trajectory<<<tile_grid(d, nprob, 3), kTileThreads, kGatherSmemBytes, s>>>(v, vp, disp, dp, d, ht, sign, active);
   return (int)cudaGetLastError();
 }
 
 int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp,
                   float* out, long long op, long long of, int nf, int nprob, const Dims& d,
                   const int* active, cudaStream_t s) {
-  int e = 0;
-  if (nf % 3 == 0) {
-    e = allow_gather_smem(k_interp<3>);
-    if (e) return e;
-    k_interp<3><<<persist_grid(d, nprob, nf / 3), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, out,
-                                                                                       op, of, d, active);
-  } else {
-    e = allow_gather_smem(k_interp<1>);
-    if (e) return e;
-    k_interp<1><<<persist_grid(d, nprob, nf), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, out, op,
-                                                                                   of, d, active);
-  }
-  return (int)cudaGetLastError();
-}
-
-int launch_adjoint_step(const float* lam_in, float* lam_out, long long lp, const float* disp,
-                        long long dp, const float* divv, const float* divvx, long long vp,
-                        const float* g, long long gp, float* b, long long bp, float ht, float w,
-                        int nprob, const Dims& d, const int* active, cudaStream_t s) {
-  int e = allow_gather_smem(k_adjoint_step);
+  int e = allow_smem(k_interp);
   if (e) return e;
-  k_adjoint_step<<<persist_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(
-      lam_in, lam_out, lp, disp, dp, divv, divvx, vp, g, gp, b, bp, ht, w, d, active);
+  k_interp<<<tile_grid(d, nprob, nf), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, out, op, of, d,
+                                                                           active);
   return (int)cudaGetLastError();
 }
 
-int launch_body_force_final(float* b, long long bp, const float* g, long long gp, const float* lam,
-                            long long lp, float w, float hd_scale, int nprob, long long n,
-                            const int* active, cudaStream_t s) {
-  k_body_force_final<<<point_grid(n, nprob), kSlThreads, 0, s>>>(b, bp, g, gp, lam, lp, w, hd_scale, n, active);
-  return (int)cudaGetLastError();
-}
-
-int launch_incstate_step(const float* mt_in, float* mt_out, long long mp, const float* disp,
-                         long long dp, const float* gx, long long gxp, const float* vtx,
-                         const float* g1, long long g1p, const float* vt, long long vtp, float ht,
-                         int nprob, const Dims& d, const int* active, cudaStream_t s) {
-  int e = allow_gather_smem(k_incstate_step);
+int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const float* c,
+                        long long cp, float* out, long long op, int nprob, const Dims& d, const int* active,
+                        cudaStream_t s) {
+  int e = allow_smem(k_gather_scale);
   if (e) return e;
-  k_incstate_step<<<persist_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(
-      mt_in, mt_out, mp, disp, dp, gx, gxp, vtx, g1, g1p, vt, vtp, ht, d, active);
+  k_gather_scale<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, c, cp, out, op,
+                                                                                d, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const float* src,
+                      long long sp, float* out, long long op, float sign, int nprob, const Dims& d,
+                      const int* active, cudaStream_t s) {
+  int e = allow_smem(k_gather_add);
+  if (e) return e;
+  k_gather_add<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, src, sp, out, op,
+                                                                              sign, d, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, float* out,
+                        long long op, float ht, int nprob, const Dims& d, const int* active, cudaStream_t s) {
+  int e = allow_smem(k_adjoint_coef);
+  if (e) return e;
+  k_adjoint_coef<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(divv, vp, disp, dp, out, op, ht,
+                                                                                d, active);
+  return (int)cudaGetLastError();
+}
+
+static dim3 quad_grid(long long n, int nprob) {
+  const long long q = n / 4;
+  return dim3((unsigned)((q + kSlThreads - 1) / kSlThreads), nprob);
+}
+
+int launch_body_force(const float* lam, long long lp, const float* gm, long long gp, float* b, long long bp,
+                      int nt, float ht, float scale, int nprob, long long n, const int* active, cudaStream_t s) {
+  if (n % 4) return (int)cudaErrorInvalidValue;
+  k_body_force<<<quad_grid(n, nprob), kSlThreads, 0, s>>>(lam, lp, gm, gp, b, bp, nt, ht, scale, n, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_incstate_source(const float* gx, long long gxp, const float* vtx, long long vtxp, const float* gm,
+                           long long gmp, const float* vt, long long vtp, float* src, long long sp, int nt,
+                           float ht, int nprob, long long n, const int* active, cudaStream_t s) {
+  if (n % 4) return (int)cudaErrorInvalidValue;
+  k_incstate_source<<<quad_grid(n, nprob), kSlThreads, 0, s>>>(gx, gxp, vtx, vtxp, gm, gmp, vt, vtp, src, sp, nt,
+                                                               ht, n, active);
   return (int)cudaGetLastError();
 }
 

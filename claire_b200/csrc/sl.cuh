@@ -17,20 +17,23 @@ struct Stencil {
   float w1[4], w2[4], w3[4];
 };
 
+// The four weights at fraction s, each cubic in Horner form.
+CB_DEVICE void lagrange4(float s, float (&w)[4]) {
+  w[0] = s * fmaf(s, fmaf(s, -1.f / 6.f, 0.5f), -1.f / 3.f);
+  w[1] = fmaf(s, fmaf(s, fmaf(s, 0.5f, -1.f), -0.5f), 1.f);
+  w[2] = s * fmaf(s, fmaf(s, -0.5f, 0.5f), 1.f);
+  w[3] = s * fmaf(s * s, 1.f / 6.f, -1.f / 6.f);
+}
+
 CB_DEVICE void axis_stencil(int i, float disp, int n, int stride, int (&o)[4], float (&w)[4]) {
   const float fl = floorf(disp);
-  const float s = disp - fl;
   int b = wrap(i + (int)fl - 1, n);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     o[k] = b * stride;
     b = (b + 1 == n) ? 0 : b + 1;
   }
-  const float sm1 = s - 1.f, sm2 = s - 2.f, sp1 = s + 1.f;
-  w[0] = (-1.f / 6.f) * s * sm1 * sm2;
-  w[1] = 0.5f * sp1 * sm1 * sm2;
-  w[2] = -0.5f * sp1 * s * sm2;
-  w[3] = (1.f / 6.f) * sp1 * s * sm1;
+  lagrange4(disp - fl, w);
 }
 
 CB_DEVICE void make_stencil(int i1, int i2, int i3, float d1, float d2, float d3, const Dims& d,
@@ -82,26 +85,38 @@ int launch_interp(const float* f, long long fp, long long ff, const float* disp,
                   float* out, long long op, long long of, int nf, int nprob, const Dims& d,
                   const int* active, cudaStream_t s);
 
-// One backward RK2 step of the (incremental) adjoint with body-force update
-// (src/CLAIRE.cpp:2646-2686, 3940-3971):
-//   lx = lam_in(X); rhs0 = lx*divvx; rhs1 = (lx + ht*rhs0)*divv;
-//   b += w * g * lam_in;  lam_out = lx + ht/2 (rhs0 + rhs1)
-int launch_adjoint_step(const float* lam_in, float* lam_out, long long lp, const float* disp,
-                        long long dp, const float* divv, const float* divvx, long long vp,
-                        const float* g, long long gp, float* b, long long bp, float ht, float w,
-                        int nprob, const Dims& d, const int* active, cudaStream_t s);
+// out[p] = c[p] * f[p](i + disp[p](i)): one backward RK2 step of the
+// (incremental) adjoint, lambda^{l-1} = c * lambda^l(X) with the per-point
+// factor c of launch_adjoint_coef (src/CLAIRE.cpp:2646-2686, 3940-3971).
+int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const float* c,
+                        long long cp, float* out, long long op, int nprob, const Dims& d, const int* active,
+                        cudaStream_t s);
 
-// b = hd_scale * (b + w * g * lam)   (t = 0 trapezoid term, src/CLAIRE.cpp:2689-2709)
-int launch_body_force_final(float* b, long long bp, const float* g, long long gp, const float* lam,
-                            long long lp, float w, float hd_scale, int nprob, long long n,
-                            const int* active, cudaStream_t s);
+// out[p] = sign * (f[p](i + disp[p](i)) + src[p](i)): one incremental state
+// step m~^{j+1} = m~^j(X) + s_j (src/CLAIRE.cpp:3220-3276); sign -1 writes the
+// incremental adjoint's final condition -m~(t=1) (src/DistanceMeasureSL2.cpp:223-283).
+int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const float* src,
+                      long long sp, float* out, long long op, float sign, int nprob, const Dims& d,
+                      const int* active, cudaStream_t s);
 
-// One incremental state step (src/CLAIRE.cpp:3220-3276):
-//   mt_out = mt_in(X) - ht/2 * (gx . vtx) - ht/2 * (g1 . vt)
-int launch_incstate_step(const float* mt_in, float* mt_out, long long mp, const float* disp,
-                         long long dp, const float* gx, long long gxp, const float* vtx,
-                         const float* g1, long long g1p, const float* vt, long long vtp, float ht,
-                         int nprob, const Dims& d, const int* active, cudaStream_t s);
+// RK2 adjoint step factor: with dx = divv(X) and dv = divv,
+//   lx + ht/2 (rhs0 + rhs1), rhs0 = lx dx, rhs1 = (lx + ht rhs0) dv
+// equals lx * (1 + ht/2 (dx + dv + ht dx dv)); out = that factor.
+int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, float* out,
+                        long long op, float ht, int nprob, const Dims& d, const int* active, cudaStream_t s);
+
+// Trapezoid body force over the stored adjoint levels (src/CLAIRE.cpp:2646-2709):
+//   b[k] = scale * sum_l w_l lam^l (d/dx_k m^l),  w_0 = w_nt = ht/2, else ht.
+// lam holds nt+1 levels (n apart), gm nt+1 levels of 3 fields (3n apart).
+int launch_body_force(const float* lam, long long lp, const float* gm, long long gp, float* b, long long bp,
+                      int nt, float ht, float scale, int nprob, long long n, const int* active, cudaStream_t s);
+
+// Incremental state sources (src/CLAIRE.cpp:3220-3276), j < nt:
+//   s_j = -ht/2 ((grad m^j)(X) . v~(X) + grad m^{j+1} . v~)
+// gx: nt levels of 3 fields, gm: nt+1 levels of 3 fields, s: nt levels.
+int launch_incstate_source(const float* gx, long long gxp, const float* vtx, long long vtxp, const float* gm,
+                           long long gmp, const float* vt, long long vtp, float* src, long long sp, int nt,
+                           float ht, int nprob, long long n, const int* active, cudaStream_t s);
 
 int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
                    const float* b, long long bp, const double* cb, double sb, long long len,

@@ -97,8 +97,8 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 // allocation
 // ---------------------------------------------------------------------------
 Solver::~Solver() {
-  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, gm, gx, divv, divvx, lam, lam2, bf, g, x,
-                  r, z, pv, q, vtx, mt, mt2, work3, spec, partials, dsc, dact, dint, dparams};
+  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, gm, gx, divv, cadj, lamh, bf, g, x,
+                  r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (hsc) cudaFreeHost(hsc);
@@ -134,7 +134,9 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   floats += 2 * 3 * n;                // trajectories
   floats += (nt + 1) * 3 * n;         // grad m cache
   floats += nt * 3 * n;               // grad m (X) cache
-  floats += 2 * n + 2 * n + 2 * n;    // divv, divvx, lam x2, mt x2
+  floats += 2 * n + 2 * n;            // divv, adjoint step factor, incremental state x2
+  floats += (nt + 1) * n;             // adjoint levels
+  floats += nt * n;                   // incremental state sources
   floats += 3 * n * 9;                // bf, g, x, r, z, p, q, vtx, work3
   long long bytes = floats * 4 + 3 * nc * 8;
   bytes += (long long)max_parts(d) * 8;
@@ -174,11 +176,11 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   CB_TRY(alloc((void**)&gm, V * (nt + 1)));
   CB_TRY(alloc((void**)&gx, V * nt));
   CB_TRY(alloc((void**)&divv, S));
-  CB_TRY(alloc((void**)&divvx, S));
-  CB_TRY(alloc((void**)&lam, S));
-  CB_TRY(alloc((void**)&lam2, S));
+  CB_TRY(alloc((void**)&cadj, S));
+  CB_TRY(alloc((void**)&lamh, S * (nt + 1)));
   CB_TRY(alloc((void**)&mt, S));
   CB_TRY(alloc((void**)&mt2, S));
+  CB_TRY(alloc((void**)&sj, S * nt));
   CB_TRY(alloc((void**)&bf, V));
   CB_TRY(alloc((void**)&g, V));
   CB_TRY(alloc((void**)&x, V));
@@ -417,22 +419,21 @@ int Solver::divergence(const float* vel, float* out, const int* act) {
   return 0;
 }
 
-// Backward RK2 sweep with trapezoid body force (src/CLAIRE.cpp:2646-2709,
-// 3940-3999), projection (src/CLAIRE.cpp:2338) and the hd scaling (:2341).
-// On entry `lam` holds lambda(t=1); on exit lambda(t=0) is in `lam`.
+// Backward RK2 sweep (src/CLAIRE.cpp:2646-2686, 3940-3971) over the stored
+// adjoint levels, then the trapezoid body force (:2689-2709), the projection
+// (src/CLAIRE.cpp:2338) and the hd scaling (:2341).  On entry level nt of
+// `lamh` holds lambda(t=1); on exit every level 0..nt is filled.  With
+// add_reg (no projection), bout receives the body force and is then expected
+// to be completed by an accumulating regularisation pass.
 int Solver::adjoint_sweep(float* bout, const int* act) {
-  const long long PGM = (nt + 1) * 3 * n;
-  cudaMemsetAsync(bout, 0, sizeof(float) * 3 * n * B, stream);
-  float* cur = lam;
-  float* nxt = lam2;
+  const long long PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
   for (int j = 0; j < nt; ++j) {
-    const float w = (j == 0) ? 0.5f * ht : ht;
-    CB_TRY(launch_adjoint_step(cur, nxt, n, disp_adj, 3 * n, divv, divvx, n, gm + (nt - j) * 3 * n, PGM, bout,
-                               3 * n, ht, w, B, d, act, stream));
-    std::swap(cur, nxt);
+    const int l = nt - j;  // lambda^{l-1} = c * lambda^l(X_adj)
+    CB_TRY(launch_gather_scale(lamh + l * n, PL, disp_adj, 3 * n, cadj, n, lamh + (l - 1) * n, PL, B, d, act,
+                               stream));
   }
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
-  CB_TRY(launch_body_force_final(bout, 3 * n, gm, PGM, cur, n, 0.5f * ht, proj ? 1.f : hd, B, n, act, stream));
+  CB_TRY(launch_body_force(lamh, PL, gm, PGM, bout, 3 * n, nt, ht, proj ? 1.f : hd, B, n, act, stream));
   note_launches(nt + 1);
   if (proj) {
     CB_TRY(launch_r2c3d(bout, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
@@ -443,27 +444,37 @@ int Solver::adjoint_sweep(float* bout, const int* act) {
                           stream));
     note_launches(6);
   }
-  if (cur != lam) {
-    CB_TRY(launch_lincomb(lam, n, cur, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
-    note_launches(1);
+  return 0;
+}
+
+// out = Reg.EvaluateGradient(vin) + body force (src/CLAIRE.cpp:1356-1361,
+// 1015-1042).  Without a projection the body force is written into out first
+// and the regularisation's inverse transform accumulates into it.
+int Solver::finish_with_reg(const float* vin, float* out, const int* act) {
+  const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
+  if (!proj) {
+    CB_TRY(adjoint_sweep(out, act));
+    CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_ADD, act));
+    return 0;
   }
+  CB_TRY(adjoint_sweep(bf, act));
+  CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_STORE, act));
+  CB_TRY(launch_lincomb(out, 3 * n, out, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
+  note_launches(1);
   return 0;
 }
 
 // EvaluateGradient at v (src/CLAIRE.cpp:871-1042); the state must be valid for v.
 int Solver::gradient(const int* act) {
-  const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n;
+  const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
   CB_TRY(launch_trajectory(v, 3 * n, disp_adj, 3 * n, B, d, ht, -1.f, act, stream));
   CB_TRY(grad_fields(m, PM, n, gm, PGM, 3 * n, nt + 1, act));
   CB_TRY(divergence(v, divv, act));
-  CB_TRY(launch_interp(divv, n, n, disp_adj, 3 * n, divvx, n, n, 1, B, d, act, stream));
+  CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, cadj, n, ht, B, d, act, stream));
   // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222)
-  CB_TRY(launch_lincomb(lam, n, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
+  CB_TRY(launch_lincomb(lamh + nt * n, PL, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
   note_launches(3);
-  CB_TRY(adjoint_sweep(bf, act));
-  CB_TRY(reg_op(v, g, OP_REG_GRAD, EPI_STORE, act));
-  CB_TRY(launch_lincomb(g, 3 * n, g, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
-  note_launches(1);
+  CB_TRY(finish_with_reg(v, g, act));
   CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, act));
   return 0;
 }
@@ -476,25 +487,32 @@ int Solver::hessian_prep(const int* act) {
   return 0;
 }
 
-// GN Hessian matvec (src/CLAIRE.cpp:1311-1379, 3147-3290, 3307-3490, 3849-4012)
+// GN Hessian matvec (src/CLAIRE.cpp:1311-1379, 3147-3290, 3307-3490, 3849-4012).
+// m~^0 = 0, so m~^1 = s_0; steps j = 1 .. nt-1 gather; the last one writes
+// lambda~(t=1) = -m~(t=1) straight into the adjoint's level nt.
 int Solver::hessian(const float* vin, float* hout, const int* act) {
-  const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n;
+  const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n, PL = (nt + 1) * n, PS = nt * n;
   CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, vtx, 3 * n, n, 3, B, d, act, stream));
-  cudaMemsetAsync(mt, 0, sizeof(float) * n * B, stream);
-  float* cur = mt;
-  float* nxt = mt2;
-  for (int j = 0; j < nt; ++j) {
-    CB_TRY(launch_incstate_step(cur, nxt, n, disp_st, 3 * n, gx + j * 3 * n, PGX, vtx, gm + (j + 1) * 3 * n, PGM,
-                                vin, 3 * n, ht, B, d, act, stream));
-    std::swap(cur, nxt);
+  CB_TRY(launch_incstate_source(gx, PGX, vtx, 3 * n, gm, PGM, vin, 3 * n, sj, PS, nt, ht, B, n, act, stream));
+  note_launches(2);
+  float* lam_end = lamh + nt * n;
+  if (nt == 1) {
+    CB_TRY(launch_lincomb(lam_end, PL, sj, PS, nullptr, -1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+    note_launches(1);
   }
-  // lambda~(t=1) = -m~(t=1) (src/DistanceMeasureSL2.cpp:223-283)
-  CB_TRY(launch_lincomb(lam, n, cur, n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
-  note_launches(2 + nt);
-  CB_TRY(adjoint_sweep(bf, act));
-  CB_TRY(reg_op(vin, hout, OP_REG_GRAD, EPI_STORE, act));
-  CB_TRY(launch_lincomb(hout, 3 * n, hout, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
-  note_launches(1);
+  const float* cur = sj;  // m~^1 = s_0
+  long long cp = PS;
+  float* bufs[2] = {mt, mt2};
+  for (int j = 1; j < nt; ++j) {
+    const bool last = (j == nt - 1);
+    float* out = last ? lam_end : bufs[j & 1];
+    CB_TRY(launch_gather_add(cur, cp, disp_st, 3 * n, sj + j * n, PS, out, last ? PL : n, last ? -1.f : 1.f, B, d,
+                             act, stream));
+    cur = out;
+    cp = n;
+  }
+  note_launches(nt - 1);
+  CB_TRY(finish_with_reg(vin, hout, act));
   return 0;
 }
 

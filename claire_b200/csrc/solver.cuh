@@ -64,9 +64,9 @@ class Solver {
   // device state (see DESIGN.md for the layout)
   float *mR = nullptr, *mT = nullptr, *v = nullptr, *vtrial = nullptr, *m = nullptr;
   float *disp_st = nullptr, *disp_adj = nullptr, *gm = nullptr, *gx = nullptr;
-  float *divv = nullptr, *divvx = nullptr, *lam = nullptr, *lam2 = nullptr, *bf = nullptr;
+  float *divv = nullptr, *cadj = nullptr, *lamh = nullptr, *bf = nullptr;
   float *g = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *q = nullptr;
-  float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *work3 = nullptr;
+  float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *sj = nullptr, *work3 = nullptr;
   float2* spec = nullptr;
   double* partials = nullptr;
   int maxparts = 0;
@@ -103,6 +103,7 @@ class Solver {
                   long long ofs, int nf, const int* act);
   int divergence(const float* vel, float* out, const int* act);
   int adjoint_sweep(float* bout, const int* act);
+  int finish_with_reg(const float* vin, float* out, const int* act);
   int gradient(const int* act);
   int hessian_prep(const int* act);
   int hessian(const float* vin, float* hout, const int* act);

@@ -10,8 +10,8 @@
   semi-axes U[0.1,0.5] rad, uniform random rotation, intensity U[0.2,1]),
   smoothed with a 1-cell Gaussian (the library's spectral smoother) and
   clipped to [0,1]; velocity with Fourier modes 1 <= |k| <= 6 and complex
-  amplitude N(0,0.3)/|k|^2; mR = SL transport of mT by that velocity with
-  the library's own forward solver.
+  amplitude N(0,0.3)/|k|^2, scaled to RMS 0.3; mR = SL transport of mT by
+  that velocity with the library's own forward solver.
 
 Random draws use NumPy's PCG64 with seed 20261203 + 1000*config + problem; the
 fields are evaluated with torch on the GPU.
@@ -23,6 +23,11 @@ import math
 import numpy as np
 
 TWO_PI = 2.0 * math.pi
+
+
+# RMS of the random velocity over grid and components (band-limited field:
+# independent of the grid size)
+VELOCITY_RMS = 0.3
 
 
 def seed(config_index: int, problem_index: int) -> int:
@@ -123,15 +128,20 @@ def ellipsoid_template(n, params, device="cuda"):
     return torch.clamp(smoothed, 0.0, 1.0).contiguous()
 
 
-def random_velocity(n, coeffs, device="cuda"):
+def random_velocity(n, coeffs, device="cuda", rms=VELOCITY_RMS):
     """Real field from half-spectrum coefficients: each coefficient contributes
-    c e^{ik.x} + c.c. (Hermitian completion of the real inverse transform)."""
+    c e^{ik.x} + c.c. (Hermitian completion of the real inverse transform),
+    scaled to the given RMS over grid and components (``rms=None`` keeps the
+    raw sum of the ~520 modes per component, RMS ~1.4: a folding map)."""
     import torch
     comps = []
     for c in coeffs:
         ct = torch.from_numpy(c * (n ** 3)).to(device)
         comps.append(torch.fft.irfftn(ct, s=(n, n, n), dim=(0, 1, 2)))
-    return torch.stack(comps).float().contiguous()
+    v = torch.stack(comps)
+    if rms is not None:
+        v = v * (rms / torch.sqrt(torch.mean(v * v)))
+    return v.float().contiguous()
 
 
 def ellipsoid_problem(n, nt, config_index=1, problem_index=0, device="cuda"):

@@ -116,7 +116,8 @@ int claire_b200_gradient(claire_b200_ctx* ctx, int b, const float* v, float* g);
 int claire_b200_hessian_matvec(claire_b200_ctx* ctx, int b, const float* v, const float* vt, float* hvt);
 /* Preconditioner::MatVec (INVREG): P x = (beta A)^-1 x (src/Preconditioner.cpp:549-580). */
 int claire_b200_precond(claire_b200_ctx* ctx, int b, const float* x, float* px);
-/* Adjoint state lambda(t=0) and body force b from the last gradient evaluation. */
+/* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
+ * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);
 int claire_b200_synchronize(claire_b200_ctx* ctx);
 /* Run the context's work on the caller's stream from now on (NULL: the

@@ -822,10 +822,16 @@ def template_ellipsoids(shape, rng, count=40, dtype=np.float64):
     return np.clip(out, 0.0, 1.0).astype(dtype)
 
 
-def velocity_random(shape, rng, kmax=6, amp=0.3, dtype=np.float64):
+def velocity_random(shape, rng, kmax=6, amp=0.3, dtype=np.float64, rms=0.3):
     """Random smooth periodic velocity: per component, complex Fourier
     coefficients N(0, amp)/|k|^2 on 1 <= |k| <= kmax, Hermitian through the
-    real inverse FFT, Nyquist zero; coefficient c gives c*e^{ik.x} + c.c."""
+    real inverse FFT, Nyquist zero; coefficient c gives c*e^{ik.x} + c.c.
+
+    The ~520 modes per component sum to an RMS of ~1.4 (displacements of up
+    to a fifth of the domain per unit time, a folding map); the field is
+    scaled to the given RMS over grid and components (``rms=None`` keeps the
+    raw sum).  The field is band-limited, so the RMS and the scale factor do
+    not depend on the grid size."""
     n1, n2, n3 = shape
     # Nyquist indices keep their magnitude n/2 > kmax, so no Nyquist mode
     # (a +-1 checkerboard on the grid) enters the field
@@ -838,7 +844,10 @@ def velocity_random(shape, rng, kmax=6, amp=0.3, dtype=np.float64):
         c = np.where(mask, c / np.where(kk > 0, kk * kk, 1.0), 0.0)
         # the real inverse transform completes the half spectrum Hermitian-wise
         out.append(np.fft.irfftn(c * (n1 * n2 * n3), s=shape, axes=(0, 1, 2)))
-    return np.stack(out).astype(dtype)
+    v = np.stack(out)
+    if rms is not None:
+        v *= rms / np.sqrt(np.mean(v * v))
+    return v.astype(dtype)
 
 
 def synthetic_c1(n=64, dtype=np.float64, nt=4):
