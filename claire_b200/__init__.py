@@ -124,7 +124,12 @@ _signatures = {
     "claire_b200_smooth": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_kernel_launches": (ctypes.c_longlong, []),
+    "claire_b200_profile": (_I, [_P, _I]),
+    "claire_b200_profile_read": (_I, [_P, _I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
 }
+
+# device timer categories (claire_b200_profile_read)
+PROF_ADJOINT_STEP, PROF_INCSTATE_STEP, PROF_STATE_STEP = 0, 1, 2
 for _name, (_res, _args) in _signatures.items():
     _fn = getattr(lib, _name)
     _fn.restype = _res
@@ -342,6 +347,18 @@ class CLAIREInterface:
         _check(lib.claire_b200_forward(self._ctx, b, p, out.ctypes.data_as(ctypes.c_void_p), 0),
                "SolveForwardProblem", self._ctx)
         return out
+
+    def profile(self, enable: bool = True) -> None:
+        """Bracket every time-step kernel launch with CUDA events (instrumented runs)."""
+        _check(lib.claire_b200_profile(self._ctx, int(bool(enable))), "profile", self._ctx)
+
+    def profile_read(self, category: int):
+        """(device ms, launches) of a timer category since the last read; resets it."""
+        ms = ctypes.c_double(0.0)
+        cnt = ctypes.c_longlong(0)
+        _check(lib.claire_b200_profile_read(self._ctx, int(category), ctypes.byref(ms), ctypes.byref(cnt)),
+               "profile_read", self._ctx)
+        return float(ms.value), int(cnt.value)
 
     def stats(self, b: int = 0) -> dict:
         st = Stats()

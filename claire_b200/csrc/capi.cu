@@ -586,4 +586,20 @@ int claire_b200_distance(const float* mR, const float* m1, const int nx[3], doub
 
 long long claire_b200_kernel_launches(void) { return launches(); }
 
+int claire_b200_profile(claire_b200_ctx* c, int enable) {
+  if (!c) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  if (!enable) {
+    if (cudaStreamSynchronize(s.stream) != cudaSuccess) return CB_ERR_CUDA;
+    s.prof_clear();
+  }
+  s.prof_on = enable != 0;
+  return CB_OK;
+}
+
+int claire_b200_profile_read(claire_b200_ctx* c, int category, double* total_ms, long long* launches_out) {
+  if (!c || category < 0 || category >= CB_PROF_NCAT) return CB_ERR_ARG;
+  return c->solver.prof_read(category, total_ms, launches_out);
+}
+
 }  // extern "C"

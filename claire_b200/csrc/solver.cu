@@ -97,6 +97,7 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 // allocation
 // ---------------------------------------------------------------------------
 Solver::~Solver() {
+  prof_clear();
   void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, gm, gx, divv, cadj, lamh, bf, g, x,
                   r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
@@ -286,10 +287,46 @@ int Solver::state_solve(const float* vel, const int* act) {
   const long long PM = (nt + 1) * n;
   CB_TRY(launch_trajectory(vel, 3 * n, disp_st, 3 * n, B, d, ht, 1.f, act, stream));
   CB_TRY(launch_lincomb(m, PM, mT, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
-  for (int j = 0; j < nt; ++j)
+  for (int j = 0; j < nt; ++j) {
+    CB_TRY(prof_mark(CB_PROF_STATE_STEP));
     CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, m + (j + 1) * n, PM, n, 1, B, d, act, stream));
+    CB_TRY(prof_mark(CB_PROF_STATE_STEP));
+  }
   note_launches(2 + nt);
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// device timers
+// ---------------------------------------------------------------------------
+int Solver::prof_mark(int cat) {
+  if (!prof_on) return 0;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return CB_ERR_CUDA;
+  prof_ev[cat].push_back(e);
+  return cudaEventRecord(e, stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
+int Solver::prof_read(int cat, double* ms, long long* count) {
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return CB_ERR_CUDA;
+  double total = 0.0;
+  std::vector<cudaEvent_t>& ev = prof_ev[cat];
+  for (size_t i = 0; i + 1 < ev.size(); i += 2) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ev[i], ev[i + 1]) == cudaSuccess) total += t;
+  }
+  if (ms) *ms = total;
+  if (count) *count = (long long)(ev.size() / 2);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  ev.clear();
+  return 0;
+}
+
+void Solver::prof_clear() {
+  for (int c = 0; c < CB_PROF_NCAT; ++c) {
+    for (cudaEvent_t e : prof_ev[c]) cudaEventDestroy(e);
+    prof_ev[c].clear();
+  }
 }
 
 // D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)
@@ -429,8 +466,10 @@ int Solver::adjoint_sweep(float* bout, const int* act) {
   const long long PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
   for (int j = 0; j < nt; ++j) {
     const int l = nt - j;  // lambda^{l-1} = c * lambda^l(X_adj)
+    CB_TRY(prof_mark(CB_PROF_ADJOINT_STEP));
     CB_TRY(launch_gather_scale(lamh + l * n, PL, disp_adj, 3 * n, cadj, n, lamh + (l - 1) * n, PL, B, d, act,
                                stream));
+    CB_TRY(prof_mark(CB_PROF_ADJOINT_STEP));
   }
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
   CB_TRY(launch_body_force(lamh, PL, gm, PGM, bout, 3 * n, nt, ht, proj ? 1.f : hd, B, n, act, stream));
@@ -506,8 +545,10 @@ int Solver::hessian(const float* vin, float* hout, const int* act) {
   for (int j = 1; j < nt; ++j) {
     const bool last = (j == nt - 1);
     float* out = last ? lam_end : bufs[j & 1];
+    CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
     CB_TRY(launch_gather_add(cur, cp, disp_st, 3 * n, sj + j * n, PS, out, last ? PL : n, last ? -1.f : 1.f, B, d,
                              act, stream));
+    CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
     cur = out;
     cp = n;
   }

@@ -85,6 +85,13 @@ class Solver {
   // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
   std::vector<int> state_of;
 
+  // device timers per category (CB_PROF_*): event pairs recorded around launches
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_ev[CB_PROF_NCAT];
+  int prof_mark(int cat);  // records one event (call before and after a launch)
+  int prof_read(int cat, double* ms, long long* count);
+  void prof_clear();
+
  private:
   long long bytes_ = 0;
   int alloc(void** p, size_t bytes);

@@ -163,6 +163,19 @@ int claire_b200_distance(const float* mR, const float* m1, const int nx[3], doub
 /* Number of CUDA kernel launches issued by this library since load (all threads). */
 long long claire_b200_kernel_launches(void);
 
+/* Device timers of the solver's time-step kernels, the counterpart of the
+ * reference's per-phase timers and counters (include/RegOpt.hpp:183-202).
+ * While enabled, every launch of a category is bracketed by CUDA events on
+ * the context's stream (host overhead per launch: use for instrumented runs).
+ * claire_b200_profile_read synchronizes the stream, returns the summed device
+ * time and the launch count of a category since the last read, and resets it. */
+#define CB_PROF_ADJOINT_STEP 0  /* lambda^{l-1} = c * lambda^l(X): one per adjoint step */
+#define CB_PROF_INCSTATE_STEP 1 /* m~^{j+1} = m~^j(X) + s_j: one per incremental step */
+#define CB_PROF_STATE_STEP 2    /* m^{j+1} = m^j(X): one per state step */
+#define CB_PROF_NCAT 3
+int claire_b200_profile(claire_b200_ctx* ctx, int enable);
+int claire_b200_profile_read(claire_b200_ctx* ctx, int category, double* total_ms, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif
