@@ -25,7 +25,7 @@ from typing import Optional, Sequence
 __all__ = [
     "lib", "RegOpt", "CLAIREInterface", "SemiLagrangian", "Regularization", "DistanceMeasureSL2",
     "Preconditioner", "fft_grad", "fft_div", "leray", "smooth", "kernel_launches", "ClaireError",
-    "NORMS", "MODELS",
+    "NORMS", "MODELS", "Server",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -58,6 +58,11 @@ class Opts(ctypes.Structure):
         ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int),
     ]
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("slots_per_pool", ctypes.c_int),
+                ("idle_ms", ctypes.c_int), ("device", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -125,6 +130,14 @@ _signatures = {
     "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_kernel_launches": (ctypes.c_longlong, []),
     "claire_b200_profile": (_I, [_P, _I]),
+    "claire_b200_server_default_opts": (None, [_P]),
+    "claire_b200_server_create": (_I, [_P, ctypes.POINTER(_P)]),
+    "claire_b200_server_submit": (_I, [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_longlong)]),
+    "claire_b200_server_poll": (_I, [_P, ctypes.c_longlong, ctypes.POINTER(_I)]),
+    "claire_b200_server_wait": (_I, [_P, ctypes.c_longlong, _I, ctypes.POINTER(_I)]),
+    "claire_b200_server_result": (_I, [_P, ctypes.c_longlong, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "claire_b200_server_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I)]),
+    "claire_b200_server_destroy": (_I, [_P]),
     "claire_b200_profile_read": (_I, [_P, _I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
 }
 
@@ -525,3 +538,89 @@ def smooth(f, sigma=(1.0, 1.0, 1.0), out=None):
     arr = (ctypes.c_double * 3)(*sigma)
     _check(lib.claire_b200_smooth(_dev_ptr(f), _dev_ptr(out), _nx(f.shape), arr, _stream()), "smooth")
     return out
+
+
+# ---------------------------------------------------------------------------
+# serving: continuous batching of registrations (claire_b200_server_*)
+# ---------------------------------------------------------------------------
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """Registration server: requests of any supported grid / nt / norm / beta
+    are queued, admitted into solver slots at GN-iteration boundaries as slots
+    and HBM free up, and retired when their stopping test fires.  Images are
+    host arrays (NumPy float32 or CPU tensors); results are host arrays."""
+
+    def __init__(self, slots_per_pool: int = 4, hbm_budget_bytes: int = 0, idle_ms: int = 2000, device: int = 0):
+        o = ServerOpts()
+        lib.claire_b200_server_default_opts(ctypes.byref(o))
+        o.slots_per_pool = int(slots_per_pool)
+        o.hbm_budget_bytes = int(hbm_budget_bytes)
+        o.idle_ms = int(idle_ms)
+        o.device = int(device)
+        h = ctypes.c_void_p()
+        _check(lib.claire_b200_server_create(ctypes.byref(o), ctypes.byref(h)), "Server")
+        self._srv = h
+
+    @staticmethod
+    def _host(x):
+        import numpy as np
+        if hasattr(x, "detach"):
+            x = x.detach().cpu().numpy()
+        return np.ascontiguousarray(x, dtype=np.float32)
+
+    def submit(self, opt: "RegOpt", mR, mT) -> int:
+        a, b = self._host(mR), self._host(mT)
+        n = opt.opts.nx[0] * opt.opts.nx[1] * opt.opts.nx[2]
+        if a.size != n or b.size != n:
+            raise ValueError("image size does not match the options' grid")
+        rid = ctypes.c_longlong(0)
+        _check(lib.claire_b200_server_submit(self._srv, ctypes.byref(opt.opts), a.ctypes.data_as(ctypes.c_void_p),
+                                             b.ctypes.data_as(ctypes.c_void_p), ctypes.byref(rid)), "Server.submit")
+        self._shape = tuple(opt.opts.nx)
+        return int(rid.value)
+
+    def poll(self, rid: int) -> int:
+        st = ctypes.c_int(0)
+        _check(lib.claire_b200_server_poll(self._srv, rid, ctypes.byref(st)), "Server.poll")
+        return st.value
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> int:
+        st = ctypes.c_int(0)
+        _check(lib.claire_b200_server_wait(self._srv, rid, int(timeout_ms), ctypes.byref(st)), "Server.wait")
+        return st.value
+
+    def result(self, rid: int, shape):
+        """(velocity (3, *shape), stats dict, submit-to-done latency ms); releases the request."""
+        import numpy as np
+        v = np.empty((3,) + tuple(shape), dtype=np.float32)
+        st = Stats()
+        lat = ctypes.c_double(0.0)
+        _check(lib.claire_b200_server_result(self._srv, rid, v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st),
+                                             ctypes.byref(lat)), "Server.result")
+        return v, st.as_dict(), float(lat.value)
+
+    def info(self) -> dict:
+        pools, queued = ctypes.c_int(0), ctypes.c_int(0)
+        used = ctypes.c_longlong(0)
+        _check(lib.claire_b200_server_info(self._srv, ctypes.byref(pools), ctypes.byref(used), ctypes.byref(queued)),
+               "Server.info")
+        return {"pools": pools.value, "bytes_used": used.value, "queued": queued.value}
+
+    def close(self):
+        if getattr(self, "_srv", None):
+            lib.claire_b200_server_destroy(self._srv)
+            self._srv = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,434 @@
+// Registration server: continuous batching of independent registrations.
+//
+// A pool is one Solver with S problem slots for one (grid, nt, solver-wide
+// options) key, its own CUDA stream and its own host worker thread.  Requests
+// are queued on submit; a pool's worker admits queued requests of its key
+// into free slots at every GN-iteration boundary (Solver::begin), advances all
+// running slots by one GN iteration per Solver::step, and retires the slots
+// whose stopping test fired (Solver::finish), copying the velocity out and
+// freeing the slot for the next request.  Pools of different keys run
+// concurrently on their own streams, so the work of requests of different
+// sizes overlaps on the device.  Pools are created while their footprint
+// (Solver::estimate_bytes) fits the HBM budget and release their memory after
+// idling, which lets queued requests of another key get a pool.
+//
+// The reference has no serving layer: each registration there is one
+// CLAIREInterface::Run call (src/CLAIREInterface.cpp:709-885); the results of
+// a request here are those of that call on the same inputs (the slots of a
+// pool never mix data: every kernel and every reduction is per problem).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace cb {
+namespace srv {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  long long id = 0;
+  claire_b200_opts opts{};
+  std::vector<float> mR, mT;  // host copies of the inputs
+  std::vector<float> v;       // result velocity (host)
+  claire_b200_stats stats{};
+  int status = CB_REQ_QUEUED;
+  int error = CB_OK;
+  Clock::time_point t_submit{}, t_done{};
+};
+
+// Options that must agree for problems to share a pool (everything but the
+// per-slot regularisation norm and weights).
+static bool same_pool(const claire_b200_opts& a, const claire_b200_opts& b) {
+  return a.nx[0] == b.nx[0] && a.nx[1] == b.nx[1] && a.nx[2] == b.nx[2] && a.nt == b.nt && a.model == b.model &&
+         a.maxit == b.maxit && a.opttol == b.opttol && a.gatol == b.gatol && a.krylovmaxit == b.krylovmaxit &&
+         a.krylovtol[0] == b.krylovtol[0] && a.krylovtol[1] == b.krylovtol[1] &&
+         a.krylovtol[2] == b.krylovtol[2] && a.krylovfseq == b.krylovfseq && a.precond == b.precond &&
+         a.iporder == b.iporder;
+}
+
+struct Pool;
+
+}  // namespace srv
+}  // namespace cb
+
+struct claire_b200_server {
+  claire_b200_server_opts opts{};
+  std::mutex mu;
+  std::condition_variable cv;          // request state changes, new work
+  std::deque<long long> queue;         // queued request ids, FIFO
+  std::map<long long, cb::srv::Request> reqs;
+  std::vector<std::unique_ptr<cb::srv::Pool>> pools;
+  long long budget = 0, used = 0;
+  long long next_id = 1;
+  bool stop = false;
+};
+
+namespace cb {
+namespace srv {
+
+struct Pool {
+  claire_b200_opts key{};
+  Solver solver;
+  std::vector<long long> slot_req;  // request id per slot, 0 = free
+  long long bytes = 0;
+  bool dead = false;  // worker has exited (memory released)
+  std::thread worker;
+};
+
+static long long pending_for(const claire_b200_server* s, const claire_b200_opts& key) {
+  long long k = 0;
+  for (long long id : s->queue)
+    if (same_pool(s->reqs.at(id).opts, key)) ++k;
+  return k;
+}
+
+static Pool* find_pool(claire_b200_server* s, const claire_b200_opts& key) {
+  for (auto& p : s->pools)
+    if (!p->dead && same_pool(p->key, key)) return p.get();
+  return nullptr;
+}
+
+static void fail_request(claire_b200_server* s, long long id, int err) {
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return;
+  it->second.status = CB_REQ_FAILED;
+  it->second.error = err;
+  it->second.t_done = Clock::now();
+}
+
+static void worker_main(claire_b200_server* s, Pool* p);
+
+// Create pools for queued keys that have none while the budget allows.
+// Caller holds s->mu.
+static void create_pools_locked(claire_b200_server* s) {
+  for (long long id : std::vector<long long>(s->queue.begin(), s->queue.end())) {
+    Request& r = s->reqs.at(id);
+    if (find_pool(s, r.opts)) continue;
+    const int slots = std::max(1, s->opts.slots_per_pool);
+    const long long need = Solver::estimate_bytes(r.opts, slots);
+    if (s->used + need > s->budget) continue;  // stays queued until memory frees up
+    auto pool = std::make_unique<Pool>();
+    pool->key = r.opts;
+    pool->key.verbosity = 0;
+    int caller_dev = 0;
+    cudaGetDevice(&caller_dev);
+    cudaSetDevice(s->opts.device);
+    const int e = pool->solver.init(pool->key, slots);
+    cudaSetDevice(caller_dev);
+    if (e) {
+      // this key cannot be served at all (unsupported grid, allocation failure)
+      for (long long q : std::vector<long long>(s->queue.begin(), s->queue.end()))
+        if (same_pool(s->reqs.at(q).opts, r.opts)) {
+          fail_request(s, q, e < 0 ? e : CB_ERR_CUDA);
+          s->queue.erase(std::find(s->queue.begin(), s->queue.end(), q));
+        }
+      s->cv.notify_all();
+      continue;
+    }
+    pool->bytes = pool->solver.footprint();
+    pool->slot_req.assign(slots, 0);
+    s->used += pool->bytes;
+    Pool* raw = pool.get();
+    s->pools.push_back(std::move(pool));
+    raw->worker = std::thread(worker_main, s, raw);
+  }
+}
+
+// Admit queued requests of the pool's key into free slots (caller holds mu).
+static std::vector<std::pair<int, long long>> admit_locked(claire_b200_server* s, Pool* p) {
+  std::vector<std::pair<int, long long>> out;
+  for (auto it = s->queue.begin(); it != s->queue.end();) {
+    const Request& r = s->reqs.at(*it);
+    if (!same_pool(r.opts, p->key)) {
+      ++it;
+      continue;
+    }
+    int slot = -1;
+    for (int b = 0; b < (int)p->slot_req.size(); ++b)
+      if (p->slot_req[b] == 0) {
+        bool taken = false;
+        for (auto& a : out) taken |= a.first == b;
+        if (!taken) {
+          slot = b;
+          break;
+        }
+      }
+    if (slot < 0) break;
+    out.push_back({slot, *it});
+    it = s->queue.erase(it);
+  }
+  for (auto& a : out) {
+    p->slot_req[a.first] = a.second;
+    s->reqs.at(a.second).status = CB_REQ_RUNNING;
+  }
+  return out;
+}
+
+static int load_slot(Solver& sv, int b, const Request& r) {
+  const long long n = sv.n;
+  if (cudaMemcpyAsync(sv.mR + b * n, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(sv.mT + b * n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+          cudaSuccess ||
+      cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess)
+    return CB_ERR_CUDA;
+  sv.state_of[b] = 0;
+  return sv.set_problem(b, r.opts);  // per-slot norm and weights (synchronises the stream)
+}
+
+static void fill_stats(const ProbState& ps, claire_b200_stats* st) {
+  std::memset(st, 0, sizeof(*st));
+  st->gn_iterations = ps.iter;
+  st->pcg_iterations = ps.pcg_total;
+  st->obj_evals = ps.obj_evals;
+  st->grad_evals = ps.grad_evals;
+  st->hess_matvecs = ps.hess_matvecs;
+  st->pc_matvecs = ps.pc_matvecs;
+  st->pde_solves = ps.pde_solves;
+  st->converged_reason = ps.reason;
+  st->J = ps.J;
+  st->J0 = ps.J0;
+  st->D = ps.D;
+  st->D0 = ps.D0;
+  st->R = ps.R;
+  st->gnorm = ps.gnorm;
+  st->gnorm0 = ps.gnorm0;
+  st->rel_mismatch = ps.rel_mismatch;
+  st->seconds = ps.seconds;
+}
+
+static void worker_main(claire_b200_server* s, Pool* p) {
+  cudaSetDevice(s->opts.device);
+  Solver& sv = p->solver;
+  const int S = sv.B;
+  int err = CB_OK;
+  while (true) {
+    std::vector<std::pair<int, long long>> admits;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->stop) break;
+      admits = admit_locked(s, p);
+      bool busy = !admits.empty();
+      for (int b = 0; b < S; ++b) busy |= p->slot_req[b] != 0;
+      if (!busy) {
+        const bool got = s->cv.wait_for(lk, std::chrono::milliseconds(std::max(1, s->opts.idle_ms)), [&] {
+          return s->stop || pending_for(s, p->key) > 0;
+        });
+        if (s->stop) break;
+        if (!got) break;  // idle: release the pool
+        continue;
+      }
+    }
+    // admission: inputs into the slots, then InitializeOptimization for them
+    std::vector<int> sel_new(S, 0);
+    for (auto& a : admits) {
+      Request* r;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r = &s->reqs.at(a.second);
+      }
+      err = load_slot(sv, a.first, *r);
+      if (err) break;
+      sel_new[a.first] = 1;
+    }
+    if (!err && !admits.empty()) err = sv.begin(sel_new);
+    std::vector<int> fin(S, 0);
+    if (!err) err = sv.step(fin);
+    // retire every slot whose GN loop has stopped
+    std::vector<int> done(S, 0);
+    bool anydone = false;
+    if (!err)
+      for (int b = 0; b < S; ++b)
+        if (p->slot_req[b] && sv.ps[b].running && sv.ps[b].done) {
+          done[b] = 1;
+          anydone = true;
+        }
+    if (!err && anydone) err = sv.finish(done);
+    if (err) break;
+    if (anydone) {
+      std::vector<std::pair<int, std::vector<float>>> outv;
+      for (int b = 0; b < S; ++b) {
+        if (!done[b]) continue;
+        std::vector<float> vh((size_t)(3 * sv.n));
+        if (cudaMemcpyAsync(vh.data(), sv.v + b * 3 * sv.n, sizeof(float) * 3 * sv.n, cudaMemcpyDeviceToHost,
+                            sv.stream) != cudaSuccess ||
+            cudaStreamSynchronize(sv.stream) != cudaSuccess) {
+          err = CB_ERR_CUDA;
+          break;
+        }
+        outv.push_back({b, std::move(vh)});
+      }
+      if (err) break;
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (auto& o : outv) {
+        const int b = o.first;
+        Request& r = s->reqs.at(p->slot_req[b]);
+        r.v = std::move(o.second);
+        fill_stats(sv.ps[b], &r.stats);
+        r.status = CB_REQ_DONE;
+        r.t_done = Clock::now();
+        p->slot_req[b] = 0;
+      }
+      s->cv.notify_all();
+    }
+  }
+  // exit: fail what this pool still holds, release the memory, let queued
+  // requests of other keys get a pool
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int b = 0; b < S; ++b)
+      if (p->slot_req[b]) fail_request(s, p->slot_req[b], err ? err : CB_ERR_STATE);
+    p->dead = true;
+  }
+  sv.~Solver();
+  new (&sv) Solver();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->used -= p->bytes;
+    p->bytes = 0;
+    if (!s->stop) create_pools_locked(s);
+    s->cv.notify_all();
+  }
+}
+
+}  // namespace srv
+}  // namespace cb
+
+using cb::srv::Clock;
+
+extern "C" {
+
+void claire_b200_server_default_opts(claire_b200_server_opts* o) {
+  if (!o) return;
+  o->hbm_budget_bytes = 0;
+  o->slots_per_pool = 4;
+  o->idle_ms = 2000;
+  o->device = 0;
+}
+
+int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_server** out) {
+  if (!o || !out || o->slots_per_pool < 1 || o->slots_per_pool > 1024) return CB_ERR_ARG;
+  *out = nullptr;
+  auto* s = new (std::nothrow) claire_b200_server();
+  if (!s) return CB_ERR_ALLOC;
+  s->opts = *o;
+  if (cudaSetDevice(o->device) != cudaSuccess) {
+    delete s;
+    return CB_ERR_CUDA;
+  }
+  size_t freeb = 0, total = 0;
+  if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+    delete s;
+    return CB_ERR_CUDA;
+  }
+  s->budget = o->hbm_budget_bytes > 0 ? o->hbm_budget_bytes : (long long)(0.9 * (double)freeb);
+  *out = s;
+  return CB_OK;
+}
+
+int claire_b200_server_submit(claire_b200_server* s, const claire_b200_opts* o, const float* mR, const float* mT,
+                              long long* id) {
+  if (!s || !o || !mR || !mT || !id) return CB_ERR_ARG;
+  if (o->nx[0] <= 0 || o->nx[1] <= 0 || o->nx[2] <= 0 || o->nt < 1) return CB_ERR_ARG;
+  const long long n = (long long)o->nx[0] * o->nx[1] * o->nx[2];
+  cb::srv::Request r;
+  r.opts = *o;
+  try {
+    r.mR.assign(mR, mR + n);
+    r.mT.assign(mT, mT + n);
+  } catch (...) {
+    return CB_ERR_ALLOC;
+  }
+  r.t_submit = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) return CB_ERR_STATE;
+  if (cb::Solver::estimate_bytes(*o, std::max(1, s->opts.slots_per_pool)) > s->budget) return CB_ERR_TOO_LARGE;
+  r.id = s->next_id++;
+  *id = r.id;
+  s->reqs.emplace(r.id, std::move(r));
+  s->queue.push_back(*id);
+  cb::srv::create_pools_locked(s);
+  s->cv.notify_all();
+  return CB_OK;
+}
+
+int claire_b200_server_poll(claire_b200_server* s, long long id, int* status) {
+  if (!s || !status) return CB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return CB_ERR_ARG;
+  *status = it->second.status;
+  return CB_OK;
+}
+
+int claire_b200_server_wait(claire_b200_server* s, long long id, int timeout_ms, int* status) {
+  if (!s) return CB_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto finished = [&] {
+    auto it = s->reqs.find(id);
+    return it == s->reqs.end() || it->second.status == CB_REQ_DONE || it->second.status == CB_REQ_FAILED;
+  };
+  if (timeout_ms < 0) s->cv.wait(lk, finished);
+  else s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return CB_ERR_ARG;
+  if (status) *status = it->second.status;
+  return CB_OK;
+}
+
+int claire_b200_server_result(claire_b200_server* s, long long id, float* v, claire_b200_stats* st,
+                              double* latency_ms) {
+  if (!s) return CB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return CB_ERR_ARG;
+  cb::srv::Request& r = it->second;
+  if (r.status == CB_REQ_FAILED) {
+    const int e = r.error ? r.error : CB_ERR_STATE;
+    s->reqs.erase(it);
+    return e;
+  }
+  if (r.status != CB_REQ_DONE) return CB_ERR_STATE;
+  if (v) std::memcpy(v, r.v.data(), sizeof(float) * r.v.size());
+  if (st) *st = r.stats;
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
+  s->reqs.erase(it);
+  return CB_OK;
+}
+
+int claire_b200_server_info(claire_b200_server* s, int* pools, long long* bytes_used, int* queued) {
+  if (!s) return CB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  int live = 0;
+  for (auto& p : s->pools) live += p->dead ? 0 : 1;
+  if (pools) *pools = live;
+  if (bytes_used) *bytes_used = s->used;
+  if (queued) *queued = (int)s->queue.size();
+  return CB_OK;
+}
+
+int claire_b200_server_destroy(claire_b200_server* s) {
+  if (!s) return CB_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (long long id : s->queue) cb::srv::fail_request(s, id, CB_ERR_STATE);
+    s->queue.clear();
+    s->cv.notify_all();
+  }
+  for (auto& p : s->pools)
+    if (p->worker.joinable()) p->worker.join();
+  delete s;
+  return CB_OK;
+}
+
+}  // extern "C"

@@ -775,9 +775,9 @@ int Solver::line_search(std::vector<int>& sel) {
 // ---------------------------------------------------------------------------
 // GN loop with CLAIRE's stopping test (src/TaoInterface.cpp:391-527)
 // ---------------------------------------------------------------------------
-int Solver::run(const std::vector<int>& sel_in) {
-  auto t0 = std::chrono::steady_clock::now();
-  std::vector<int> sel = sel_in;
+// InitializeOptimization (src/CLAIRE.cpp:227-357) for the selected problems:
+// J0, D0, ||g0|| at the current velocity; the problems join the GN loop.
+int Solver::begin(const std::vector<int>& sel) {
   for (int b = 0; b < B; ++b)
     if (sel[b]) {
       ProbState keep = ps[b];
@@ -787,9 +787,10 @@ int Solver::run(const std::vector<int>& sel_in) {
       ps[b].beta0 = keep.beta0;
       ps[b].beta1 = keep.beta1;
       ps[b].beta2 = keep.beta2;
+      ps[b].running = true;
+      ps[b].t0 = std::chrono::steady_clock::now();
       state_of[b] = 0;
     }
-  // InitializeOptimization (src/CLAIRE.cpp:227-357): J0, D0, ||g0|| at the initial guess
   CB_TRY(objective_at(v, sel));
   CB_TRY(gradient_at_current(sel));
   for (int b = 0; b < B; ++b)
@@ -798,77 +799,107 @@ int Solver::run(const std::vector<int>& sel_in) {
       ps[b].D0 = ps[b].D;
       ps[b].gnorm0 = ps[b].gnorm > 0.0 ? ps[b].gnorm : 1.0;
     }
+  return 0;
+}
+
+// One GN iteration (src/Optimizer.cpp:257-445) of every running problem that
+// has not met a stopping test (src/TaoInterface.cpp:391-527).  Problems that
+// stop are listed in `finished` (running, done, final values pending).
+int Solver::step(std::vector<int>& finished) {
+  finished.assign(B, 0);
   const double gttol = opts.opttol, gatol = opts.gatol, minstep = 1.0 / 1024.0;
-  while (true) {
-    std::vector<int> act(B, 0);
-    bool any = false;
-    for (int b = 0; b < B; ++b) {
-      if (!sel[b] || ps[b].done) continue;
-      ProbState& s = ps[b];
-      if (!std::isfinite(s.J) || !std::isfinite(s.gnorm)) { s.done = true; s.reason = -1; continue; }
-      if (s.step < minstep) { s.done = true; s.reason = 4; continue; }
-      if (s.gnorm < gttol * s.gnorm0) { s.done = true; s.reason = 1; continue; }
-      if (s.gnorm < gatol) { s.done = true; s.reason = 2; continue; }
-      if (s.iter > opts.maxit - 1) { s.done = true; s.reason = 3; continue; }
-      act[b] = 1;
-      any = true;
-    }
-    if (!any) break;
-    // forcing sequence (src/KrylovInterface.cpp:134-165)
-    std::vector<double> rtol(B, opts.krylovtol[0]);
-    for (int b = 0; b < B; ++b) {
-      if (!act[b]) continue;
-      ProbState& s = ps[b];
-      if (opts.krylovfseq != CB_FSEQ_NONE) {
-        if (s.krylov_g0 < 0) s.krylov_g0 = s.gnorm;
-        const double gr = s.gnorm / s.krylov_g0;
-        double rt = (opts.krylovfseq == CB_FSEQ_QUADRATIC) ? gr : std::sqrt(gr);
-        rt = std::max(1e-16, std::min(0.5, rt));
-        rtol[b] = rt;
-      }
-    }
-    cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
-    CB_TRY(upload_mask(act, dact));
-    CB_TRY(hessian_prep(dact));
-    CB_TRY(pcg(act, std::max(0, opts.krylovmaxit - 1)));
-    std::vector<int> acc = act;
-    CB_TRY(line_search(acc));
-    bool anyacc = false;
-    for (int b = 0; b < B; ++b) anyacc |= (acc[b] != 0);
-    if (anyacc) CB_TRY(gradient_at_current(acc));
-    for (int b = 0; b < B; ++b)
-      if (acc[b]) ps[b].iter++;
-    if (opts.verbosity > 0) {
-      // OptimizationMonitor line (src/TaoInterface.cpp:529-606)
-      for (int b = 0; b < B; ++b)
-        if (act[b])
-          std::fprintf(stderr, "[claire_b200] p%d it %d J/J0 %.6e D/D0 %.6e |g|/|g0| %.6e pcg %d reason %d step %.3e\n",
-                       b, ps[b].iter, ps[b].J / ps[b].J0, ps[b].D / ps[b].D0, ps[b].gnorm / ps[b].gnorm0,
-                       hint[I_IT * B + b], hint[I_REASON * B + b], ps[b].step);
+  std::vector<int> act(B, 0);
+  bool any = false;
+  for (int b = 0; b < B; ++b) {
+    if (!ps[b].running || ps[b].done) continue;
+    ProbState& s = ps[b];
+    if (!std::isfinite(s.J) || !std::isfinite(s.gnorm)) { s.done = true; s.reason = -1; }
+    else if (s.step < minstep) { s.done = true; s.reason = 4; }
+    else if (s.gnorm < gttol * s.gnorm0) { s.done = true; s.reason = 1; }
+    else if (s.gnorm < gatol) { s.done = true; s.reason = 2; }
+    else if (s.iter > opts.maxit - 1) { s.done = true; s.reason = 3; }
+    if (s.done) { finished[b] = 1; continue; }
+    act[b] = 1;
+    any = true;
+  }
+  if (!any) return 0;
+  // forcing sequence (src/KrylovInterface.cpp:134-165)
+  std::vector<double> rtol(B, opts.krylovtol[0]);
+  for (int b = 0; b < B; ++b) {
+    if (!act[b]) continue;
+    ProbState& s = ps[b];
+    if (opts.krylovfseq != CB_FSEQ_NONE) {
+      if (s.krylov_g0 < 0) s.krylov_g0 = s.gnorm;
+      const double gr = s.gnorm / s.krylov_g0;
+      double rt = (opts.krylovfseq == CB_FSEQ_QUADRATIC) ? gr : std::sqrt(gr);
+      rt = std::max(1e-16, std::min(0.5, rt));
+      rtol[b] = rt;
     }
   }
-  // final relative mismatch ||mR - m1|| / ||mR - mT|| (src/CLAIRE.cpp:4232-4262)
-  std::vector<int> need(B, 0);
-  bool anyneed = false;
+  cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+  CB_TRY(upload_mask(act, dact));
+  CB_TRY(hessian_prep(dact));
+  CB_TRY(pcg(act, std::max(0, opts.krylovmaxit - 1)));
+  std::vector<int> acc = act;
+  CB_TRY(line_search(acc));
+  bool anyacc = false;
+  for (int b = 0; b < B; ++b) anyacc |= (acc[b] != 0);
+  if (anyacc) CB_TRY(gradient_at_current(acc));
   for (int b = 0; b < B; ++b)
+    if (acc[b]) ps[b].iter++;
+  if (opts.verbosity > 0) {
+    // OptimizationMonitor line (src/TaoInterface.cpp:529-606)
+    for (int b = 0; b < B; ++b)
+      if (act[b])
+        std::fprintf(stderr, "[claire_b200] p%d it %d J/J0 %.6e D/D0 %.6e |g|/|g0| %.6e pcg %d reason %d step %.3e\n",
+                     b, ps[b].iter, ps[b].J / ps[b].J0, ps[b].D / ps[b].D0, ps[b].gnorm / ps[b].gnorm0,
+                     hint[I_IT * B + b], hint[I_REASON * B + b], ps[b].step);
+  }
+  return 0;
+}
+
+// Final relative mismatch ||mR - m1|| / ||mR - mT|| (src/CLAIRE.cpp:4232-4262)
+// of the selected problems; they leave the GN loop.
+int Solver::finish(const std::vector<int>& sel) {
+  std::vector<int> need(B, 0);
+  bool anyneed = false, anysel = false;
+  for (int b = 0; b < B; ++b) {
+    anysel |= sel[b] != 0;
     if (sel[b] && state_of[b] != 1) { need[b] = 1; anyneed = true; }
+  }
+  if (!anysel) return 0;
   if (anyneed) CB_TRY(objective_at(v, need));
+  CB_TRY(upload_mask(sel, dact));
   const long long PM = (nt + 1) * n;
   const int np = dot_partials(n);
-  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, nullptr, stream));
+  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, dact, stream));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_PQ), B, 1.0, false, stream));
-  CB_TRY(launch_diff_sumsq(mR, n, mT, n, n, B, partials, maxparts, nullptr, stream));
+  CB_TRY(launch_diff_sumsq(mR, n, mT, n, n, B, partials, maxparts, dact, stream));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream));
   note_launches(4);
   CB_TRY(fetch_scalars());
-  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  const auto t1 = std::chrono::steady_clock::now();
   for (int b = 0; b < B; ++b) {
     if (!sel[b]) continue;
     const double num = std::sqrt(hsc[S_PQ * B + b]), den = std::sqrt(hsc[S_RR * B + b]);
     ps[b].rel_mismatch = den > 0 ? num / den : num;
-    ps[b].seconds = secs;
+    ps[b].seconds = std::chrono::duration<double>(t1 - ps[b].t0).count();
+    ps[b].running = false;
+    ps[b].done = true;
   }
   return 0;
+}
+
+int Solver::run(const std::vector<int>& sel) {
+  CB_TRY(begin(sel));
+  std::vector<int> fin;
+  while (true) {
+    bool running = false;
+    for (int b = 0; b < B; ++b) running |= sel[b] && ps[b].running && !ps[b].done;
+    if (!running) break;
+    CB_TRY(step(fin));
+  }
+  return finish(sel);
 }
 
 }  // namespace cb

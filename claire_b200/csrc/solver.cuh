@@ -7,6 +7,7 @@
 // on the device switches problems off once they converge.
 #pragma once
 
+#include <chrono>
 #include <string>
 #include <vector>
 
@@ -28,6 +29,8 @@ struct ProbState {
   double step = 1.0;
   int iter = 0, pcg_total = 0, reason = 0;
   bool done = false;
+  bool running = false;  // between begin() and finish()
+  std::chrono::steady_clock::time_point t0{};
   int obj_evals = 0, grad_evals = 0, hess_matvecs = 0, pc_matvecs = 0, pde_solves = 0;
   double seconds = 0.0, rel_mismatch = -1.0;
 };
@@ -40,7 +43,10 @@ class Solver {
   static long long estimate_bytes(const claire_b200_opts& o, int B);
 
   // ---- public operations (problems selected by the host mask `sel`) -------
-  int run(const std::vector<int>& sel);
+  int run(const std::vector<int>& sel);                  // begin + steps + finish
+  int begin(const std::vector<int>& sel);                // join the GN loop (J0, ||g0||)
+  int step(std::vector<int>& finished);                  // one GN iteration of the running problems
+  int finish(const std::vector<int>& sel);               // final mismatch; leave the loop
   int objective_at(const float* vel, const std::vector<int>& sel);  // fills ps[p].J/D/R
   int gradient_at_current(const std::vector<int>& sel);              // g, ||g|| for v
   int hessian_matvec(const float* vin, float* hout, const std::vector<int>& sel);

@@ -163,6 +163,48 @@ int claire_b200_distance(const float* mR, const float* m1, const int nx[3], doub
 /* Number of CUDA kernel launches issued by this library since load (all threads). */
 long long claire_b200_kernel_launches(void);
 
+/* ---- Serving: continuous batching of independent registrations ----------
+ * The reference runs one registration per CLAIREInterface::Run call
+ * (src/CLAIREInterface.cpp:709-885) and has no serving layer; a server runs
+ * many such calls concurrently on one GPU.  It keeps pools of solver slots,
+ * one pool per (grid, nt, solver-wide options), each with its own stream and
+ * host thread.  A submitted request waits until a slot of its pool is free,
+ * is admitted at the next GN-iteration boundary, keeps its state on the device
+ * until its stopping test fires and frees the slot.  Pools are created while
+ * their footprint (claire_b200_estimate_bytes) fits the HBM budget and release
+ * their memory after idling.  Per-request options that may differ inside a
+ * pool: regnorm and beta.  Results equal those of claire_b200_run on the same
+ * inputs (no data is shared between slots). */
+typedef struct claire_b200_server claire_b200_server;
+typedef struct claire_b200_server_opts {
+  long long hbm_budget_bytes; /* device memory all pools may hold (0: 90% of the free memory) */
+  int slots_per_pool;         /* problems per pool (batch width) */
+  int idle_ms;                /* a pool without work for this long releases its memory */
+  int device;                 /* CUDA device of the server */
+} claire_b200_server_opts;
+#define CB_REQ_QUEUED 0
+#define CB_REQ_RUNNING 1
+#define CB_REQ_DONE 2
+#define CB_REQ_FAILED 3
+void claire_b200_server_default_opts(claire_b200_server_opts* o);
+int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_server** srv);
+/* Queue a registration of host images mR, mT (nx[0]*nx[1]*nx[2] floats each,
+ * copied); zero initial velocity.  CB_ERR_TOO_LARGE if one pool of its key
+ * cannot fit the budget. */
+int claire_b200_server_submit(claire_b200_server* srv, const claire_b200_opts* o, const float* mR, const float* mT,
+                              long long* request_id);
+int claire_b200_server_poll(claire_b200_server* srv, long long request_id, int* status);
+/* Block until the request is done or failed (timeout_ms < 0: no limit). */
+int claire_b200_server_wait(claire_b200_server* srv, long long request_id, int timeout_ms, int* status);
+/* Velocity (host, 3n floats, may be NULL), statistics and submit-to-done
+ * latency of a finished request; releases it.  A failed request returns its
+ * error code. */
+int claire_b200_server_result(claire_b200_server* srv, long long request_id, float* v, claire_b200_stats* stats,
+                              double* latency_ms);
+int claire_b200_server_info(claire_b200_server* srv, int* pools, long long* bytes_used, int* queued);
+/* Fails queued requests, waits for running ones' pools to stop, frees everything. */
+int claire_b200_server_destroy(claire_b200_server* srv);
+
 /* Device timers of the solver's time-step kernels, the counterpart of the
  * reference's per-phase timers and counters (include/RegOpt.hpp:183-202).
  * While enabled, every launch of a category is bracketed by CUDA events on
