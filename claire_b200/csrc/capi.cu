@@ -385,8 +385,15 @@ int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt,
 int claire_b200_interp3(const float* f, const float* disp, float* out, const int nx[3], int dof, void* stream) {
   if (!f || !disp || !out || !dims_ok(nx) || (dof != 1 && dof != 3)) return CB_ERR_ARG;
   Dims d{nx[0], nx[1], nx[2]};
-  note_launches(1);
-  return cuda_status(launch_interp(f, 0, d.n(), disp, 0, out, 0, d.n(), dof, 1, d, nullptr, (cudaStream_t)stream));
+  cudaStream_t s = (cudaStream_t)stream;
+  // box table of this displacement (stream-ordered scratch, freed in order)
+  int4* tab = nullptr;
+  if (cudaMallocAsync((void**)&tab, sizeof(int4) * tile_table_int4s(d), s) != cudaSuccess) return CB_ERR_ALLOC;
+  int e = launch_tile_table(disp, 0, tab, 0, 1, d, nullptr, s);
+  if (!e) e = launch_interp(f, 0, d.n(), disp, 0, tab, 0, out, 0, d.n(), dof, 1, d, nullptr, s);
+  cudaFreeAsync(tab, s);
+  note_launches(2);
+  return cuda_status(e);
 }
 
 int claire_b200_fft_grad(const float* f, float* gout, const int nx[3], void* stream) {

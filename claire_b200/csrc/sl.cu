@@ -118,48 +118,64 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
 // field z of f (ff apart) -> field z of out (of apart)
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_interp(const float* __restrict__ f, long long fp, long long ff, const float* __restrict__ disp, long long dp,
-             float* __restrict__ out, long long op, long long of, Dims d, const int* __restrict__ active) {
+             const int4* __restrict__ tab, long long tp, float* __restrict__ out, long long op, long long of, Dims d,
+             const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  DispSource src{disp + p * dp};
   StoreEpi epi{out + p * op + (long long)blockIdx.z * of};
-  tile_gather(sbuf, src, f + p * fp + (long long)blockIdx.z * ff, d, epi);
+  tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp + (long long)blockIdx.z * ff, d, epi);
 }
 
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_gather_scale(const float* __restrict__ f, long long fp, const float* __restrict__ disp, long long dp,
-                   const float* __restrict__ c, long long cp, float* __restrict__ out, long long op, Dims d,
-                   const int* __restrict__ active) {
+                   const int4* __restrict__ tab, long long tp, const float* __restrict__ c, long long cp,
+                   float* __restrict__ out, long long op, Dims d, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  DispSource src{disp + p * dp};
   ScaleEpi epi{c + p * cp, out + p * op};
-  tile_gather(sbuf, src, f + p * fp, d, epi);
+  tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp, d, epi);
 }
 
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_gather_add(const float* __restrict__ f, long long fp, const float* __restrict__ disp, long long dp,
-                 const float* __restrict__ s, long long sp, float* __restrict__ out, long long op, float sign,
-                 Dims d, const int* __restrict__ active) {
+                 const int4* __restrict__ tab, long long tp, const float* __restrict__ s, long long sp,
+                 float* __restrict__ out, long long op, float sign, Dims d, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  DispSource src{disp + p * dp};
   AddEpi epi{s + p * sp, out + p * op, sign};
-  tile_gather(sbuf, src, f + p * fp, d, epi);
+  tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp, d, epi);
 }
 
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_adjoint_coef(const float* __restrict__ divv, long long vp, const float* __restrict__ disp, long long dp,
-                   float* __restrict__ out, long long op, float ht, Dims d, const int* __restrict__ active) {
+                   const int4* __restrict__ tab, long long tp, float* __restrict__ out, long long op, float ht, Dims d,
+                   const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  DispSource src{disp + p * dp};
   AdjCoefEpi epi{divv + p * vp, out + p * op, ht};
-  tile_gather(sbuf, src, divv + p * vp, d, epi);
+  tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, divv + p * vp, d, epi);
+}
+
+// Box table of a displacement field (sl_tile.cuh box_from_table layout).
+__global__ void __launch_bounds__(kTileThreads)
+    k_tile_table(const float* __restrict__ disp, long long dp, int4* __restrict__ tab, long long tp, Dims d,
+                 const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const TileThread tt = tile_thread(d);
+  float dd[kTilePts][3];
+  DispSource{disp + p * dp}.load(dd, tt, d);
+  int lo[3], hi[3];
+  tile_bounds(dd, tt, lo, hi);
+  if (threadIdx.x == 0) {
+    int4* t = tab + p * tp + 2 * blockIdx.x;
+    t[0] = make_int4(lo[0], lo[1], lo[2], hi[0]);
+    t[1] = make_int4(hi[1], hi[2], 0, 0);
+  }
 }
 
 // ---- pointwise kernels (4 consecutive points per thread, float4) ---------------
@@ -238,42 +254,51 @@ int launch_trajectory(const float* v, long long vp, float* disp, long long dp, i
   return (int)cudaGetLastError();
 }
 
-int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp,
-                  float* out, long long op, long long of, int nf, int nprob, const Dims& d,
+long long tile_table_int4s(const Dims& d) { return 2LL * tile_count(d); }
+
+int launch_tile_table(const float* disp, long long dp, int4* tab, long long tp, int nprob, const Dims& d,
+                      const int* active, cudaStream_t s) {
+  k_tile_table<<<tile_grid(d, nprob, 1), kTileThreads, 0, s>>>(disp, dp, tab, tp, d, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp, const int4* tab,
+                  long long tp, float* out, long long op, long long of, int nf, int nprob, const Dims& d,
                   const int* active, cudaStream_t s) {
   int e = allow_smem(k_interp);
   if (e) return e;
-  k_interp<<<tile_grid(d, nprob, nf), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, out, op, of, d,
-                                                                           active);
+  k_interp<<<tile_grid(d, nprob, nf), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, tab, tp, out, op,
+                                                                           of, d, active);
   return (int)cudaGetLastError();
 }
 
-int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const float* c,
-                        long long cp, float* out, long long op, int nprob, const Dims& d, const int* active,
-                        cudaStream_t s) {
+int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const int4* tab,
+                        long long tp, const float* c, long long cp, float* out, long long op, int nprob,
+                        const Dims& d, const int* active, cudaStream_t s) {
   int e = allow_smem(k_gather_scale);
   if (e) return e;
-  k_gather_scale<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, c, cp, out, op,
-                                                                                d, active);
+  k_gather_scale<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, tab, tp, c, cp,
+                                                                                out, op, d, active);
   return (int)cudaGetLastError();
 }
 
-int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const float* src,
-                      long long sp, float* out, long long op, float sign, int nprob, const Dims& d,
-                      const int* active, cudaStream_t s) {
+int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const int4* tab,
+                      long long tp, const float* src, long long sp, float* out, long long op, float sign, int nprob,
+                      const Dims& d, const int* active, cudaStream_t s) {
   int e = allow_smem(k_gather_add);
   if (e) return e;
-  k_gather_add<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, src, sp, out, op,
-                                                                              sign, d, active);
+  k_gather_add<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, tab, tp, src, sp,
+                                                                              out, op, sign, d, active);
   return (int)cudaGetLastError();
 }
 
-int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, float* out,
-                        long long op, float ht, int nprob, const Dims& d, const int* active, cudaStream_t s) {
+int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, const int4* tab,
+                        long long tp, float* out, long long op, float ht, int nprob, const Dims& d,
+                        const int* active, cudaStream_t s) {
   int e = allow_smem(k_adjoint_coef);
   if (e) return e;
-  k_adjoint_coef<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(divv, vp, disp, dp, out, op, ht,
-                                                                                d, active);
+  k_adjoint_coef<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(divv, vp, disp, dp, tab, tp, out,
+                                                                                op, ht, d, active);
   return (int)cudaGetLastError();
 }
 

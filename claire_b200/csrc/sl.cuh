@@ -80,30 +80,38 @@ CB_DEVICE void point_index(long long i, const Dims& d, int& i1, int& i2, int& i3
 int launch_trajectory(const float* v, long long vp, float* disp, long long dp, int nprob,
                       const Dims& d, float ht, float sign, const int* active, cudaStream_t s);
 
-// out[p][f] <- f[p][f](i + disp[p](i)), f = 0..nf-1; fields ff apart.
-int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp,
-                  float* out, long long op, long long of, int nf, int nprob, const Dims& d,
+// Box table of displacement field disp[p] for the tile gathers below:
+// 2 int4 per 8x8x16 tile (tile_table_int4s(d) int4 per problem, tp apart).
+int launch_tile_table(const float* disp, long long dp, int4* tab, long long tp, int nprob, const Dims& d,
+                      const int* active, cudaStream_t s);
+long long tile_table_int4s(const Dims& d);
+
+// out[p][f] <- f[p][f](i + disp[p](i)), f = 0..nf-1; fields ff apart; tab =
+// disp's box table.
+int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp, const int4* tab,
+                  long long tp, float* out, long long op, long long of, int nf, int nprob, const Dims& d,
                   const int* active, cudaStream_t s);
 
 // out[p] = c[p] * f[p](i + disp[p](i)): one backward RK2 step of the
 // (incremental) adjoint, lambda^{l-1} = c * lambda^l(X) with the per-point
 // factor c of launch_adjoint_coef (src/CLAIRE.cpp:2646-2686, 3940-3971).
-int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const float* c,
-                        long long cp, float* out, long long op, int nprob, const Dims& d, const int* active,
-                        cudaStream_t s);
+int launch_gather_scale(const float* f, long long fp, const float* disp, long long dp, const int4* tab,
+                        long long tp, const float* c, long long cp, float* out, long long op, int nprob,
+                        const Dims& d, const int* active, cudaStream_t s);
 
 // out[p] = sign * (f[p](i + disp[p](i)) + src[p](i)): one incremental state
 // step m~^{j+1} = m~^j(X) + s_j (src/CLAIRE.cpp:3220-3276); sign -1 writes the
 // incremental adjoint's final condition -m~(t=1) (src/DistanceMeasureSL2.cpp:223-283).
-int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const float* src,
-                      long long sp, float* out, long long op, float sign, int nprob, const Dims& d,
-                      const int* active, cudaStream_t s);
+int launch_gather_add(const float* f, long long fp, const float* disp, long long dp, const int4* tab,
+                      long long tp, const float* src, long long sp, float* out, long long op, float sign, int nprob,
+                      const Dims& d, const int* active, cudaStream_t s);
 
 // RK2 adjoint step factor: with dx = divv(X) and dv = divv,
 //   lx + ht/2 (rhs0 + rhs1), rhs0 = lx dx, rhs1 = (lx + ht rhs0) dv
 // equals lx * (1 + ht/2 (dx + dv + ht dx dv)); out = that factor.
-int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, float* out,
-                        long long op, float ht, int nprob, const Dims& d, const int* active, cudaStream_t s);
+int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, const int4* tab,
+                        long long tp, float* out, long long op, float ht, int nprob, const Dims& d,
+                        const int* active, cudaStream_t s);
 
 // Trapezoid body force over the stored adjoint levels (src/CLAIRE.cpp:2646-2709):
 //   b[k] = scale * sum_l w_l lam^l (d/dx_k m^l),  w_0 = w_nt = ht/2, else ht.

@@ -44,6 +44,23 @@ __host__ __device__ inline unsigned tile_count(const Dims& d) {
   return (unsigned)(((d.n1 + kT1 - 1) / kT1) * ((d.n2 + kT2 - 1) / kT2) * ((d.n3 + kT3 - 1) / kT3));
 }
 
+// q / m for 0 <= q < 2^22 and 1 <= m < 2^12 without an integer division:
+// float estimate, then one correction each way.
+CB_DEVICE int small_div(int q, int m) {
+  int t = __float2int_rz((float)q * (1.f / (float)m));
+  const int r = q - t * m;
+  t += (r >= m) ? 1 : 0;
+  t -= (r < 0) ? 1 : 0;
+  return t;
+}
+
+// x mod n for x in [-n, 2n)
+CB_DEVICE int wrap_near(int x, int n) {
+  x += (x < 0) ? n : 0;
+  x -= (x >= n) ? n : 0;
+  return x;
+}
+
 // This thread's points in the CTA's tile: (t1 + 2a, i2, i3), a < 4.  Point
 // indices are 32-bit (grids up to 1024^3 points).
 struct TileThread {
@@ -59,8 +76,8 @@ struct TileThread {
 CB_DEVICE TileThread tile_thread(const Dims& d) {
   const int nb3 = (d.n3 + kT3 - 1) / kT3, nb2 = (d.n2 + kT2 - 1) / kT2;
   const int t = blockIdx.x;
-  const int c3 = t % nb3, r = t / nb3;
-  const int c2 = r % nb2, c1 = r / nb2;
+  const int r = small_div(t, nb3), c3 = t - r * nb3;
+  const int c1 = small_div(r, nb2), c2 = r - c1 * nb2;
   const int lane = threadIdx.x & 31;
   TileThread tt;
   tt.t1 = c1 * kT1 + (lane >> 4);
@@ -84,14 +101,44 @@ struct TileBox {
   bool within;     // copyable (one wrap per axis, whole chunks)
 };
 
-// Block-wide bounding box of the stencil taps of the tile's valid points.
+// Box of the stencil bases b in [lo, hi] per axis (taps b .. b+3).
+CB_DEVICE TileBox box_from_bounds(const int (&lo)[3], const int (&hi)[3], const Dims& d) {
+  TileBox bx;
+  int ext[3];
+  bool within = true;
+  const int nk[3] = {d.n1, d.n2, d.n3};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    bx.lo[k] = lo[k];
+    const long long e = (long long)hi[k] - (long long)lo[k] + 4;
+    ext[k] = (e > 0 && e <= 4096) ? (int)e : 4096;
+    // one wrap per coordinate in the copy, origin within one period
+    within = within && e > 0 && e <= nk[k] && lo[k] >= -nk[k] && lo[k] < nk[k];
+  }
+  // x3: start on a multiple of 4 floats and cover whole 4-float chunks so the
+  // box is copied in 16-byte pieces (N3 % 4 == 0: no chunk straddles the seam)
+  const int lo3a = bx.lo[2] & ~3;
+  bx.e3 = ((bx.lo[2] + ext[2] - lo3a) + 3) & ~3;
+  bx.lo[2] = lo3a;
+  within = within && bx.e3 <= d.n3 && bx.e3 <= 64 && (d.n3 & 3) == 0;
+  bx.e1 = ext[0];
+  bx.e2 = ext[1];
+  bx.P = bx.e3 <= 32 ? 32 : 64;
+  bx.Q = bx.e2 * bx.P + 16;
+  const long long vol = ((long long)bx.e1 * bx.Q + 31) & ~31LL;
+  bx.vol = vol < (1 << 24) ? (int)vol : (1 << 24);
+  bx.within = within;
+  return bx;
+}
+
+// Block-wide min / max of the stencil bases of the tile's valid points.
 // Contains __syncthreads: call once, from uniform control flow.
-CB_DEVICE TileBox tile_box(const float (&dd)[kTilePts][3], const TileThread& tt, const Dims& d) {
+CB_DEVICE void tile_bounds(const float (&dd)[kTilePts][3], const TileThread& tt, int (&lo)[3], int (&hi)[3]) {
   __shared__ int red[6][kTileThreads / 32];
   int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
   for (int a = 0; a < kTilePts; ++a) {
-    if (!tt.valid(a, d)) continue;
+    if (!tt.valid_idx(a)) continue;
     const int b1 = tt.x1(a) + (int)floorf(dd[a][0]) - 1;
     const int b2 = tt.i2 + (int)floorf(dd[a][1]) - 1;
     const int b3 = tt.i3 + (int)floorf(dd[a][2]) - 1;
@@ -116,37 +163,28 @@ CB_DEVICE TileBox tile_box(const float (&dd)[kTilePts][3], const TileThread& tt,
     }
   }
   __syncthreads();
-  TileBox bx;
-  int ext[3];
-  bool within = true;
-  const int nk[3] = {d.n1, d.n2, d.n3};
+  // every warp reduces the 8 warp partials itself (lane l reads partial l % 8)
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
-    int lo = INT_MAX, hi = INT_MIN;
-#pragma unroll
-    for (int w = 0; w < kTileThreads / 32; ++w) {
-      lo = min(lo, red[k][w]);
-      hi = max(hi, red[3 + k][w]);
-    }
-    bx.lo[k] = lo;
-    const long long e = (long long)hi - (long long)lo + 4;  // taps b .. b+3
-    ext[k] = (e > 0 && e <= 4096) ? (int)e : 4096;
-    within = within && e > 0 && e <= nk[k];  // one wrap per coordinate in the copy
+    lo[k] = __reduce_min_sync(0xffffffffu, red[k][lane & 7]);
+    hi[k] = __reduce_max_sync(0xffffffffu, red[3 + k][lane & 7]);
   }
-  // x3: start on a multiple of 4 floats and cover whole 4-float chunks so the
-  // box is copied in 16-byte pieces (N3 % 4 == 0: no chunk straddles the seam)
-  const int lo3a = bx.lo[2] & ~3;
-  bx.e3 = ((bx.lo[2] + ext[2] - lo3a) + 3) & ~3;
-  bx.lo[2] = lo3a;
-  within = within && bx.e3 <= d.n3 && bx.e3 <= 64 && (d.n3 & 3) == 0;
-  bx.e1 = ext[0];
-  bx.e2 = ext[1];
-  bx.P = bx.e3 <= 32 ? 32 : 64;
-  bx.Q = bx.e2 * bx.P + 16;
-  const long long vol = ((long long)bx.e1 * bx.Q + 31) & ~31LL;
-  bx.vol = vol < (1 << 24) ? (int)vol : (1 << 24);
-  bx.within = within;
-  return bx;
+}
+
+CB_DEVICE TileBox tile_box(const float (&dd)[kTilePts][3], const TileThread& tt, const Dims& d) {
+  int lo[3], hi[3];
+  tile_bounds(dd, tt, lo, hi);
+  return box_from_bounds(lo, hi, d);
+}
+
+// Per-tile box table of a displacement field: two int4 per tile,
+// {lo1, lo2, lo3, hi1}, {hi2, hi3, 0, 0} of the stencil bases.  It depends on
+// the displacement only, so one table serves every gather at that
+// characteristic (all time steps, all matvecs of a GN iterate).
+CB_DEVICE TileBox box_from_table(const int4* __restrict__ tab, const Dims& d) {
+  const int4 a = __ldg(tab + 2 * blockIdx.x), b = __ldg(tab + 2 * blockIdx.x + 1);
+  const int lo[3] = {a.x, a.y, a.z}, hi[3] = {a.w, b.x, b.y};
+  return box_from_bounds(lo, hi, d);
 }
 
 CB_DEVICE void cp_async16(float* smem_dst, const float* gmem_src) {
@@ -161,22 +199,23 @@ CB_DEVICE void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" :::
 // incrementally, without divisions.  The box never exceeds the grid along an
 // axis, so one conditional subtraction wraps each coordinate.
 CB_DEVICE void issue_box(float* __restrict__ sb, const float* __restrict__ f, const TileBox& bx, const Dims& d) {
-  const int nck = bx.e3 >> 2;  // 16-byte chunks per row, 1 .. 16
-  const int rpi = 32 / nck;    // rows a warp copies per step
+  const int nck = bx.e3 >> 2;           // 16-byte chunks per row, 1 .. 16
+  const int rpi = small_div(32, nck);   // rows a warp copies per step
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lr = lane / nck, lc = lane - lr * nck;
+  const int lr = small_div(lane, nck), lc = lane - lr * nck;
   if (lr >= rpi) return;
-  const int w1 = wrap(bx.lo[0], d.n1), w2 = wrap(bx.lo[1], d.n2);
-  int g3 = wrap(bx.lo[2], d.n3) + 4 * lc;
+  const int w1 = wrap_near(bx.lo[0], d.n1), w2 = wrap_near(bx.lo[1], d.n2);
+  int g3 = wrap_near(bx.lo[2], d.n3) + 4 * lc;
   g3 -= (g3 >= d.n3) ? d.n3 : 0;
+  const float* fb = f + g3;
   const int rstep = rpi * (kTileThreads / 32);
   const int r0 = warp * rpi + lr;
-  int l1 = r0 / bx.e2, l2 = r0 - l1 * bx.e2;
+  int l1 = small_div(r0, bx.e2), l2 = r0 - l1 * bx.e2;
   while (l1 < bx.e1) {
     int g1 = w1 + l1, g2 = w2 + l2;
     g1 -= (g1 >= d.n1) ? d.n1 : 0;
     g2 -= (g2 >= d.n2) ? d.n2 : 0;
-    cp_async16(sb + l1 * bx.Q + l2 * bx.P + 4 * lc, f + ((long long)g1 * d.n2 + g2) * d.n3 + g3);
+    cp_async16(sb + l1 * bx.Q + l2 * bx.P + 4 * lc, fb + ((unsigned)g1 * (unsigned)d.n2 + (unsigned)g2) * (unsigned)d.n3);
     l2 += rstep;
     while (l2 >= bx.e2) {
       l2 -= bx.e2;
@@ -254,6 +293,50 @@ CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ 
   if (bx.within && bx.vol <= kGatherBudget) {
     issue_box(sb, f, bx, d);
     cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
+#pragma unroll
+    for (int a = 0; a < kTilePts; ++a) {
+      const BoxPoint bp = box_point(dd[a], tt.x1(a), tt, tt.valid_idx(a), bx);
+      epi(tt, a, gather_staged(sbase, bp, bx));
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < kTilePts; ++a) {
+      if (!tt.valid_idx(a)) continue;
+      Stencil st;
+      make_stencil(tt.x1(a), tt.i2, tt.i3, dd[a][0], dd[a][1], dd[a][2], d, st);
+      epi(tt, a, gather(f, st));
+    }
+  }
+}
+
+// Tile gather of one field at a displacement field with a precomputed box
+// table: the box copy is issued first and the points' displacements load
+// while it is in flight.
+template <class Epi>
+CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const int4* __restrict__ tab,
+                               const float* __restrict__ f, const Dims& d, const Epi& epi) {
+  const TileBox bx = box_from_table(tab, d);
+  const bool staged = bx.within && bx.vol <= kGatherBudget;
+  if (staged) {
+    issue_box(sb, f, bx, d);
+    cp_async_commit();
+  }
+  const TileThread tt = tile_thread(d);
+  float dd[kTilePts][3];
+  const float* d2 = disp + d.n();
+  const float* d3 = d2 + d.n();
+#pragma unroll
+  for (int a = 0; a < kTilePts; ++a) {
+    const bool ok = tt.valid_idx(a);
+    const unsigned i = tt.idx(a);
+    dd[a][0] = ok ? __ldg(disp + i) : 0.f;
+    dd[a][1] = ok ? __ldg(d2 + i) : 0.f;
+    dd[a][2] = ok ? __ldg(d3 + i) : 0.f;
+  }
+  if (staged) {
     cp_async_wait_all();
     __syncthreads();
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);

@@ -98,7 +98,7 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 // ---------------------------------------------------------------------------
 Solver::~Solver() {
   prof_clear();
-  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, gm, gx, divv, cadj, lamh, bf, g, x,
+  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
                   r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -140,6 +140,7 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   floats += nt * n;                   // incremental state sources
   floats += 3 * n * 9;                // bf, g, x, r, z, p, q, vtx, work3
   long long bytes = floats * 4 + 3 * nc * 8;
+  bytes += 2 * tile_table_int4s(d) * 16;  // box tables of the two characteristics
   bytes += (long long)max_parts(d) * 8;
   return bytes * B;
 }
@@ -174,6 +175,9 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   CB_TRY(alloc((void**)&m, S * (nt + 1)));
   CB_TRY(alloc((void**)&disp_st, V));
   CB_TRY(alloc((void**)&disp_adj, V));
+  TP = tile_table_int4s(d);
+  CB_TRY(alloc((void**)&tab_st, sizeof(int4) * TP * B));
+  CB_TRY(alloc((void**)&tab_adj, sizeof(int4) * TP * B));
   CB_TRY(alloc((void**)&gm, V * (nt + 1)));
   CB_TRY(alloc((void**)&gx, V * nt));
   CB_TRY(alloc((void**)&divv, S));
@@ -283,13 +287,24 @@ int Solver::dot(const float* a, long long ap, const float* b, long long bp, long
 // ---------------------------------------------------------------------------
 // forward problem (src/CLAIRE.cpp:1861-1984, 2116-2175)
 // ---------------------------------------------------------------------------
+// RK2 characteristic (sign +1 state into disp_st, -1 adjoint into disp_adj)
+// and the box table its gathers use.
+int Solver::characteristic(const float* vel, float sign, const int* act) {
+  float* disp = sign > 0 ? disp_st : disp_adj;
+  int4* tab = sign > 0 ? tab_st : tab_adj;
+  CB_TRY(launch_trajectory(vel, 3 * n, disp, 3 * n, B, d, ht, sign, act, stream));
+  CB_TRY(launch_tile_table(disp, 3 * n, tab, TP, B, d, act, stream));
+  note_launches(1);
+  return 0;
+}
+
 int Solver::state_solve(const float* vel, const int* act) {
   const long long PM = (nt + 1) * n;
-  CB_TRY(launch_trajectory(vel, 3 * n, disp_st, 3 * n, B, d, ht, 1.f, act, stream));
+  CB_TRY(characteristic(vel, 1.f, act));
   CB_TRY(launch_lincomb(m, PM, mT, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
   for (int j = 0; j < nt; ++j) {
     CB_TRY(prof_mark(CB_PROF_STATE_STEP));
-    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, m + (j + 1) * n, PM, n, 1, B, d, act, stream));
+    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, tab_st, TP, m + (j + 1) * n, PM, n, 1, B, d, act, stream));
     CB_TRY(prof_mark(CB_PROF_STATE_STEP));
   }
   note_launches(2 + nt);
@@ -467,8 +482,8 @@ int Solver::adjoint_sweep(float* bout, const int* act) {
   for (int j = 0; j < nt; ++j) {
     const int l = nt - j;  // lambda^{l-1} = c * lambda^l(X_adj)
     CB_TRY(prof_mark(CB_PROF_ADJOINT_STEP));
-    CB_TRY(launch_gather_scale(lamh + l * n, PL, disp_adj, 3 * n, cadj, n, lamh + (l - 1) * n, PL, B, d, act,
-                               stream));
+    CB_TRY(launch_gather_scale(lamh + l * n, PL, disp_adj, 3 * n, tab_adj, TP, cadj, n, lamh + (l - 1) * n, PL, B,
+                               d, act, stream));
     CB_TRY(prof_mark(CB_PROF_ADJOINT_STEP));
   }
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
@@ -506,10 +521,10 @@ int Solver::finish_with_reg(const float* vin, float* out, const int* act) {
 // EvaluateGradient at v (src/CLAIRE.cpp:871-1042); the state must be valid for v.
 int Solver::gradient(const int* act) {
   const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
-  CB_TRY(launch_trajectory(v, 3 * n, disp_adj, 3 * n, B, d, ht, -1.f, act, stream));
+  CB_TRY(characteristic(v, -1.f, act));
   CB_TRY(grad_fields(m, PM, n, gm, PGM, 3 * n, nt + 1, act));
   CB_TRY(divergence(v, divv, act));
-  CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, cadj, n, ht, B, d, act, stream));
+  CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, tab_adj, TP, cadj, n, ht, B, d, act, stream));
   // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222)
   CB_TRY(launch_lincomb(lamh + nt * n, PL, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
   note_launches(3);
@@ -521,7 +536,7 @@ int Solver::gradient(const int* act) {
 // caches for the Hessian: (grad m^j)(X_state), j < nt
 int Solver::hessian_prep(const int* act) {
   const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n;
-  CB_TRY(launch_interp(gm, PGM, n, disp_st, 3 * n, gx, PGX, n, 3 * nt, B, d, act, stream));
+  CB_TRY(launch_interp(gm, PGM, n, disp_st, 3 * n, tab_st, TP, gx, PGX, n, 3 * nt, B, d, act, stream));
   note_launches(1);
   return 0;
 }
@@ -531,7 +546,7 @@ int Solver::hessian_prep(const int* act) {
 // lambda~(t=1) = -m~(t=1) straight into the adjoint's level nt.
 int Solver::hessian(const float* vin, float* hout, const int* act) {
   const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n, PL = (nt + 1) * n, PS = nt * n;
-  CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, vtx, 3 * n, n, 3, B, d, act, stream));
+  CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, tab_st, TP, vtx, 3 * n, n, 3, B, d, act, stream));
   CB_TRY(launch_incstate_source(gx, PGX, vtx, 3 * n, gm, PGM, vin, 3 * n, sj, PS, nt, ht, B, n, act, stream));
   note_launches(2);
   float* lam_end = lamh + nt * n;
@@ -546,8 +561,8 @@ int Solver::hessian(const float* vin, float* hout, const int* act) {
     const bool last = (j == nt - 1);
     float* out = last ? lam_end : bufs[j & 1];
     CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
-    CB_TRY(launch_gather_add(cur, cp, disp_st, 3 * n, sj + j * n, PS, out, last ? PL : n, last ? -1.f : 1.f, B, d,
-                             act, stream));
+    CB_TRY(launch_gather_add(cur, cp, disp_st, 3 * n, tab_st, TP, sj + j * n, PS, out, last ? PL : n,
+                             last ? -1.f : 1.f, B, d, act, stream));
     CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
     cur = out;
     cp = n;
@@ -602,10 +617,11 @@ int Solver::forward(const float* m0, float* m1, const std::vector<int>& sel) {
   // m0 / m1 are device arrays laid out like mT (problem stride n)
   CB_TRY(upload_mask(sel, dact));
   const long long PM = (nt + 1) * n;
-  CB_TRY(launch_trajectory(v, 3 * n, disp_st, 3 * n, B, d, ht, 1.f, dact, stream));
+  CB_TRY(characteristic(v, 1.f, dact));
   CB_TRY(launch_lincomb(m, PM, m0, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
   for (int j = 0; j < nt; ++j)
-    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, m + (j + 1) * n, PM, n, 1, B, d, dact, stream));
+    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, tab_st, TP, m + (j + 1) * n, PM, n, 1, B, d, dact,
+                         stream));
   CB_TRY(launch_lincomb(m1, n, m + nt * n, PM, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
   note_launches(3 + nt);
   for (int b = 0; b < B; ++b)

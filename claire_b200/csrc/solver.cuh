@@ -70,6 +70,8 @@ class Solver {
   // device state (see DESIGN.md for the layout)
   float *mR = nullptr, *mT = nullptr, *v = nullptr, *vtrial = nullptr, *m = nullptr;
   float *disp_st = nullptr, *disp_adj = nullptr, *gm = nullptr, *gx = nullptr;
+  int4 *tab_st = nullptr, *tab_adj = nullptr;  // box tables of the two characteristics
+  long long TP = 0;                              // int4 per problem in a box table
   float *divv = nullptr, *cadj = nullptr, *lamh = nullptr, *bf = nullptr;
   float *g = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *q = nullptr;
   float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *sj = nullptr, *work3 = nullptr;
@@ -108,6 +110,7 @@ class Solver {
   int fetch_scalars();
 
   // building blocks (act: device mask)
+  int characteristic(const float* vel, float sign, const int* act);
   int state_solve(const float* vel, const int* act);
   int distance(const int* act);
   int reg_functional(const float* vel, const std::vector<int>& sel, const int* act);
