@@ -78,20 +78,23 @@ constexpr int kThreads = kFftThreads;
 // accumulate its square.  For EPI_ADD the old values of a group of 8 elements
 // are loaded before any of them is stored, so the loads overlap.
 template <int N, int P, int PITCH>
-CB_DEVICE double rows_epilogue(const float* re, const float* im, float* __restrict__ dst, int row0, int nr,
-                               int epi, float al) {
+CB_DEVICE double rows_epilogue(const float* re, const float* im, float* __restrict__ dst,
+                               const float* __restrict__ other, int row0, int nr, int epi, float al) {
   constexpr int TOTAL = 2 * P * N;
   constexpr int G = 8;
+  const bool add = (epi == EPI_ADD || epi == EPI_ADD_DOT);
+  const bool dot = (epi == EPI_STORE_DOT || epi == EPI_ADD_DOT);
   double acc = 0.0;
   for (int i0 = threadIdx.x; i0 < TOTAL; i0 += G * kThreads) {
-    float old[G];
-    if (epi == EPI_ADD) {
+    float old[G], oth[G];
 #pragma unroll
-      for (int u = 0; u < G; ++u) {
-        const int idx = i0 + u * kThreads;
-        const int r = idx / N, e = idx - r * N;
-        old[u] = (idx < TOTAL && r < nr) ? dst[(long long)(row0 + r) * N + e] : 0.f;
-      }
+    for (int u = 0; u < G; ++u) {
+      const int idx = i0 + u * kThreads;
+      const int r = idx / N, e = idx - r * N;
+      const bool in = idx < TOTAL && r < nr;
+      const long long gi = (long long)(row0 + r) * N + e;
+      old[u] = (add && in) ? dst[gi] : 0.f;
+      oth[u] = (dot && in) ? other[gi] : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < G; ++u) {
@@ -100,13 +103,19 @@ CB_DEVICE double rows_epilogue(const float* re, const float* im, float* __restri
       if (idx >= TOTAL || r >= nr) continue;
       const float val = al * ((r & 1) ? im : re)[e * PITCH + (r >> 1)];
       const long long gi = (long long)(row0 + r) * N + e;
-      if (epi == EPI_STORE) dst[gi] = val;
-      else if (epi == EPI_ADD) dst[gi] = old[u] + val;
-      else acc += (double)val * (double)val;
+      if (epi == EPI_SUMSQ) {
+        acc += (double)val * (double)val;
+        continue;
+      }
+      const float nv = add ? old[u] + val : val;
+      dst[gi] = nv;
+      if (dot) acc += (double)nv * (double)oth[u];
     }
   }
   return acc;
 }
+
+CB_DEVICE bool epi_reduces(int epi) { return epi == EPI_SUMSQ || epi == EPI_STORE_DOT || epi == EPI_ADD_DOT; }
 
 // ---------------------------------------------------------------------------
 // load helpers
@@ -221,6 +230,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
                                                         const float2* __restrict__ twg, int epi,
                                                         const float* __restrict__ alpha,
                                                         double* __restrict__ partials, int nparts,
+                                                        const float* __restrict__ other,
                                                         const int* __restrict__ active) {
   constexpr int P = RowCfg<N>::P, PITCH = RowCfg<N>::PITCH, NH = N / 2 + 1;
   if (active && !active[blockIdx.z]) return;
@@ -234,6 +244,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
   float* sti = str + 2 * P * NH;
   const float2* src = in + blockIdx.z * ip + blockIdx.y * ifs;
   float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
+  const float* oth = other ? other + blockIdx.z * op + blockIdx.y * ofs : nullptr;
   const int row0 = blockIdx.x * 2 * P;
   const int nr = min(2 * P, nrows - row0);
   load_twiddles<N>(tw, twg);
@@ -282,8 +293,8 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
   __syncthreads();
   fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
   const float al = alpha ? alpha[blockIdx.z] : 1.f;
-  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, row0, nr, epi, al);
-  if (epi == EPI_SUMSQ) {
+  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, oth, row0, nr, epi, al);
+  if (epi_reduces(epi)) {
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
   }
 }
@@ -581,7 +592,7 @@ __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict
   mul_ik<N, P, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
   fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
-  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, row0, nr, epi, 1.f);
+  const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, nullptr, row0, nr, epi, 1.f);
   if (epi == EPI_SUMSQ)
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
 }
@@ -696,7 +707,7 @@ static int r2c_rows_impl(const float* in, long long ip, long long ifs, float2* o
 template <int N>
 static int c2r_rows_impl(const float2* in, long long ip, long long ifs, float* out, long long op,
                          long long ofs, int nrows, int nf, int nprob, int epi, const float* alpha,
-                         double* partials, int nparts, const int* active, cudaStream_t s) {
+                         double* partials, int nparts, const float* other, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
   size_t sm = row_smem<N>(true);
@@ -704,7 +715,7 @@ static int c2r_rows_impl(const float2* in, long long ip, long long ifs, float* o
   if (e) return e;
   dim3 grid((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), nf, nprob);
   k_c2r_rows<N><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op, ofs, nrows, tw, epi, alpha, partials,
-                                            nparts, active);
+                                            nparts, other, active);
   return (int)cudaGetLastError();
 }
 
@@ -808,7 +819,8 @@ int c2r_partials(const Dims& d, int nf) {
 
 int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long long ofs, int nf,
                  int nprob, const Dims& d, int epi, const float* alpha, double* partials, int nparts,
-                 const int* active, cudaStream_t s) {
+                 const int* active, cudaStream_t s, const float* other) {
+  if ((epi == EPI_STORE_DOT || epi == EPI_ADD_DOT) && !other) return (int)cudaErrorInvalidValue;
   if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
@@ -817,7 +829,7 @@ int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long lon
                                                nf, nprob, active, s)));
   if (e) return e;
   CB_DISPATCH_N(d.n3, e = c2r_rows_impl<NN>(spec, sp, nc, out, op_, ofs, d.n1 * d.n2, nf, nprob, epi, alpha,
-                                            partials, nparts, active, s));
+                                            partials, nparts, other, active, s));
   return e;
 }
 
@@ -905,7 +917,7 @@ static int spectral3_explicit_impl(const float* in, float* out, float2* spec, co
   k_cols<N, true><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                          nullptr);
   k_c2r_rows<N><<<rows, kThreads, row_smem<N>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
-                                                           nullptr, 0, nullptr);
+                                                           nullptr, 0, nullptr, nullptr);
   return (int)cudaGetLastError();
 }
 

@@ -17,6 +17,8 @@ int dot_partials(long long len) {
   return (int)(need < kRedBlocks ? (need < 1 ? 1 : need) : kRedBlocks);
 }
 
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
 __global__ void __launch_bounds__(kRedThreads) k_dot(const float* __restrict__ a, long long ap,
                                                       const float* __restrict__ b, long long bp,
                                                       long long len, double* __restrict__ partials,
@@ -29,6 +31,65 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(const float* __restrict__ a
        i += (long long)gridDim.x * blockDim.x)
     acc += (double)pa[i] * (double)pb[i];
   block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+// float4 form (len % 4 == 0, 16-byte aligned rows): four products per load
+__global__ void __launch_bounds__(kRedThreads) k_dot4(const float4* __restrict__ a, long long ap,
+                                                       const float4* __restrict__ b, long long bp,
+                                                       long long len4, double* __restrict__ partials,
+                                                       int nparts, const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const float4* pa = a + blockIdx.y * ap;
+  const float4* pb = b + blockIdx.y * bp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len4;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float4 x = __ldg(pa + i), y = __ldg(pb + i);
+    acc += (double)x.x * (double)y.x + (double)x.y * (double)y.y + (double)x.z * (double)y.z +
+           (double)x.w * (double)y.w;
+  }
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+// PCG update x += alpha p, r -= alpha q, partial sums of r.r (the new residual)
+__global__ void __launch_bounds__(kRedThreads) k_cg_update(float4* __restrict__ x, float4* __restrict__ r,
+                                                            const float4* __restrict__ p,
+                                                            const float4* __restrict__ q, long long vp,
+                                                            long long len4, const double* __restrict__ alpha,
+                                                            double* __restrict__ partials, int nparts,
+                                                            const int* __restrict__ active) {
+  const int pb = blockIdx.y;
+  if (active && !active[pb]) return;
+  const float al = (float)alpha[pb];
+  float4* px = x + pb * vp;
+  float4* pr = r + pb * vp;
+  const float4* pp = p + pb * vp;
+  const float4* pq = q + pb * vp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len4;
+       i += (long long)gridDim.x * blockDim.x) {
+    float4 xv = px[i], rv = pr[i];
+    const float4 pv = __ldg(pp + i), qv = __ldg(pq + i);
+    xv.x += al * pv.x; xv.y += al * pv.y; xv.z += al * pv.z; xv.w += al * pv.w;
+    rv.x -= al * qv.x; rv.y -= al * qv.y; rv.z -= al * qv.z; rv.w -= al * qv.w;
+    px[i] = xv;
+    pr[i] = rv;
+    acc += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y + (double)rv.z * (double)rv.z +
+           (double)rv.w * (double)rv.w;
+  }
+  block_reduce_store(acc, partials + (long long)pb * nparts, blockIdx.x);
+}
+
+int launch_cg_update(float* x, float* r, const float* p, const float* q, long long vp, long long len,
+                     const double* alpha, int nprob, double* partials, int stride, const int* active,
+                     cudaStream_t s) {
+  if ((len & 3) || (vp & 3) || !aligned16(x) || !aligned16(r) || !aligned16(p) || !aligned16(q))
+    return (int)cudaErrorInvalidValue;
+  dim3 grid(dot_partials(len), nprob);
+  k_cg_update<<<grid, kRedThreads, 0, s>>>(reinterpret_cast<float4*>(x), reinterpret_cast<float4*>(r),
+                                            reinterpret_cast<const float4*>(p), reinterpret_cast<const float4*>(q),
+                                            vp / 4, len / 4, alpha, partials, stride, active);
+  return (int)cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_diff_sumsq(const float* __restrict__ a, long long ap,
@@ -66,7 +127,12 @@ int launch_finalize(const double* partials, int stride, int count, double* out, 
 int launch_dot(const float* a, long long ap, const float* b, long long bp, long long len, int nprob,
                double* partials, int stride, const int* active, cudaStream_t s) {
   dim3 grid(dot_partials(len), nprob);
-  k_dot<<<grid, kRedThreads, 0, s>>>(a, ap, b, bp, len, partials, stride, active);
+  if (!(len & 3) && !(ap & 3) && !(bp & 3) && aligned16(a) && aligned16(b))
+    k_dot4<<<grid, kRedThreads, 0, s>>>(reinterpret_cast<const float4*>(a), ap / 4,
+                                        reinterpret_cast<const float4*>(b), bp / 4, len / 4, partials, stride,
+                                        active);
+  else
+    k_dot<<<grid, kRedThreads, 0, s>>>(a, ap, b, bp, len, partials, stride, active);
   return (int)cudaGetLastError();
 }
 
@@ -98,9 +164,45 @@ __global__ void k_lincomb(float* y, long long yp, const float* a, long long ap,
   }
 }
 
+// float4 form of k_lincomb
+__global__ void k_lincomb4(float4* y, long long yp, const float4* a, long long ap, const double* __restrict__ ca,
+                           double sa, const float4* b, long long bp, const double* __restrict__ cb, double sb,
+                           long long len4, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const float fa = (float)(sa * (ca ? ca[p] : 1.0));
+  const float fb = b ? (float)(sb * (cb ? cb[p] : 1.0)) : 0.f;
+  float4* py = y + p * yp;
+  const float4* pa = a + p * ap;
+  const float4* pb = b ? b + p * bp : nullptr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len4;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float4 u = pa[i];
+    float4 v = make_float4(fa * u.x, fa * u.y, fa * u.z, fa * u.w);
+    if (pb) {
+      const float4 w = pb[i];
+      v.x += fb * w.x;
+      v.y += fb * w.y;
+      v.z += fb * w.z;
+      v.w += fb * w.w;
+    }
+    py[i] = v;
+  }
+}
+
 int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
                    const float* b, long long bp, const double* cb, double sb, long long len,
                    int nprob, const int* active, cudaStream_t s) {
+  if (!(len & 3) && !(yp & 3) && !(ap & 3) && (!b || !(bp & 3)) && aligned16(y) && aligned16(a) &&
+      (!b || aligned16(b))) {
+    long long blocks = (len / 4 + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    dim3 grid((unsigned)blocks, nprob);
+    k_lincomb4<<<grid, 256, 0, s>>>(reinterpret_cast<float4*>(y), yp / 4, reinterpret_cast<const float4*>(a),
+                                    ap / 4, ca, sa, reinterpret_cast<const float4*>(b), bp / 4, cb, sb, len / 4,
+                                    active);
+    return (int)cudaGetLastError();
+  }
   long long blocks = (len + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
   dim3 grid((unsigned)blocks, nprob);

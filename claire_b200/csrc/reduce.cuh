@@ -6,6 +6,8 @@
 // problem gives the same numbers alone and inside a batch.
 #pragma once
 
+#include <stdint.h>
+
 #include "common.cuh"
 
 namespace cb {
@@ -45,6 +47,12 @@ int dot_partials(long long len);
 // (FP32 inputs, FP64 sums).  Inactive problems are skipped.
 int launch_dot(const float* a, long long ap, const float* b, long long bp, long long len, int nprob,
                double* partials, int stride, const int* active, cudaStream_t s);
+
+// PCG update of problem p: x += alpha[p] p, r -= alpha[p] q; partials of the new
+// r.r in the dot layout.  len % 4 == 0 and 16-byte aligned vectors (vp apart).
+int launch_cg_update(float* x, float* r, const float* p, const float* q, long long vp, long long len,
+                     const double* alpha, int nprob, double* partials, int stride, const int* active,
+                     cudaStream_t s);
 
 // same layout, partial sums of (a[p][i] - b[p][i])^2
 int launch_diff_sumsq(const float* a, long long ap, const float* b, long long bp, long long len,

@@ -446,9 +446,20 @@ int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
 // ---------------------------------------------------------------------------
 // spectral building blocks
 // ---------------------------------------------------------------------------
-int Solver::reg_op(const float* vin, float* out, int op, int epi, const int* act) {
+// out = F^-1(symbol F(vin)) with epilogue epi; with dot_with, out . dot_with
+// (FP64) lands in slot dot_slot (the inverse transform's epilogue sums it).
+int Solver::reg_op(const float* vin, float* out, int op, int epi, const int* act, const float* dot_with,
+                   int dot_slot) {
   CB_TRY(launch_r2c3d(vin, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
   CB_TRY(launch_pencil(spec, 3 * nc, B, d, op, dparams, 3, 3, act, stream));
+  if (dot_with) {
+    const int e2 = (epi == EPI_ADD) ? EPI_ADD_DOT : EPI_STORE_DOT;
+    CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, e2, nullptr, partials, maxparts, act, stream,
+                        dot_with));
+    CB_TRY(launch_finalize(partials, maxparts, c2r_partials(d, 3), slot(dot_slot), B, 1.0, false, stream));
+    note_launches(6);
+    return 0;
+  }
   CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, epi, nullptr, nullptr, 0, act, stream));
   note_launches(5);
   return 0;
@@ -504,17 +515,18 @@ int Solver::adjoint_sweep(float* bout, const int* act) {
 // out = Reg.EvaluateGradient(vin) + body force (src/CLAIRE.cpp:1356-1361,
 // 1015-1042).  Without a projection the body force is written into out first
 // and the regularisation's inverse transform accumulates into it.
-int Solver::finish_with_reg(const float* vin, float* out, const int* act) {
+int Solver::finish_with_reg(const float* vin, float* out, const int* act, const float* dot_with, int dot_slot) {
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
   if (!proj) {
     CB_TRY(adjoint_sweep(out, act));
-    CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_ADD, act));
+    CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_ADD, act, dot_with, dot_slot));
     return 0;
   }
   CB_TRY(adjoint_sweep(bf, act));
   CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_STORE, act));
   CB_TRY(launch_lincomb(out, 3 * n, out, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
   note_launches(1);
+  if (dot_with) CB_TRY(dot(out, 3 * n, dot_with, 3 * n, 3 * n, dot_slot, act));
   return 0;
 }
 
@@ -544,7 +556,7 @@ int Solver::hessian_prep(const int* act) {
 // GN Hessian matvec (src/CLAIRE.cpp:1311-1379, 3147-3290, 3307-3490, 3849-4012).
 // m~^0 = 0, so m~^1 = s_0; steps j = 1 .. nt-1 gather; the last one writes
 // lambda~(t=1) = -m~(t=1) straight into the adjoint's level nt.
-int Solver::hessian(const float* vin, float* hout, const int* act) {
+int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) {
   const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n, PL = (nt + 1) * n, PS = nt * n;
   CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, tab_st, TP, vtx, 3 * n, n, 3, B, d, act, stream));
   CB_TRY(launch_incstate_source(gx, PGX, vtx, 3 * n, gm, PGM, vin, 3 * n, sj, PS, nt, ht, B, n, act, stream));
@@ -568,7 +580,7 @@ int Solver::hessian(const float* vin, float* hout, const int* act) {
     cp = n;
   }
   note_launches(nt - 1);
-  CB_TRY(finish_with_reg(vin, hout, act));
+  CB_TRY(finish_with_reg(vin, hout, act, pq_slot >= 0 ? vin : nullptr, pq_slot));
   return 0;
 }
 
@@ -656,13 +668,14 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   CB_TRY(dot(r, 3 * n, r, 3 * n, 3 * n, S_RR, act));
   k_pcg_init<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, opts.krylovtol[1]);
   note_launches(1);
-  auto apply_pc = [&]() -> int {
-    if (opts.precond) return reg_op(r, z, OP_REG_INV, EPI_STORE, act);
+  // z = P r and r.z into slot s (the inverse transform's epilogue sums it)
+  auto apply_pc = [&](int s) -> int {
+    if (opts.precond) return reg_op(r, z, OP_REG_INV, EPI_STORE, act, r, s);
     note_launches(1);
-    return launch_lincomb(z, 3 * n, r, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream);
+    CB_TRY(launch_lincomb(z, 3 * n, r, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+    return dot(r, 3 * n, z, 3 * n, 3 * n, s, act);
   };
-  CB_TRY(apply_pc());
-  CB_TRY(dot(r, 3 * n, z, 3 * n, 3 * n, S_RZ, act));
+  CB_TRY(apply_pc(S_RZ));
   CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
   note_launches(1);
   std::vector<int> hact(B);
@@ -681,19 +694,17 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
         ps[b].hess_matvecs++;
       }
     if (!any || maxit == 0) break;
-    CB_TRY(hessian(pv, q, act));
-    CB_TRY(dot(pv, 3 * n, q, 3 * n, 3 * n, S_PQ, act));
+    CB_TRY(hessian(pv, q, act, S_PQ));  // q = H p and p.q
     k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
-    CB_TRY(launch_lincomb(x, 3 * n, x, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_ALPHA), 1.0, 3 * n, B, act, stream));
-    CB_TRY(launch_lincomb(r, 3 * n, r, 3 * n, nullptr, 1.0, q, 3 * n, slot(S_ALPHA), -1.0, 3 * n, B, act, stream));
+    // x += alpha p, r -= alpha q and the new r.r in one pass
+    CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
+    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream));
     note_launches(3);
-    CB_TRY(dot(r, 3 * n, r, 3 * n, 3 * n, S_RR, act));
     k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
     note_launches(1);
-    CB_TRY(apply_pc());
+    CB_TRY(apply_pc(S_RZNEW));
     for (int b = 0; b < B; ++b)
       if (hact[b]) ps[b].pc_matvecs++;
-    CB_TRY(dot(r, 3 * n, z, 3 * n, 3 * n, S_RZNEW, act));
     k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
     CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
     note_launches(2);

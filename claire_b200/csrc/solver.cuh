@@ -114,15 +114,17 @@ class Solver {
   int state_solve(const float* vel, const int* act);
   int distance(const int* act);
   int reg_functional(const float* vel, const std::vector<int>& sel, const int* act);
-  int reg_op(const float* vin, float* out, int op, int epi, const int* act);
+  int reg_op(const float* vin, float* out, int op, int epi, const int* act, const float* dot_with = nullptr,
+             int dot_slot = -1);
   int grad_fields(const float* f, long long fp, long long ifs, float* out, long long op,
                   long long ofs, int nf, const int* act);
   int divergence(const float* vel, float* out, const int* act);
   int adjoint_sweep(float* bout, const int* act);
-  int finish_with_reg(const float* vin, float* out, const int* act);
+  int finish_with_reg(const float* vin, float* out, const int* act, const float* dot_with = nullptr,
+                      int dot_slot = -1);
   int gradient(const int* act);
   int hessian_prep(const int* act);
-  int hessian(const float* vin, float* hout, const int* act);
+  int hessian(const float* vin, float* hout, const int* act, int pq_slot = -1);
   int pcg(const std::vector<int>& sel, double maxit);
   int line_search(std::vector<int>& sel);
   int dot(const float* a, long long ap, const float* b, long long bp, long long len, int slot,

@@ -32,7 +32,9 @@ struct SpecParams {
 };
 
 // Epilogue of the inverse row pass.
-enum Epi : int { EPI_STORE = 0, EPI_ADD = 1, EPI_SUMSQ = 2 };
+// Epilogues of the inverse transforms: store, accumulate, sum of squares, or
+// store / accumulate and sum out * other (FP64 partials, c2r only).
+enum Epi : int { EPI_STORE = 0, EPI_ADD = 1, EPI_SUMSQ = 2, EPI_STORE_DOT = 3, EPI_ADD_DOT = 4 };
 
 struct Batch {
   int nprob;              // problems in the launch
@@ -50,7 +52,7 @@ int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
 // Inverse c2r of nf fields with epilogue: out[p*op + f*ofs] = alpha[p]*x (+ out) or sumsq.
 int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long long ofs, int nf,
                  int nprob, const Dims& d, int epi, const float* alpha, double* partials, int nparts,
-                 const int* active, cudaStream_t s);
+                 const int* active, cudaStream_t s, const float* other = nullptr);
 
 // Spectral first derivative along one axis (0:x1, 1:x2, 2:x3) of nf real
 // fields with Nyquist set to zero; out = d/dx_axis in (+ out) or sumsq.
