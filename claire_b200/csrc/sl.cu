@@ -60,41 +60,42 @@ struct TrajectoryEpi {
   }
 };
 
+// Epilogues of the table-driven gathers: operator()(tt, a, value, aux_a) with
+// aux_a = aux[point] prefetched by the gather (aux may be null).
 struct StoreEpi {
   float* dst;
-  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
+  const float* aux = nullptr;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val, float) const {
     if (tt.valid_idx(a)) dst[tt.idx(a)] = val;
   }
 };
 
-// out = c * val
+// out = c * val (aux = c)
 struct ScaleEpi {
-  const float* c;
   float* out;
-  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
-    if (tt.valid_idx(a)) out[tt.idx(a)] = __ldg(c + tt.idx(a)) * val;
+  const float* aux;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val, float c) const {
+    if (tt.valid_idx(a)) out[tt.idx(a)] = c * val;
   }
 };
 
-// out = sign * (val + src)
+// out = sign * (val + src) (aux = src)
 struct AddEpi {
-  const float* src;
   float* out;
   float sign;
-  CB_DEVICE void operator()(const TileThread& tt, int a, float val) const {
-    if (tt.valid_idx(a)) out[tt.idx(a)] = sign * (val + __ldg(src + tt.idx(a)));
+  const float* aux;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val, float src) const {
+    if (tt.valid_idx(a)) out[tt.idx(a)] = sign * (val + src);
   }
 };
 
-// out = 1 + ht/2 (dx + dv + ht dx dv), dx = divv(X) (the gathered value), dv = divv
+// out = 1 + ht/2 (dx + dv + ht dx dv), dx = divv(X) (the gathered value), dv = divv (aux)
 struct AdjCoefEpi {
-  const float* divv;
   float* out;
   float ht;
-  CB_DEVICE void operator()(const TileThread& tt, int a, float dx) const {
-    if (!tt.valid_idx(a)) return;
-    const float dv = __ldg(divv + tt.idx(a));
-    out[tt.idx(a)] = 1.f + 0.5f * ht * (dx + dv + ht * dx * dv);
+  const float* aux;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float dx, float dv) const {
+    if (tt.valid_idx(a)) out[tt.idx(a)] = 1.f + 0.5f * ht * (dx + dv + ht * dx * dv);
   }
 };
 
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  StoreEpi epi{out + p * op + (long long)blockIdx.z * of};
+  StoreEpi epi{out + p * op + (long long)blockIdx.z * of, nullptr};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp + (long long)blockIdx.z * ff, d, epi);
 }
 
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  ScaleEpi epi{c + p * cp, out + p * op};
+  ScaleEpi epi{out + p * op, c + p * cp};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp, d, epi);
 }
 
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  AddEpi epi{s + p * sp, out + p * op, sign};
+  AddEpi epi{out + p * op, sign, s + p * sp};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp, d, epi);
 }
 
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  AdjCoefEpi epi{divv + p * vp, out + p * op, ht};
+  AdjCoefEpi epi{out + p * op, ht, divv + p * vp};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, divv + p * vp, d, epi);
 }
 

@@ -313,8 +313,9 @@ CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ 
 }
 
 // Tile gather of one field at a displacement field with a precomputed box
-// table: the box copy is issued first and the points' displacements load
-// while it is in flight.
+// table: the box copy is issued first and the points' displacements (and the
+// epilogue's per-point operand epi.aux, when it has one) load while it is in
+// flight; epi(tt, a, value, aux_a) finishes point a.
 template <class Epi>
 CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const int4* __restrict__ tab,
                                const float* __restrict__ f, const Dims& d, const Epi& epi) {
@@ -325,7 +326,7 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
     cp_async_commit();
   }
   const TileThread tt = tile_thread(d);
-  float dd[kTilePts][3];
+  float dd[kTilePts][3], aux[kTilePts];
   const float* d2 = disp + d.n();
   const float* d3 = d2 + d.n();
 #pragma unroll
@@ -335,6 +336,7 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
     dd[a][0] = ok ? __ldg(disp + i) : 0.f;
     dd[a][1] = ok ? __ldg(d2 + i) : 0.f;
     dd[a][2] = ok ? __ldg(d3 + i) : 0.f;
+    aux[a] = (ok && epi.aux) ? __ldg(epi.aux + i) : 0.f;
   }
   if (staged) {
     cp_async_wait_all();
@@ -343,7 +345,7 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
 #pragma unroll
     for (int a = 0; a < kTilePts; ++a) {
       const BoxPoint bp = box_point(dd[a], tt.x1(a), tt, tt.valid_idx(a), bx);
-      epi(tt, a, gather_staged(sbase, bp, bx));
+      epi(tt, a, gather_staged(sbase, bp, bx), aux[a]);
     }
   } else {
 #pragma unroll
@@ -351,7 +353,7 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
       if (!tt.valid_idx(a)) continue;
       Stencil st;
       make_stencil(tt.x1(a), tt.i2, tt.i3, dd[a][0], dd[a][1], dd[a][2], d, st);
-      epi(tt, a, gather(f, st));
+      epi(tt, a, gather(f, st), aux[a]);
     }
   }
 }
