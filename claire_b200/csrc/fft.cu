@@ -62,12 +62,16 @@ bool fft_size_supported(int n) {
 }
 
 // Packed lines per CTA for row kernels, and columns per CTA for column kernels.
+// Lines per CTA.  With 256 threads and at least 32 lines a warp's lanes are
+// 32 consecutive lines at one element index in every radix stage, so the
+// split re / im arrays (odd line pitch) are read and written without bank
+// conflicts; grids of 192 and 256 points use 16 lines to keep two CTAs per SM.
 template <int N> struct RowCfg {
-  static constexpr int P = (2048 / N) > 64 ? 64 : ((2048 / N) >= 32 ? 32 : ((2048 / N) >= 16 ? 16 : 8));
+  static constexpr int P = N <= 32 ? 64 : (N <= 128 ? 32 : 16);
   static constexpr int PITCH = P + 1;
 };
 template <int N> struct ColCfg {
-  static constexpr int C = N >= 192 ? 8 : 16;
+  static constexpr int C = N <= 128 ? 32 : 16;
   static constexpr int PITCH = C + 1;
 };
 
@@ -166,15 +170,21 @@ CB_DEVICE void load_row_chunk(float* re, float* im, const float* __restrict__ sr
     const int r = (4 * q) / N;
     v[k] = (r < nr) ? __ldg(reinterpret_cast<const float4*>(src) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
   }
+  // lane l writes its four elements in the order rotated by l / 8, so the 32
+  // lanes of each store hit 32 distinct banks (e * PITCH strides otherwise
+  // fold four lanes onto one bank)
+  const int rot = (threadIdx.x >> 3) & 3;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int q = threadIdx.x + k * kThreads;
     const int r = (4 * q) / N, e = 4 * q - r * N;
     float* dst = ((r & 1) ? im : re) + (r >> 1);
-    dst[(e + 0) * PITCH] = v[k].x;
-    dst[(e + 1) * PITCH] = v[k].y;
-    dst[(e + 2) * PITCH] = v[k].z;
-    dst[(e + 3) * PITCH] = v[k].w;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = (i + rot) & 3;
+      const float val = c == 0 ? v[k].x : (c == 1 ? v[k].y : (c == 2 ? v[k].z : v[k].w));
+      dst[(e + c) * PITCH] = val;
+    }
   }
 }
 

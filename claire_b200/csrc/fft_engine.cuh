@@ -134,7 +134,7 @@ template <> struct Plan<128> { static constexpr int R0 = 16, R1 = 8; };
 template <> struct Plan<192> { static constexpr int R0 = 12, R1 = 16; };
 template <> struct Plan<256> { static constexpr int R0 = 16, R1 = 16; };
 
-constexpr int kFftThreads = 128;  // threads per CTA of every FFT kernel
+constexpr int kFftThreads = 256;  // threads per CTA of every FFT kernel
 
 template <int N, int R, int NS, bool INV, int NL, int PITCH>
 CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict__ sim,
