@@ -15,6 +15,10 @@
 
 namespace cb {
 
+// Set by a host thread while it records a CUDA graph: launchers skip
+// non-stream calls (function attributes are set by an earlier uncaptured run).
+inline thread_local bool g_graph_capture = false;
+
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 6.28318530717958647692;
 

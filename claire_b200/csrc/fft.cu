@@ -678,7 +678,7 @@ template <int N> static size_t col_smem(int nbuf) {
 }
 
 template <typename K> static int set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) {
+  if (bytes > 48 * 1024 && !g_graph_capture) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return (int)e;
   }

@@ -26,6 +26,7 @@ static dim3 tile_grid(const Dims& d, int nprob, int nz) { return dim3(tile_count
 
 template <typename K>
 static int allow_smem(K kernel) {
+  if (g_graph_capture) return 0;
   return (int)cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kGatherSmemBytes);
 }
 

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "reduce.cuh"
@@ -98,6 +99,7 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 // ---------------------------------------------------------------------------
 Solver::~Solver() {
   prof_clear();
+  if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
   void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
                   r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
@@ -160,6 +162,11 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   }
   n = d.n();
   nc = d.nc();
+  {
+    // CLAIRE_B200_GRAPHS=0 runs PCG iterations as direct launches
+    const char* ge = std::getenv("CLAIRE_B200_GRAPHS");
+    graphs = !(ge && ge[0] == '0');
+  }
   ht = (float)(1.0 / nt);
   hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
   if (cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -679,39 +686,77 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
   note_launches(1);
   std::vector<int> hact(B);
-  for (int b = 0; b < B; ++b)
-    if (sel[b]) ps[b].pc_matvecs++;
-  for (int it = 0; it <= maxit; ++it) {
+  // One PCG iteration.  It reads and writes device data only (vectors, the
+  // per-problem scalars and the active mask, which k_pcg_alpha / k_pcg_check
+  // clear when a problem stops), so it is recorded once as a CUDA graph and
+  // replayed, and several iterations can run between host checks.
+  auto body = [&]() -> int {
+    CB_TRY(hessian(pv, q, act, S_PQ));  // q = H p and p.q
+    k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
+    // x += alpha p, r -= alpha q and the new r.r in one pass
+    CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
+    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream));
+    k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
+    note_launches(4);
+    CB_TRY(apply_pc(S_RZNEW));
+    k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
+    CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
+    note_launches(2);
+    return 0;
+  };
+  auto run_body = [&]() -> int {
+    if (!graphs || prof_on) return body();
+    if (!pcg_exec) {
+      if (!pcg_warm) {  // first run uncaptured: sets function attributes, builds FFT tables
+        pcg_warm = true;
+        return body();
+      }
+      const long long l0 = launches();
+      g_graph_capture = true;
+      cudaError_t ce = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+      int e = ce == cudaSuccess ? body() : CB_ERR_CUDA;
+      cudaGraph_t gr = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(stream, &gr);
+      g_graph_capture = false;
+      pcg_exec_launches = launches() - l0;
+      if (!e && ee == cudaSuccess && gr && cudaGraphInstantiate(&pcg_exec, gr, 0) != cudaSuccess) pcg_exec = nullptr;
+      if (gr) cudaGraphDestroy(gr);
+      if (e || ee != cudaSuccess || !pcg_exec) {
+        cudaGetLastError();
+        graphs = false;  // fall back to direct launches for this solver
+        return body();
+      }
+      // the recorded launches were not executed: replay them now
+    }
+    note_launches(pcg_exec_launches);
+    return cudaGraphLaunch(pcg_exec, stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+  };
+  constexpr int kItersPerCheck = 2;
+  int launched = 0;
+  while (true) {
     cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream);
     if (cudaStreamSynchronize(stream) != cudaSuccess) {
       err = "device error in PCG";
       return CB_ERR_CUDA;
     }
     bool any = false;
-    for (int b = 0; b < B; ++b)
-      if (hact[b]) {
-        any = true;
-        ps[b].hess_matvecs++;
-      }
-    if (!any || maxit == 0) break;
-    CB_TRY(hessian(pv, q, act, S_PQ));  // q = H p and p.q
-    k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
-    // x += alpha p, r -= alpha q and the new r.r in one pass
-    CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
-    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream));
-    note_launches(3);
-    k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
-    note_launches(1);
-    CB_TRY(apply_pc(S_RZNEW));
-    for (int b = 0; b < B; ++b)
-      if (hact[b]) ps[b].pc_matvecs++;
-    k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
-    CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
-    note_launches(2);
+    for (int b = 0; b < B; ++b) any |= hact[b] != 0;
+    if (!any || launched >= maxit) break;
+    for (int k = 0; k < kItersPerCheck && launched < maxit; ++k, ++launched) CB_TRY(run_body());
   }
   CB_TRY(fetch_scalars());
-  for (int b = 0; b < B; ++b)
-    if (sel[b]) ps[b].pcg_total += hint[I_IT * B + b];
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    // Hessian applications: every iteration a problem entered active; an
+    // iteration that stopped on indefinite curvature applied it without
+    // counting; the preconditioner ran once up front and after every
+    // iteration that did not stop
+    const int its = hint[I_IT * B + b], reason = hint[I_REASON * B + b];
+    const bool stopped_at_check = reason == 1 || reason == 2 || reason == 4;
+    ps[b].hess_matvecs += its + (reason == 3 ? 1 : 0);
+    ps[b].pc_matvecs += 1 + its - (stopped_at_check ? 1 : 0);
+    ps[b].pcg_total += its;
+  }
   return 0;
 }
 

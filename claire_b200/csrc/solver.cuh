@@ -93,6 +93,12 @@ class Solver {
   // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
   std::vector<int> state_of;
 
+  // PCG iteration recorded as a CUDA graph (built on the second iteration the
+  // solver runs; graphs = false switches replay off)
+  bool graphs = true, pcg_warm = false;
+  cudaGraphExec_t pcg_exec = nullptr;
+  long long pcg_exec_launches = 0;
+
   // device timers per category (CB_PROF_*): event pairs recorded around launches
   bool prof_on = false;
   std::vector<cudaEvent_t> prof_ev[CB_PROF_NCAT];
