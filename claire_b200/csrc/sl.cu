@@ -175,8 +175,7 @@ __global__ void __launch_bounds__(kTileThreads)
   tile_bounds(dd, tt, lo, hi);
   if (threadIdx.x == 0) {
     int4* t = tab + p * tp + 2 * blockIdx.x;
-    t[0] = make_int4(lo[0], lo[1], lo[2], hi[0]);
-    t[1] = make_int4(hi[1], hi[2], 0, 0);
+    pack_box(box_from_bounds(lo, hi, d), t[0], t[1]);
   }
 }
 

@@ -177,14 +177,29 @@ CB_DEVICE TileBox tile_box(const float (&dd)[kTilePts][3], const TileThread& tt,
   return box_from_bounds(lo, hi, d);
 }
 
-// Per-tile box table of a displacement field: two int4 per tile,
-// {lo1, lo2, lo3, hi1}, {hi2, hi3, 0, 0} of the stencil bases.  It depends on
-// the displacement only, so one table serves every gather at that
+// Per-tile box table of a displacement field: the tile's TileBox packed in two
+// int4, {lo1, lo2, lo3, e1 | e2 << 16}, {e3 | P << 16, Q, vol, within}.  It
+// depends on the displacement only, so one table serves every gather at that
 // characteristic (all time steps, all matvecs of a GN iterate).
-CB_DEVICE TileBox box_from_table(const int4* __restrict__ tab, const Dims& d) {
+CB_DEVICE void pack_box(const TileBox& bx, int4& a, int4& b) {
+  a = make_int4(bx.lo[0], bx.lo[1], bx.lo[2], (bx.e1 & 0xffff) | (bx.e2 << 16));
+  b = make_int4((bx.e3 & 0xffff) | (bx.P << 16), bx.Q, bx.vol, bx.within ? 1 : 0);
+}
+
+CB_DEVICE TileBox box_from_table(const int4* __restrict__ tab, const Dims&) {
   const int4 a = __ldg(tab + 2 * blockIdx.x), b = __ldg(tab + 2 * blockIdx.x + 1);
-  const int lo[3] = {a.x, a.y, a.z}, hi[3] = {a.w, b.x, b.y};
-  return box_from_bounds(lo, hi, d);
+  TileBox bx;
+  bx.lo[0] = a.x;
+  bx.lo[1] = a.y;
+  bx.lo[2] = a.z;
+  bx.e1 = a.w & 0xffff;
+  bx.e2 = a.w >> 16;
+  bx.e3 = b.x & 0xffff;
+  bx.P = b.x >> 16;
+  bx.Q = b.y;
+  bx.vol = b.z;
+  bx.within = b.w != 0;
+  return bx;
 }
 
 CB_DEVICE void cp_async16(float* smem_dst, const float* gmem_src) {
@@ -199,28 +214,33 @@ CB_DEVICE void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" :::
 // incrementally, without divisions.  The box never exceeds the grid along an
 // axis, so one conditional subtraction wraps each coordinate.
 CB_DEVICE void issue_box(float* __restrict__ sb, const float* __restrict__ f, const TileBox& bx, const Dims& d) {
+  // warp w copies x1 planes w, w + 8, ...; its lanes cover rpi rows of nck
+  // 16-byte chunks at a time; pointers advance by whole rows, with one
+  // conditional wrap per row along x2 and per plane along x1
   const int nck = bx.e3 >> 2;           // 16-byte chunks per row, 1 .. 16
   const int rpi = small_div(32, nck);   // rows a warp copies per step
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lr = small_div(lane, nck), lc = lane - lr * nck;
-  if (lr >= rpi) return;
-  const int w1 = wrap_near(bx.lo[0], d.n1), w2 = wrap_near(bx.lo[1], d.n2);
+  if (lr >= rpi || lr >= bx.e2) return;
+  int g1 = wrap_near(bx.lo[0] + warp, d.n1);
+  const int w2 = wrap_near(bx.lo[1] + lr, d.n2);
   int g3 = wrap_near(bx.lo[2], d.n3) + 4 * lc;
   g3 -= (g3 >= d.n3) ? d.n3 : 0;
   const float* fb = f + g3;
-  const int rstep = rpi * (kTileThreads / 32);
-  const int r0 = warp * rpi + lr;
-  int l1 = small_div(r0, bx.e2), l2 = r0 - l1 * bx.e2;
-  while (l1 < bx.e1) {
-    int g1 = w1 + l1, g2 = w2 + l2;
-    g1 -= (g1 >= d.n1) ? d.n1 : 0;
-    g2 -= (g2 >= d.n2) ? d.n2 : 0;
-    cp_async16(sb + l1 * bx.Q + l2 * bx.P + 4 * lc, fb + ((unsigned)g1 * (unsigned)d.n2 + (unsigned)g2) * (unsigned)d.n3);
-    l2 += rstep;
-    while (l2 >= bx.e2) {
-      l2 -= bx.e2;
-      ++l1;
+  const unsigned row = (unsigned)d.n3, plane = (unsigned)d.n2 * (unsigned)d.n3;
+  constexpr int kWarps = kTileThreads / 32;
+  for (int l1 = warp; l1 < bx.e1; l1 += kWarps) {
+    const float* fp = fb + (unsigned)g1 * plane;
+    float* sp = sb + l1 * bx.Q + lr * bx.P + 4 * lc;
+    int g2 = w2;
+    for (int l2 = lr; l2 < bx.e2; l2 += rpi) {
+      cp_async16(sp, fp + (unsigned)g2 * row);
+      sp += rpi * bx.P;
+      g2 += rpi;
+      while (g2 >= d.n2) g2 -= d.n2;
     }
+    g1 += kWarps;
+    g1 -= (g1 >= d.n1) ? d.n1 : 0;
   }
 }
 
