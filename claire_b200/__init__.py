@@ -130,6 +130,7 @@ _signatures = {
     "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_kernel_launches": (ctypes.c_longlong, []),
     "claire_b200_profile": (_I, [_P, _I]),
+    "claire_b200_det_def_grad": (_I, [_P, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "claire_b200_server_default_opts": (None, [_P]),
     "claire_b200_server_create": (_I, [_P, ctypes.POINTER(_P)]),
     "claire_b200_server_submit": (_I, [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_longlong)]),
@@ -360,6 +361,16 @@ class CLAIREInterface:
         _check(lib.claire_b200_forward(self._ctx, b, p, out.ctypes.data_as(ctypes.c_void_p), 0),
                "SolveForwardProblem", self._ctx)
         return out
+
+    def ComputeDetDefGrad(self, b: int = 0, inverse: bool = False):
+        """det(grad y) at the current velocity (DeformationFields::ComputeDetDefGrad, SL
+        solver): (J as a host array, (min, mean, max))."""
+        import numpy as np
+        jac = np.empty(tuple(self.shape), dtype=np.float32)
+        st = (ctypes.c_double * 3)()
+        _check(lib.claire_b200_det_def_grad(self._ctx, b, int(bool(inverse)), jac.ctypes.data_as(ctypes.c_void_p), st),
+               "ComputeDetDefGrad", self._ctx)
+        return jac, (st[0], st[1], st[2])
 
     def profile(self, enable: bool = True) -> None:
         """Bracket every time-step kernel launch with CUDA events (instrumented runs)."""

@@ -333,6 +333,23 @@ int claire_b200_precond(claire_b200_ctx* c, int b, const float* xin, float* px) 
   return copy_out(s, px, s.z + b * 3 * s.n, 3 * s.n, 0);
 }
 
+int claire_b200_det_def_grad(claire_b200_ctx* c, int b, int inverse, float* jac, double stats[3]) {
+  if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  std::vector<double> st;
+  int e = s.det_def_grad(sel, inverse != 0, st);
+  if (e) return cuda_status(e);
+  if (stats) {
+    stats[0] = st[3 * b];
+    stats[1] = st[3 * b + 1];
+    stats[2] = st[3 * b + 2];
+  }
+  if (jac) return copy_out(s, jac, s.work3 + b * 3 * s.n, s.n, 0);
+  return CB_OK;
+}
+
 int claire_b200_get_adjoint(claire_b200_ctx* c, int b, float* lambda0, float* body_force) {
   if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

@@ -190,6 +190,22 @@ __global__ void k_lincomb4(float4* y, long long yp, const float4* a, long long a
   }
 }
 
+__global__ void k_fill(float* y, long long yp, float value, long long len, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  float* py = y + p * yp;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x)
+    py[i] = value;
+}
+
+int launch_fill(float* y, long long yp, float value, long long len, int nprob, const int* active, cudaStream_t s) {
+  long long blocks = (len + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_fill<<<dim3((unsigned)blocks, nprob), 256, 0, s>>>(y, yp, value, len, active);
+  return (int)cudaGetLastError();
+}
+
 int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
                    const float* b, long long bp, const double* cb, double sb, long long len,
                    int nprob, const int* active, cudaStream_t s) {

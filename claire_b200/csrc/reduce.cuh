@@ -54,6 +54,9 @@ int launch_cg_update(float* x, float* r, const float* p, const float* q, long lo
                      const double* alpha, int nprob, double* partials, int stride, const int* active,
                      cudaStream_t s);
 
+// y[p][i] = value, i < len
+int launch_fill(float* y, long long yp, float value, long long len, int nprob, const int* active, cudaStream_t s);
+
 // same layout, partial sums of (a[p][i] - b[p][i])^2
 int launch_diff_sumsq(const float* a, long long ap, const float* b, long long bp, long long len,
                       int nprob, double* partials, int stride, const int* active, cudaStream_t s);

@@ -90,15 +90,59 @@ struct AddEpi {
   }
 };
 
-// out = 1 + ht/2 (dx + dv + ht dx dv), dx = divv(X) (the gathered value), dv = divv (aux)
+// out = 1 + ht/2 (s dx + s dv + ht dx dv), dx = divv(X) (the gathered value),
+// dv = divv (aux), s = +-1
 struct AdjCoefEpi {
   float* out;
-  float ht;
+  float ht, sgn;
   const float* aux;
   CB_DEVICE void operator()(const TileThread& tt, int a, float dx, float dv) const {
-    if (tt.valid_idx(a)) out[tt.idx(a)] = 1.f + 0.5f * ht * (dx + dv + ht * dx * dv);
+    if (tt.valid_idx(a)) out[tt.idx(a)] = 1.f + 0.5f * ht * (sgn * (dx + dv) + ht * dx * dv);
   }
 };
+
+// per-problem partials of sum, min and max of a scalar field (FP64 sum)
+__global__ void __launch_bounds__(256) k_field_stats(const float* __restrict__ f, long long fp, long long n,
+                                                     double* __restrict__ out, int nparts) {
+  const float* pf = f + blockIdx.y * fp;
+  double s = 0.0;
+  float mn = INFINITY, mx = -INFINITY;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float x = pf[i];
+    s += (double)x;
+    mn = fminf(mn, x);
+    mx = fmaxf(mx, x);
+  }
+  __shared__ double ss[8];
+  __shared__ float smn[8], smx[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    ss[w] = s;
+    smn[w] = mn;
+    smx[w] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s = ss[0];
+    mn = smn[0];
+    mx = smx[0];
+    for (int k = 1; k < 8; ++k) {
+      s += ss[k];
+      mn = fminf(mn, smn[k]);
+      mx = fmaxf(mx, smx[k]);
+    }
+    double* o = out + (long long)blockIdx.y * 3 * nparts;
+    o[blockIdx.x] = s;
+    o[nparts + blockIdx.x] = mn;
+    o[2 * nparts + blockIdx.x] = mx;
+  }
+}
 
 // ---- gather kernels (grid: tiles x problems x fields) -------------------------
 
@@ -153,12 +197,12 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
 
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
     k_adjoint_coef(const float* __restrict__ divv, long long vp, const float* __restrict__ disp, long long dp,
-                   const int4* __restrict__ tab, long long tp, float* __restrict__ out, long long op, float ht, Dims d,
-                   const int* __restrict__ active) {
+                   const int4* __restrict__ tab, long long tp, float* __restrict__ out, long long op, float ht,
+                   float sgn, Dims d, const int* __restrict__ active) {
   const int p = blockIdx.y;
   if (active && !active[p]) return;
   extern __shared__ __align__(16) float sbuf[];
-  AdjCoefEpi epi{out + p * op, ht, divv + p * vp};
+  AdjCoefEpi epi{out + p * op, ht, sgn, divv + p * vp};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, divv + p * vp, d, epi);
 }
 
@@ -295,11 +339,11 @@ int launch_gather_add(const float* f, long long fp, const float* disp, long long
 
 int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, const int4* tab,
                         long long tp, float* out, long long op, float ht, int nprob, const Dims& d,
-                        const int* active, cudaStream_t s) {
+                        const int* active, cudaStream_t s, float sgn) {
   int e = allow_smem(k_adjoint_coef);
   if (e) return e;
   k_adjoint_coef<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(divv, vp, disp, dp, tab, tp, out,
-                                                                                op, ht, d, active);
+                                                                                op, ht, sgn, d, active);
   return (int)cudaGetLastError();
 }
 
@@ -321,6 +365,21 @@ int launch_incstate_source(const float* gx, long long gxp, const float* vtx, lon
   if (n % 4) return (int)cudaErrorInvalidValue;
   k_incstate_source<<<quad_grid(n, nprob), kSlThreads, 0, s>>>(gx, gxp, vtx, vtxp, gm, gmp, vt, vtp, src, sp, nt,
                                                                ht, n, active);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace cb
+
+namespace cb {
+
+int field_stats_parts(long long n) {
+  const long long b = (n + 256 * 8 - 1) / (256 * 8);
+  return (int)(b < 296 ? (b < 1 ? 1 : b) : 296);
+}
+
+int launch_field_stats(const float* f, long long fp, long long n, int nprob, double* partials, cudaStream_t s) {
+  const int np = field_stats_parts(n);
+  k_field_stats<<<dim3(np, nprob), 256, 0, s>>>(f, fp, n, partials, np);
   return (int)cudaGetLastError();
 }
 

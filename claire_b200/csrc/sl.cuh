@@ -109,9 +109,15 @@ int launch_gather_add(const float* f, long long fp, const float* disp, long long
 // RK2 adjoint step factor: with dx = divv(X) and dv = divv,
 //   lx + ht/2 (rhs0 + rhs1), rhs0 = lx dx, rhs1 = (lx + ht rhs0) dv
 // equals lx * (1 + ht/2 (dx + dv + ht dx dv)); out = that factor.
+// sgn -1: the factor of det(grad(inv(y))) (src/DeformationFields.cpp:686-712)
 int launch_adjoint_coef(const float* divv, long long vp, const float* disp, long long dp, const int4* tab,
                         long long tp, float* out, long long op, float ht, int nprob, const Dims& d,
-                        const int* active, cudaStream_t s);
+                        const int* active, cudaStream_t s, float sgn = 1.f);
+
+// partials[p][0..3*np): np sums, np minima, np maxima of f[p] (n values);
+// np = field_stats_parts(n)
+int field_stats_parts(long long n);
+int launch_field_stats(const float* f, long long fp, long long n, int nprob, double* partials, cudaStream_t s);
 
 // Trapezoid body force over the stored adjoint levels (src/CLAIRE.cpp:2646-2709):
 //   b[k] = scale * sum_l w_l lam^l (d/dx_k m^l),  w_0 = w_nt = ht/2, else ht.

@@ -123,6 +123,7 @@ static int max_parts(const Dims& d) {
   int mp = dot_partials(3 * d.n());
   for (int a = 0; a < 3; ++a) mp = std::max(mp, deriv_partials(d, a, 3));
   mp = std::max(mp, c2r_partials(d, 3));
+  mp = std::max(mp, 3 * field_stats_parts(d.n()));
   return mp;
 }
 
@@ -588,6 +589,57 @@ int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) 
   }
   note_launches(nt - 1);
   CB_TRY(finish_with_reg(vin, hout, act, pq_slot >= 0 ? vin : nullptr, pq_slot));
+  return 0;
+}
+
+// det(grad y) (inverse: det(grad(inv(y)))) of the selected problems at their
+// velocity v by the SL scheme of DeformationFields::ComputeDetDefGradSL
+// (src/DeformationFields.cpp:636-739): J^0 = 1, J^{j+1} = c J^j(X_state) with
+// the RK2 factor c of the signed divergence terms.  J lands in the first n
+// floats of each problem's work3 block; stats[b] = (min, mean, max).
+int Solver::det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<double>& stats) {
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(characteristic(v, 1.f, dact));
+  CB_TRY(divergence(v, divv, dact));
+  float* c = work3 + n;      // step factor
+  float* j0 = work3;         // J (final result)
+  float* j1 = work3 + 2 * n; // ping-pong buffer
+  CB_TRY(launch_adjoint_coef(divv, n, disp_st, 3 * n, tab_st, TP, c, 3 * n, ht, B, d, dact, stream,
+                             inverse ? -1.f : 1.f));
+  CB_TRY(launch_fill(j0, 3 * n, 1.f, n, B, dact, stream));  // J^0 = 1 (:336)
+  float* cur = j0;
+  float* nxt = j1;
+  for (int j = 0; j < nt; ++j) {
+    CB_TRY(launch_gather_scale(cur, 3 * n, disp_st, 3 * n, tab_st, TP, c, 3 * n, nxt, 3 * n, B, d, dact, stream));
+    std::swap(cur, nxt);
+  }
+  if (cur != j0) CB_TRY(launch_lincomb(j0, 3 * n, cur, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact,
+                                       stream));
+  note_launches(nt + 5);
+  // the state characteristic now belongs to v: cached state levels are stale
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) state_of[b] = 0;
+  const int np = field_stats_parts(n);
+  CB_TRY(launch_field_stats(j0, 3 * n, n, B, partials, stream));
+  note_launches(1);
+  std::vector<double> h((size_t)3 * np * B);
+  if (cudaMemcpyAsync(h.data(), partials, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return CB_ERR_CUDA;
+  stats.assign((size_t)3 * B, 0.0);
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    const double* pp = h.data() + (size_t)3 * np * b;
+    double sum = 0.0, mn = pp[np], mx = pp[2 * np];
+    for (int k = 0; k < np; ++k) {
+      sum += pp[k];
+      mn = std::min(mn, pp[np + k]);
+      mx = std::max(mx, pp[2 * np + k]);
+    }
+    stats[3 * b] = mn;
+    stats[3 * b + 1] = sum / (double)n;
+    stats[3 * b + 2] = mx;
+  }
   return 0;
 }
 

@@ -52,6 +52,7 @@ class Solver {
   int hessian_matvec(const float* vin, float* hout, const std::vector<int>& sel);
   int precond(const float* rin, float* zout, const std::vector<int>& sel);
   int forward(const float* m0, float* m1, const std::vector<int>& sel);
+  int det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<double>& stats);
   int final_state(float* m1, int b);
   int set_problem(int b, const claire_b200_opts& o);
   long long footprint() const { return bytes_; }

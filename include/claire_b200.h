@@ -116,6 +116,12 @@ int claire_b200_gradient(claire_b200_ctx* ctx, int b, const float* v, float* g);
 int claire_b200_hessian_matvec(claire_b200_ctx* ctx, int b, const float* v, const float* vt, float* hvt);
 /* Preconditioner::MatVec (INVREG): P x = (beta A)^-1 x (src/Preconditioner.cpp:549-580). */
 int claire_b200_precond(claire_b200_ctx* ctx, int b, const float* x, float* px);
+/* det(grad y) of problem b at its current velocity (inverse != 0:
+ * det(grad(inv(y)))), DeformationFields::ComputeDetDefGrad with the SL solver
+ * (src/DeformationFields.cpp:315-388, 636-739; CLAIREInterface::ComputeDetDefGrad,
+ * include/CLAIREInterface.hpp:42-90).  jac (host, n floats) may be NULL;
+ * stats = {min, mean, max} (the reference's monitor values, :367-375). */
+int claire_b200_det_def_grad(claire_b200_ctx* ctx, int b, int inverse, float* jac, double stats[3]);
 /* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
  * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);

@@ -779,6 +779,28 @@ def forward_transport(mT, v, nt):
     return m
 
 
+def det_def_grad(v, nt, inverse=False):
+    """det(grad y) by the SL scheme of DeformationFields::ComputeDetDefGradSL
+    (src/DeformationFields.cpp:636-739, initial condition 1 at :336): along the
+    state characteristic, jX = J(X); rhs0 = a jX divv(X); rhs1 = a (jX + ht
+    rhs0) divv; J = jX + ht/2 (rhs0 + rhs1), a = -1 for det(grad(inv(y))).
+    Returns (J, (min, mean, max)) as the reference's monitor values (:367-375)."""
+    v = np.asarray(v)
+    shape = v.shape[1:]
+    ht = 1.0 / nt
+    a = -1.0 if inverse else 1.0
+    tr = Trajectory(v, nt, "state")
+    dv = div(v)
+    dvx = tr.interp(dv)
+    jac = np.ones(shape, dtype=v.dtype)
+    for _ in range(nt):
+        jx = tr.interp(jac)
+        rhs0 = a * jx * dvx
+        rhs1 = a * (jx + ht * rhs0) * dv
+        jac = jx + 0.5 * ht * (rhs0 + rhs1)
+    return jac, (float(jac.min()), float(jac.mean()), float(jac.max()))
+
+
 def gaussian_smooth(f: np.ndarray, sigma_cells=1.0) -> np.ndarray:
     """Spectral Gaussian smoothing (src/Preprocessing.cpp:1956-2056): multiply by
     exp(-1/2 sum_i k_i^2 (sigma_i h_i)^2), Nyquist index kept as +N/2."""

@@ -148,3 +148,29 @@ def test_batch_equals_single(cb):
             st = ci.stats(b)
             assert st["gn_iterations"] == single[b][1]["gn_iterations"]
             assert rel(vb, single[b][0]) < 1e-6
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_det_def_grad_matches_oracle(cb, inverse):
+    # DeformationFields::ComputeDetDefGradSL (src/DeformationFields.cpp:636-739)
+    n, nt = 32, 8
+    rng = np.random.Generator(np.random.PCG64(11))
+    v = R.velocity_random((n, n, n), rng, rms=0.2)
+    ref, (mn, me, mx) = R.det_def_grad(v, nt, inverse=inverse)
+    mR, mT, _ = c1_problem(n, 4)
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.SetInitialGuess(v.astype(np.float32))
+        jac, (gmn, gme, gmx) = ci.ComputeDetDefGrad(inverse=inverse)
+    assert rel(jac, ref) < 1e-5
+    assert abs(gmn - mn) < 1e-5 and abs(gmx - mx) < 1e-5 and abs(gme - me) < 1e-6
+
+
+def test_det_def_grad_volume_preserving(cb):
+    n, nt = 32, 4
+    mR, mT, vstar = c1_problem(n, nt)   # divergence-free trig velocity
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.SetInitialGuess(vstar)
+        jac, (mn, me, mx) = ci.ComputeDetDefGrad()
+    assert abs(mn - 1) < 1e-5 and abs(mx - 1) < 1e-5 and abs(me - 1) < 1e-6

@@ -190,3 +190,22 @@ def test_gauss_newton_reduces_gradient_on_reference_problem():
     res = R.gauss_newton(prob, R.GNOptions(maxit=10, gttol=1e-2))
     assert res["reason"] == "gttol"
     assert R.relative_mismatch(mR, res["m1"], mT) < 0.5
+
+
+def test_det_def_grad_known_answers():
+    # divergence-free and constant velocities preserve volume: det(grad y) = 1
+    n = 16
+    v = R.velocity_trig((n, n, n), 0.5)
+    jac, (mn, me, mx) = R.det_def_grad(v, 4)
+    assert abs(mn - 1) < 1e-12 and abs(mx - 1) < 1e-12 and abs(me - 1) < 1e-12
+    vc = np.zeros((3, n, n, n))
+    vc[1] += 0.4
+    assert np.allclose(R.det_def_grad(vc, 4)[0], 1.0, atol=1e-14)
+    # a compressible field changes volume; the inverse map's determinant
+    # (a = -1) is its reciprocal to first order
+    rng = np.random.Generator(np.random.PCG64(5))
+    vr = R.velocity_random((n, n, n), rng, rms=0.1)
+    jf, _ = R.det_def_grad(vr, 8)
+    ji, _ = R.det_def_grad(vr, 8, inverse=True)
+    assert np.abs(jf - 1).max() > 1e-3
+    assert np.abs(jf * ji - 1).max() < 0.1 * np.abs(jf - 1).max()
