@@ -56,6 +56,8 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->krylovtol[1] = 1e-16;
   o->krylovtol[2] = 1e6;
   o->krylovfseq = CB_FSEQ_SUPERLINEAR;
+  o->betacont = 0.0;
+  o->presolvetol = 1e-1;  // src/RegOpt.cpp:1172
   o->precond = 1;
   o->iporder = 3;
   o->verbosity = 0;
@@ -117,6 +119,10 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
     } else if (!std::strcmp(a, "-krylovtol")) {
       if (next(&val)) return CB_ERR_ARG;
       o->krylovtol[0] = std::atof(val);
+    } else if (!std::strcmp(a, "-betacont")) {
+      // src/RegOpt.cpp:755-765
+      if (next(&val)) return CB_ERR_ARG;
+      o->betacont = std::atof(val);
     } else if (!std::strcmp(a, "-krylovfseq")) {
       if (next(&val)) return CB_ERR_ARG;
       if (!std::strcmp(val, "none")) o->krylovfseq = CB_FSEQ_NONE;

@@ -929,18 +929,21 @@ int Solver::begin(const std::vector<int>& sel) {
 // One GN iteration (src/Optimizer.cpp:257-445) of every running problem that
 // has not met a stopping test (src/TaoInterface.cpp:391-527).  Problems that
 // stop are listed in `finished` (running, done, final values pending).
-int Solver::step(std::vector<int>& finished) {
+int Solver::step(std::vector<int>& finished, double gttol, int miniter) {
   finished.assign(B, 0);
-  const double gttol = opts.opttol, gatol = opts.gatol, minstep = 1.0 / 1024.0;
+  if (gttol < 0) gttol = opts.opttol;
+  const double gatol = opts.gatol, minstep = 1.0 / 1024.0;
   std::vector<int> act(B, 0);
   bool any = false;
   for (int b = 0; b < B; ++b) {
     if (!ps[b].running || ps[b].done) continue;
     ProbState& s = ps[b];
+    // step / gradient tests only from iteration miniter on (src/TaoInterface.cpp:438-470)
+    const bool tests = s.iter >= miniter;
     if (!std::isfinite(s.J) || !std::isfinite(s.gnorm)) { s.done = true; s.reason = -1; }
-    else if (s.step < minstep) { s.done = true; s.reason = 4; }
-    else if (s.gnorm < gttol * s.gnorm0) { s.done = true; s.reason = 1; }
-    else if (s.gnorm < gatol) { s.done = true; s.reason = 2; }
+    else if (tests && s.step < minstep) { s.done = true; s.reason = 4; }
+    else if (tests && s.gnorm < gttol * s.gnorm0) { s.done = true; s.reason = 1; }
+    else if (tests && s.gnorm < gatol) { s.done = true; s.reason = 2; }
     else if (s.iter > opts.maxit - 1) { s.done = true; s.reason = 3; }
     if (s.done) { finished[b] = 1; continue; }
     act[b] = 1;
@@ -1014,7 +1017,57 @@ int Solver::finish(const std::vector<int>& sel) {
   return 0;
 }
 
+// Regularisation-parameter continuation (CLAIREInterface::RunSolverRegParaContReduction,
+// src/CLAIREInterface.cpp:1300-1376): J0 and ||g0|| at beta = 1 (:1324-1331);
+// levels beta = 1, 1/10, ... while beta > beta*, each a GN solve to the
+// presolve tolerance warm-started from the previous level (Optimizer::Run with
+// presolve, src/Optimizer.cpp:451-494; at least one iteration per level,
+// src/RegOpt.cpp:757-760); then the solve at beta* to opttol.  The Krylov
+// forcing reference ||g|| is set once (src/KrylovInterface.cpp:125-139).
+int Solver::run_betacont(const std::vector<int>& sel, double beta_star, double presolve_gttol) {
+  if (!(beta_star > 0.0 && beta_star < 1.0)) {
+    err = "target beta not in (0,1)";
+    return CB_ERR_ARG;
+  }
+  auto set_beta = [&](double beta) -> int {
+    for (int b = 0; b < B; ++b)
+      if (sel[b]) ps[b].beta0 = beta;
+    return upload_params();
+  };
+  auto level = [&](double gttol) -> int {
+    for (int b = 0; b < B; ++b)
+      if (sel[b]) {
+        ps[b].iter = 0;
+        ps[b].done = false;
+        ps[b].step = 1.0;
+        state_of[b] = 0;  // the objective changed with beta
+      }
+    CB_TRY(objective_at(v, sel));
+    CB_TRY(gradient_at_current(sel));
+    std::vector<int> fin;
+    while (true) {
+      bool running = false;
+      for (int b = 0; b < B; ++b) running |= sel[b] && ps[b].running && !ps[b].done;
+      if (!running) break;
+      CB_TRY(step(fin, gttol, 1));
+    }
+    return 0;
+  };
+  double beta = 1.0;
+  CB_TRY(set_beta(beta));
+  CB_TRY(begin(sel));
+  while (beta > beta_star) {
+    CB_TRY(level(presolve_gttol));
+    beta /= 10.0;
+    CB_TRY(set_beta(beta));
+  }
+  CB_TRY(set_beta(beta_star));
+  CB_TRY(level(opts.opttol));
+  return finish(sel);
+}
+
 int Solver::run(const std::vector<int>& sel) {
+  if (opts.betacont > 0.0) return run_betacont(sel, opts.betacont, opts.presolvetol);
   CB_TRY(begin(sel));
   std::vector<int> fin;
   while (true) {

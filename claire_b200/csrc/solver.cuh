@@ -45,7 +45,8 @@ class Solver {
   // ---- public operations (problems selected by the host mask `sel`) -------
   int run(const std::vector<int>& sel);                  // begin + steps + finish
   int begin(const std::vector<int>& sel);                // join the GN loop (J0, ||g0||)
-  int step(std::vector<int>& finished);                  // one GN iteration of the running problems
+  int step(std::vector<int>& finished, double gttol = -1.0, int miniter = 0);  // one GN iteration
+  int run_betacont(const std::vector<int>& sel, double beta_star, double presolve_gttol);
   int finish(const std::vector<int>& sel);               // final mismatch; leave the loop
   int objective_at(const float* vel, const std::vector<int>& sel);  // fills ps[p].J/D/R
   int gradient_at_current(const std::vector<int>& sel);              // g, ||g|| for v

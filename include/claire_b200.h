@@ -60,6 +60,8 @@ typedef struct claire_b200_opts {
   int iporder;          /* -iporder: 3 (tricubic) is the only order on this path */
   int verbosity;        /* -verbosity */
   int bf16_images;      /* store transported images in bf16 (gathers accumulate in fp32) */
+  double betacont;      /* -betacont beta*: regularisation-parameter continuation to beta* (0: off) */
+  double presolvetol;   /* relative gradient tolerance of the continuation levels (1e-1) */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {

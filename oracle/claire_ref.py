@@ -653,9 +653,13 @@ class GNOptions:
     min_step: float = 2.0 ** -10
 
 
-def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None):
+def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None, g0=None, krylov_g0=None,
+                 miniter=0):
     """GN-Krylov with Armijo backtracking and CLAIRE's gradient stopping test.
 
+    ``g0`` / ``krylov_g0`` fix the reference gradient norms (continuation
+    levels keep those of the first initialisation); the step and gradient
+    tests apply from iteration ``miniter`` on (src/TaoInterface.cpp:438-470).
     Returns a dict with the velocity, iteration counts and monitor values.
     """
     v = np.zeros((3,) + prob.shape, dtype=prob.dtype) if v0 is None else np.asarray(v0, prob.dtype).copy()
@@ -663,8 +667,8 @@ def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None
     D0 = prob.last_D
     g = prob.gradient(v)
     gnorm = math.sqrt(dot(g, g))
-    g0 = gnorm if gnorm > 0 else 1.0
-    krylov_g0 = None
+    if g0 is None:
+        g0 = gnorm if gnorm > 0 else 1.0
     it = 0
     step = 1.0
     pcg_iters = []
@@ -673,13 +677,13 @@ def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None
         if not (math.isfinite(J) and math.isfinite(gnorm)):
             reason = "nan"
             break
-        if step < opts.min_step:
+        if it >= miniter and step < opts.min_step:
             reason = "steptol"
             break
-        if gnorm < opts.gttol * g0:
+        if it >= miniter and gnorm < opts.gttol * g0:
             reason = "gttol"
             break
-        if gnorm < opts.gatol:
+        if it >= miniter and gnorm < opts.gatol:
             reason = "gatol"
             break
         if it > opts.maxit - 1:
@@ -721,7 +725,39 @@ def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None
         m = prob.solve_state()
     return dict(v=v, J=J, D=prob.last_D if hasattr(prob, "last_D") else None, D0=D0,
                 gnorm=gnorm, g0=g0, iters=it, pcg_iters=pcg_iters, reason=reason,
-                m1=m[prob.nt].copy())
+                m1=m[prob.nt].copy(), krylov_g0=krylov_g0)
+
+
+def beta_continuation(prob: Problem, beta_star: float, opts: GNOptions = GNOptions(), presolve_gttol=1e-1,
+                      log=None):
+    """Regularisation-parameter continuation (CLAIREInterface::
+    RunSolverRegParaContReduction, src/CLAIREInterface.cpp:1300-1376): ||g0||
+    at beta = 1 and v = 0; levels beta = 1, 1/10, ... while beta > beta*, each
+    warm-started and solved to presolve_gttol with at least one iteration;
+    then beta* to opts.gttol.  Returns the last level's result with the list of
+    per-level GN iteration counts."""
+    import dataclasses
+    beta = 1.0
+    prob.reg = dataclasses.replace(prob.reg, beta0=beta)
+    prob.set_velocity(np.zeros((3,) + prob.shape, dtype=prob.dtype))
+    g = prob.gradient(np.zeros((3,) + prob.shape, dtype=prob.dtype))
+    g0 = math.sqrt(dot(g, g))
+    g0 = g0 if g0 > 0 else 1.0
+    v = None
+    kg0 = None
+    levels = []
+    pre = dataclasses.replace(opts, gttol=presolve_gttol)
+    while beta > beta_star:
+        prob.reg = dataclasses.replace(prob.reg, beta0=beta)
+        res = gauss_newton(prob, pre, v0=v, log=log, g0=g0, krylov_g0=kg0, miniter=1)
+        v, kg0 = res["v"], res["krylov_g0"]
+        levels.append(res["iters"])
+        beta /= 10.0
+    prob.reg = dataclasses.replace(prob.reg, beta0=beta_star)
+    res = gauss_newton(prob, opts, v0=v, log=log, g0=g0, krylov_g0=kg0, miniter=1)
+    levels.append(res["iters"])
+    res["levels"] = levels
+    return res
 
 
 def relative_mismatch(mR, m1, mT) -> float:

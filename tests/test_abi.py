@@ -76,3 +76,10 @@ def test_memory_estimate_scales():
     b = cb.RegOpt(["-nx", "128", "-nt", "4"]).estimate_bytes(1)
     assert 7.5 < b / a < 8.5
     assert cb.RegOpt(["-nx", "64"]).estimate_bytes(4) == 4 * a
+
+
+def test_parse_betacont():
+    import claire_b200 as cb
+    o = cb.RegOpt(["-nx", "32", "-betacont", "1e-4"]).opts
+    assert o.betacont == 1e-4 and o.presolvetol == 1e-1
+    assert cb.RegOpt().opts.betacont == 0.0

@@ -174,3 +174,23 @@ def test_det_def_grad_volume_preserving(cb):
         ci.SetInitialGuess(vstar)
         jac, (mn, me, mx) = ci.ComputeDetDefGrad()
     assert abs(mn - 1) < 1e-5 and abs(mx - 1) < 1e-5 and abs(me - 1) < 1e-6
+
+
+def test_beta_continuation_matches_oracle(cb):
+    # CLAIREInterface::RunSolverRegParaContReduction (src/CLAIREInterface.cpp:1300-1376)
+    n, nt = 32, 4
+    mR, mT, vstar = c1_problem(n, nt)
+    prob = R.Problem(mR.astype(np.float64), mT.astype(np.float64), nt, R.Regularization("h1s", 1.0))
+    res = R.beta_continuation(prob, 1e-3, R.GNOptions(maxit=10, gttol=1e-2))
+    opt = make_opt(cb, n, nt, "h1s", 1e-2)
+    opt.set("betacont", 1e-3)
+    opt.set("maxit", 10)
+    opt.set("opttol", 1e-2)
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        ci.Run()
+        v = np.asarray(ci.GetSolution())
+        st = ci.stats()
+    assert rel(v, res["v"]) < 1e-4
+    assert abs(st["gn_iterations"] - res["iters"]) <= 1   # iterations of the final level
+    assert st["gnorm0"] > 0 and abs(st["gnorm0"] - res["g0"]) <= 1e-5 * res["g0"]
