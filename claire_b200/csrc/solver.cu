@@ -400,6 +400,22 @@ int Solver::reg_functional(const float* vel, const std::vector<int>& sel, const 
   return 0;
 }
 
+// CLAIREDivReg::EvaluteRegularizationDIV (src/CLAIREDivReg.cpp:165-245):
+// S_RW = ||grad div v||^2 + ||div v||^2 (spectral derivatives, FP64 sums);
+// the caller scales by hd beta_w / 2.
+int Solver::div_penalty(const float* vel, const int* act) {
+  float* dv = work3;  // div v of problem p at dv + p*n (scratch)
+  CB_TRY(divergence(vel, dv, act));
+  CB_TRY(dot(dv, n, dv, n, n, S_RW, act));
+  for (int a = 0; a < 3; ++a) {
+    const int np = deriv_partials(d, a, 1);
+    CB_TRY(launch_deriv(dv, n, n, nullptr, 0, 0, 1, B, d, a, EPI_SUMSQ, partials, maxparts, act, stream));
+    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RW), B, 1.0, true, stream));
+  }
+  note_launches(6);
+  return 0;
+}
+
 static double reg_factor(const ProbState& s, double hd, double sumsq, double vv) {
   switch (s.norm) {
     case NORM_H1SN: return 0.5 * hd * s.beta0 * sumsq;
@@ -437,10 +453,13 @@ int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
   if (any_b) {
     CB_TRY(reg_functional(vel, sb, dact));
   }
+  if (opts.model == CB_MODEL_RELAXEDSTOKES) CB_TRY(div_penalty(vel, dact));
   CB_TRY(fetch_scalars());
   for (int b = 0; b < B; ++b) {
     if (!sel[b]) continue;
     if (sb[b]) R[b] = reg_factor(ps[b], hd, hsc[S_R * B + b], 0.0);
+    // CLAIREDivReg::EvaluateObjective: J = D + R1(v) + R2(div v) (src/CLAIREDivReg.cpp:109-160)
+    if (opts.model == CB_MODEL_RELAXEDSTOKES) R[b] += 0.5 * hd * ps[b].beta2 * hsc[S_RW * B + b];
     ps[b].D = hsc[S_D * B + b];
     ps[b].R = R[b];
     ps[b].J = ps[b].D + ps[b].R;

@@ -89,7 +89,7 @@ class Solver {
   int* hint = nullptr;     // pinned host mirror of dint
 
   enum Slot { S_D = 0, S_R, S_RV, S_GG, S_PQ, S_RR, S_RZ, S_RZNEW, S_ALPHA, S_BETA, S_TOL,
-              S_RN0, S_GD, S_RTOL, NSLOT };
+              S_RN0, S_GD, S_RTOL, S_RW, NSLOT };
   enum ISlot { I_IT = 0, I_REASON, NISLOT };
 
   // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
@@ -127,6 +127,7 @@ class Solver {
   int grad_fields(const float* f, long long fp, long long ifs, float* out, long long op,
                   long long ofs, int nf, const int* act);
   int divergence(const float* vel, float* out, const int* act);
+  int div_penalty(const float* vel, const int* act);
   int adjoint_sweep(float* bout, const int* act);
   int finish_with_reg(const float* vin, float* out, const int* act, const float* dot_with = nullptr,
                       int dot_slot = -1);

@@ -431,6 +431,7 @@ class Problem:
         self.hd = lebesgue_measure(self.shape)
         self.reg = reg
         self.projection = projection
+        self.beta_w = 1e-4  # -beta-div (src/RegOpt.cpp:729-731, default 1e-4)
         self.v = None
         self.m = None
         self.counters = dict(obj=0, grad=0, hessmatvec=0, pcmatvec=0, pdesolve=0)
@@ -490,10 +491,21 @@ class Problem:
         dr = self.mR.astype(np.float64) - m[self.nt].astype(np.float64)
         return 0.5 * self.hd * float(np.sum(dr * dr))
 
+    def div_penalty(self, v) -> float:
+        """CLAIREDivReg::EvaluteRegularizationDIV (src/CLAIREDivReg.cpp:165-245):
+        R_w = 1/2 hd beta_w (||grad div v||^2 + ||div v||^2), beta_w = -beta-div."""
+        dv = div(v)
+        gd = grad(dv)
+        s = float(np.sum(gd.astype(np.float64) ** 2)) + float(np.sum(dv.astype(np.float64) ** 2))
+        return 0.5 * self.hd * self.beta_w * s
+
     def objective(self, v) -> float:
         self.set_velocity(v)
         D = self.distance()
         R = 0.0 if not np.any(self.v) else self.reg.functional(self.v)
+        if self.projection == "relaxedstokes" and np.any(self.v):
+            # CLAIREDivReg::EvaluateObjective: J = D + R1(v) + R2(div v) (src/CLAIREDivReg.cpp:109-160)
+            R += self.div_penalty(self.v)
         self.counters["obj"] += 1
         self.last_D, self.last_R = D, R
         return D + R

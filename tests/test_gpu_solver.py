@@ -194,3 +194,28 @@ def test_beta_continuation_matches_oracle(cb):
     assert rel(v, res["v"]) < 1e-4
     assert abs(st["gn_iterations"] - res["iters"]) <= 1   # iterations of the final level
     assert st["gnorm0"] > 0 and abs(st["gnorm0"] - res["g0"]) <= 1e-5 * res["g0"]
+
+
+@pytest.mark.parametrize("flag,model", [("h1s-stokes", "stokes"), ("h1s-div", "relaxedstokes")])
+def test_projection_models_match_oracle(cb, flag, model):
+    # CLAIREStokes / CLAIREDivReg: projected body force (src/CLAIREStokes.cpp:407-540,
+    # src/CLAIREDivReg.cpp:313-460); the relaxed model adds R2(div v) to J (:109-245)
+    n, nt = 32, 4
+    mR, mT, vstar = c1_problem(n, nt)
+    rng = np.random.default_rng(3)
+    v = (0.3 * vstar + 0.05 * rng.standard_normal(vstar.shape)).astype(np.float32)
+    vt = (0.1 * rng.standard_normal(vstar.shape)).astype(np.float32)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2), projection=model)
+    J = prob.objective(v.astype(np.float64))
+    g = prob.gradient(v.astype(np.float64))
+    H = prob.hessian_matvec(vt.astype(np.float64))
+    opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", flag, "-beta", "1e-2"])
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        Jg, Dg, Rg = ci.EvaluateObjective(v)
+        assert abs(Jg - J) <= 1e-5 * abs(J)
+        assert abs(Rg - prob.last_R) <= 1e-5 * abs(prob.last_R)
+        assert rel(ci.EvaluateGradient(v), g) < 1e-5
+        assert rel(ci.HessianMatVec(v, vt), H) < 1e-5
+    if model == "relaxedstokes":
+        assert prob.div_penalty(v.astype(np.float64)) > 0
