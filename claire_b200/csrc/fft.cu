@@ -490,7 +490,9 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
   load_col_tile<N, C, PITCH>(re, im, colp, ncols);
   __syncthreads();
   fft_lines<N, false, C, PITCH>(re, im, sre, sim, tw);
-#pragma unroll
+  // one copy of the symbol code (a rolled loop keeps the kernel small enough
+  // for the instruction cache)
+#pragma unroll 1
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
     const int a = e * PITCH + c;
