@@ -167,6 +167,8 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     // CLAIRE_B200_GRAPHS=0 runs PCG iterations as direct launches
     const char* ge = std::getenv("CLAIRE_B200_GRAPHS");
     graphs = !(ge && ge[0] == '0');
+    const char* fd = std::getenv("CLAIRE_B200_FUSED_DOTS");
+    fused_dots = fd && fd[0] == '1';
   }
   ht = (float)(1.0 / nt);
   hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
@@ -479,13 +481,18 @@ int Solver::reg_op(const float* vin, float* out, int op, int epi, const int* act
                    int dot_slot) {
   CB_TRY(launch_r2c3d(vin, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
   CB_TRY(launch_pencil(spec, 3 * nc, B, d, op, dparams, 3, 3, act, stream));
-  if (dot_with) {
+  if (dot_with && fused_dots) {
     const int e2 = (epi == EPI_ADD) ? EPI_ADD_DOT : EPI_STORE_DOT;
     CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, e2, nullptr, partials, maxparts, act, stream,
                         dot_with));
     CB_TRY(launch_finalize(partials, maxparts, c2r_partials(d, 3), slot(dot_slot), B, 1.0, false, stream));
     note_launches(6);
     return 0;
+  }
+  if (dot_with) {
+    CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, epi, nullptr, nullptr, 0, act, stream));
+    note_launches(5);
+    return dot(out, 3 * n, dot_with, 3 * n, 3 * n, dot_slot, act);
   }
   CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, epi, nullptr, nullptr, 0, act, stream));
   note_launches(5);

@@ -98,6 +98,9 @@ class Solver {
   // PCG iteration recorded as a CUDA graph (built on the second iteration the
   // solver runs; graphs = false switches replay off)
   bool graphs = true, pcg_warm = false;
+  // p.q and r.z summed inside the inverse transforms' epilogues instead of a
+  // separate dot pass (CLAIRE_B200_FUSED_DOTS=1)
+  bool fused_dots = false;
   cudaGraphExec_t pcg_exec = nullptr;
   long long pcg_exec_launches = 0;
 
