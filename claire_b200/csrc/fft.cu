@@ -250,7 +250,10 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
   float* im = re + N * PITCH;
   float* sre = im + N * PITCH;
   float* sim = sre + N * PITCH;
-  float* str = sim + N * PITCH;  // staging: 2P rows x NH
+  // staging of the 2P half-spectrum rows: it is dead before the transform
+  // starts, so it shares the transform's scratch (sre / sim) when that is large
+  // enough (row_smem sizes the block for the larger of the two)
+  float* str = sre;
   float* sti = str + 2 * P * NH;
   const float2* src = in + blockIdx.z * ip + blockIdx.y * ifs;
   float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
@@ -671,9 +674,10 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N> static size_t row_smem(bool c2r) {
-  size_t s = (2 * N + 4 * N * RowCfg<N>::PITCH) * sizeof(float);
-  if (c2r) s += 2 * 2 * RowCfg<N>::P * (N / 2 + 1) * sizeof(float);
-  return s;
+  const size_t scratch = 2 * N * RowCfg<N>::PITCH;           // sre + sim
+  const size_t staging = 2 * 2 * RowCfg<N>::P * (N / 2 + 1);  // c2r half-spectrum rows (shares scratch)
+  const size_t tail = (c2r && staging > scratch) ? staging : scratch;
+  return (2 * N + 2 * N * RowCfg<N>::PITCH + tail) * sizeof(float);
 }
 template <int N> static size_t col_smem(int nbuf) {
   return (2 * N + 2 * nbuf * N * ColCfg<N>::PITCH) * sizeof(float);
