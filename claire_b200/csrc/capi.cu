@@ -622,6 +622,8 @@ int claire_b200_profile(claire_b200_ctx* c, int enable) {
   if (!enable) {
     if (cudaStreamSynchronize(s.stream) != cudaSuccess) return CB_ERR_CUDA;
     s.prof_clear();
+  } else if (s.prof_reserve(4096)) {
+    return CB_ERR_CUDA;
   }
   s.prof_on = enable != 0;
   return CB_OK;

@@ -324,10 +324,26 @@ int Solver::state_solve(const float* vel, const int* act) {
 // ---------------------------------------------------------------------------
 // device timers
 // ---------------------------------------------------------------------------
+// Events come from a recycled pool: creating one per mark costs host time
+// between the launches being timed, which would stretch the measured gaps.
+int Solver::prof_reserve(int count) {
+  while ((int)prof_pool.size() < count) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return CB_ERR_CUDA;
+    prof_pool.push_back(e);
+  }
+  return 0;
+}
+
 int Solver::prof_mark(int cat) {
   if (!prof_on) return 0;
   cudaEvent_t e;
-  if (cudaEventCreate(&e) != cudaSuccess) return CB_ERR_CUDA;
+  if (!prof_pool.empty()) {
+    e = prof_pool.back();
+    prof_pool.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    return CB_ERR_CUDA;
+  }
   prof_ev[cat].push_back(e);
   return cudaEventRecord(e, stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
 }
@@ -342,7 +358,7 @@ int Solver::prof_read(int cat, double* ms, long long* count) {
   }
   if (ms) *ms = total;
   if (count) *count = (long long)(ev.size() / 2);
-  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  prof_pool.insert(prof_pool.end(), ev.begin(), ev.end());
   ev.clear();
   return 0;
 }
@@ -352,6 +368,8 @@ void Solver::prof_clear() {
     for (cudaEvent_t e : prof_ev[c]) cudaEventDestroy(e);
     prof_ev[c].clear();
   }
+  for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
+  prof_pool.clear();
 }
 
 // D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)

@@ -107,6 +107,8 @@ class Solver {
   // device timers per category (CB_PROF_*): event pairs recorded around launches
   bool prof_on = false;
   std::vector<cudaEvent_t> prof_ev[CB_PROF_NCAT];
+  std::vector<cudaEvent_t> prof_pool;  // recorded-and-read events, reused by prof_mark
+  int prof_reserve(int count);         // pre-creates events for the pool
   int prof_mark(int cat);  // records one event (call before and after a launch)
   int prof_read(int cat, double* ms, long long* count);
   void prof_clear();
