@@ -54,6 +54,12 @@ def parse():
     ap.add_argument("--requests", type=int, default=40, help="--serve: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="--serve: arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="--serve: slots per pool")
+    ap.add_argument("--mixed", action="store_true",
+                    help="mixed batch instead: 12 x 64^3 + 12 x 96^3 + 8 x 128^3 (H1 beta=1e-2, nt=4) served "
+                         "together against plain one-at-a-time runs")
+    ap.add_argument("--mixed-slots", type=int, default=12, help="--mixed: slots per pool")
+    ap.add_argument("--precision", action="store_true",
+                    help="bf16-image study instead: 256^3 H2 beta=1e-4 nt=8 with bf16 and FP32 image storage")
     return ap.parse_args()
 
 
@@ -482,6 +488,200 @@ def run_serve(a, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
+# mixed batch (--mixed): 32 registrations of uneven sizes
+# ---------------------------------------------------------------------------
+MIXED = [64] * 12 + [96] * 12 + [128] * 8
+
+
+def run_mixed(a, rank, world, local):
+    """12 x 64^3 + 12 x 96^3 + 8 x 128^3, H1 beta=1e-2 (beta1=1e-4), nt=4,
+    seeded ellipsoid / random-velocity recipe (config index 2), all submitted
+    at once to the registration server (one pool per size, concurrent streams)
+    and, for comparison, solved one at a time by plain single-problem contexts
+    (one per size, created before timing).  Both legs are timed on the device
+    (events around the whole batch, synchronised)."""
+    import torch
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nt, norm, beta = 4, "h1", 1e-2
+    probs = []
+    for i, n in enumerate(MIXED):
+        mR, mT, _ = synthetic.ellipsoid_problem(n, nt, 2, rank * len(MIXED) + i, dev)
+        probs.append((n, mR, mT, mR.cpu().numpy(), mT.cpu().numpy()))
+    opts = {n: cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", norm, "-beta", repr(beta),
+                          "-maxit", str(a.maxit), "-opttol", repr(a.opttol)]) for n in sorted(set(MIXED))}
+    stream = torch.cuda.Stream(device=dev)
+    srv = cb.Server(slots_per_pool=a.mixed_slots, idle_ms=600000, device=local)
+
+    def serve_all():
+        ids = [srv.submit(opts[n], mRh, mTh) for n, _, _, mRh, mTh in probs]
+        out = []
+        for (n, *_), rid in zip(probs, ids):
+            if srv.wait(rid, -1) != cb.REQ_DONE:
+                raise RuntimeError("registration request failed")
+            out.append(srv.result(rid, (n, n, n)))
+        return out
+
+    serve_all()  # pools are created (and their memory allocated) before timing
+    with Clocks(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = serve_all()
+        torch.cuda.synchronize()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    served_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    lats = gather_list([r[2] for r in res], world)
+    srv.close()
+
+    ctx = {n: cb.CLAIREInterface(opts[n], nbatch=1) for n in opts}
+    zero = {n: torch.zeros((3, n, n, n), device=dev) for n in opts}
+    for c in ctx.values():
+        c.set_stream(stream)
+
+    def plain_all():
+        for n, mR, mT, _, _ in probs:
+            ctx[n].set_images(mR, mT)
+            ctx[n].SetInitialGuess(zero[n])
+            ctx[n].Run()
+
+    for n, mR, mT, _, _ in probs[::12]:  # one warm run per size
+        ctx[n].set_images(mR, mT)
+        ctx[n].SetInitialGuess(zero[n])
+        ctx[n].Run()
+    barrier(world)
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_all()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(p0.elapsed_time(p1), world)
+    for c in ctx.values():
+        c.close()
+    if rank != 0:
+        return
+    total = world * len(MIXED)
+    ls = sorted(lats)
+    line = {
+        "metric": "registrations/s, mixed batch (12 x 64^3 + 12 x 96^3 + 8 x 128^3, H1 beta=1e-2, nt=4)",
+        "value": total / (served_ms / 1e3), "unit": "registrations/s", "n_gpus": world, "steps": 1,
+        "warmup": 1, "ms_per_step": served_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "32 registrations per GPU of uneven sizes through the registration server "
+                               f"(one pool per size, {a.mixed_slots} slots), maxit {a.maxit}, opttol {a.opttol}",
+                   "plain_single_problem_value": total / (plain_ms / 1e3),
+                   "served_over_plain": plain_ms / served_ms,
+                   "latency_ms": {"p50": float(np.percentile(ls, 50)), "p99": float(np.percentile(ls, 99)),
+                                  "what": "per request, submit of host images to host velocity, all 32 "
+                                          "submitted at once"},
+                   "mean_gn_iterations": float(np.mean([r[1]["gn_iterations"] for r in res])),
+                   "mean_pcg_iterations": float(np.mean([r[1]["pcg_iterations"] for r in res]))},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# bf16 image storage study (--precision): 256^3 H2 beta=1e-4 nt=8
+# ---------------------------------------------------------------------------
+def run_precision(a, rank, world, local):
+    """One 256^3 problem (ellipsoid recipe, config index 3) with bf16 and with
+    FP32 image storage.  Errors of the bf16 storage are measured per operation
+    at one fixed velocity (half the recipe's velocity; random direction for the
+    Hessian): distance, relative mismatch, body force (the data part of the
+    gradient), gradient, GN Hessian matvec and transported image, each against
+    the FP32-image result on the same GPU (the device has no FP64 path; the
+    FP64 oracle's agreement with both formats is tested at 32^3).  Both
+    formats then solve the registration; with H2's gradient lacking the hd
+    factor of its objective the GN path of this problem is sensitive to any
+    perturbation, so the two solves are reported side by side, not differenced."""
+    import torch
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, nt, norm, beta = 256, 8, "h2", 1e-4
+    mR, mT, vrec = synthetic.ellipsoid_problem(n, nt, 3, rank, dev)
+    v = (0.5 * vrec).cpu().numpy()
+    vt = np.random.default_rng(3).standard_normal(v.shape).astype(np.float32) * float(np.std(v))
+    torch.cuda.synchronize()
+    out = {}
+    for tag, extra in (("fp32", []), ("bf16", ["-bf16images"])):
+        opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", norm, "-beta", repr(beta), "-maxit",
+                         str(a.maxit), "-opttol", repr(a.opttol)] + extra)
+        with cb.CLAIREInterface(opt) as ci:
+            stream = torch.cuda.Stream(device=dev)
+            ci.set_stream(stream)
+            ci.set_images(mR, mT)
+            r = {"bytes": ci.footprint_bytes()}
+            r["J"], r["D"], _ = ci.EvaluateObjective(v)
+            r["g"] = ci.EvaluateGradient(v)
+            r["bf"] = ci.GetAdjoint()[1]
+            r["H"] = ci.HessianMatVec(v, vt)
+            ci.SetInitialGuess(v)
+            r["m1"] = ci.GetFinalState()
+            ci.SetInitialGuess(np.zeros_like(v))
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ci.Run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            r["ms"] = e0.elapsed_time(e1)
+            r["stats"] = ci.stats()
+            out[tag] = r
+        torch.cuda.synchronize()
+    if rank != 0:
+        return
+
+    def rel(x, y):
+        x = np.asarray(x, np.float64)
+        y = np.asarray(y, np.float64)
+        return float(np.linalg.norm((x - y).ravel()) / max(np.linalg.norm(y.ravel()), 1e-300))
+
+    f, h = out["fp32"], out["bf16"]
+    mRn, mTn = mR.cpu().numpy().astype(np.float64), mT.cpu().numpy().astype(np.float64)
+    den = np.linalg.norm((mRn - mTn).ravel())
+    mis = {k: float(np.linalg.norm((mRn - out[k]["m1"]).ravel()) / den) for k in out}
+
+    def solve(r):
+        st = r["stats"]
+        return {"ms": r["ms"], "gn_iterations": st["gn_iterations"], "pcg_iterations": st["pcg_iterations"],
+                "rel_mismatch": st["rel_mismatch"], "grad_reduction": st["gnorm"] / st["gnorm0"],
+                "reason": st["converged_reason"]}
+
+    line = {
+        "metric": "256^3 registration with bf16 image storage: per-operation error against FP32 images, and time",
+        "value": h["ms"], "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": h["ms"],
+        "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "bf16 images / f32 / f64 dots",
+        "data": "synthetic",
+        "config": {"workload": f"256^3 h2 beta=1e-4 nt=8 maxit={a.maxit} opttol={a.opttol}, ellipsoid recipe",
+                   "footprint_bytes": {"fp32": f["bytes"], "bf16": h["bytes"]},
+                   "errors_vs_fp32_images_at_fixed_velocity": {
+                       "objective": abs(h["J"] - f["J"]) / abs(f["J"]),
+                       "distance": abs(h["D"] - f["D"]) / abs(f["D"]),
+                       "rel_mismatch": abs(mis["bf16"] - mis["fp32"]) / mis["fp32"],
+                       "transported_image_rel_l2": rel(h["m1"], f["m1"]),
+                       "body_force_rel_l2": rel(h["bf"], f["bf"]),
+                       "gradient_rel_l2": rel(h["g"], f["g"]),
+                       "hessian_matvec_rel_l2": rel(h["H"], f["H"])},
+                   "solve": {"fp32": solve(f), "bf16": solve(h)},
+                   "reference_for_errors": "the FP32-image result on the same GPU (no FP64 device path)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 def main():
     a = parse()
     rank, world, local = dist_init(a)
@@ -490,6 +690,12 @@ def main():
         return
     if a.serve:
         run_serve(a, rank, world, local)
+        return
+    if a.mixed:
+        run_mixed(a, rank, world, local)
+        return
+    if a.precision:
+        run_precision(a, rank, world, local)
         return
     r = run_ours(a, rank, world, local)
     if rank != 0:

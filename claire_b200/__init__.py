@@ -121,6 +121,7 @@ _signatures = {
     "claire_b200_set_stream": (_I, [_P, _P]),
     "claire_b200_trajectory": (_I, [_P, _P, _IA, _I, _I, _P]),
     "claire_b200_interp3": (_I, [_P, _P, _P, _IA, _I, _P]),
+    "claire_b200_interp3_bf16": (_I, [_P, _P, _P, _IA, _P]),
     "claire_b200_fft_grad": (_I, [_P, _P, _IA, _P]),
     "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
     "claire_b200_reg_apply": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
@@ -180,6 +181,13 @@ def _dev_ptr(t, shape_hint: str = ""):
         raise TypeError(f"expected a CUDA tensor {shape_hint}")
     if t.dtype != torch.float32 or not t.is_contiguous():
         raise TypeError(f"expected a contiguous float32 CUDA tensor {shape_hint}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _dev_ptr_bf16(t, shape_hint: str = ""):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.bfloat16 or not t.is_contiguous():
+        raise TypeError(f"expected a contiguous bfloat16 CUDA tensor {shape_hint}")
     return ctypes.c_void_p(t.data_ptr())
 
 
@@ -471,6 +479,16 @@ class SemiLagrangian:
             out = torch.empty_like(f)
         _check(lib.claire_b200_interp3(_dev_ptr(f), _dev_ptr(disp), _dev_ptr(out), _nx(shape), dof, _stream()),
                "Interpolate")
+        return out
+
+    @staticmethod
+    def InterpolateBF16(f, disp, out=None):
+        """Interpolate one bfloat16 volume (the -bf16images storage format)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty_like(f)
+        _check(lib.claire_b200_interp3_bf16(_dev_ptr_bf16(f), _dev_ptr(disp), _dev_ptr_bf16(out), _nx(f.shape),
+                                            _stream()), "InterpolateBF16")
         return out
 
 

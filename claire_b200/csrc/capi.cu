@@ -138,6 +138,8 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (next(&val)) return CB_ERR_ARG;
       o->iporder = std::atoi(val);
       if (o->iporder != 3) return CB_ERR_UNSUPPORTED;
+    } else if (!std::strcmp(a, "-bf16images")) {
+      o->bf16_images = 1;  // no reference counterpart: bf16 storage of the image volumes
     } else if (!std::strcmp(a, "-verbosity")) {
       if (next(&val)) return CB_ERR_ARG;
       o->verbosity = std::atoi(val);
@@ -203,6 +205,22 @@ static int copy_out(Solver& s, float* dst, const float* src, long long count, in
 int claire_b200_set_images(claire_b200_ctx* c, int b, const float* mR, const float* mT, int on_device) {
   if (!c || !mR || !mT || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;
+  if (s.img16) {
+    // host images stage through problem b's PCG work vector (2n of its 3n
+    // floats; idle between solver calls), then round to bf16
+    const float *dR = mR, *dT = mT;
+    if (!on_device) {
+      float* st = s.x + b * 3 * s.n;
+      int e = copy_in(s, st, mR, s.n, 0);
+      if (!e) e = copy_in(s, st + s.n, mT, s.n, 0);
+      if (e) return e;
+      dR = st;
+      dT = st + s.n;
+    }
+    int e = s.load_images(b, dR, dT);
+    if (!e && cudaStreamSynchronize(s.stream) != cudaSuccess) e = CB_ERR_CUDA;
+    return cuda_status(e);
+  }
   int e = copy_in(s, s.mR + b * s.n, mR, s.n, on_device);
   if (!e) e = copy_in(s, s.mT + b * s.n, mT, s.n, on_device);
   s.state_of[b] = 0;
@@ -414,6 +432,23 @@ int claire_b200_interp3(const float* f, const float* disp, float* out, const int
   if (cudaMallocAsync((void**)&tab, sizeof(int4) * tile_table_int4s(d), s) != cudaSuccess) return CB_ERR_ALLOC;
   int e = launch_tile_table(disp, 0, tab, 0, 1, d, nullptr, s);
   if (!e) e = launch_interp(f, 0, d.n(), disp, 0, tab, 0, out, 0, d.n(), dof, 1, d, nullptr, s);
+  cudaFreeAsync(tab, s);
+  note_launches(2);
+  return cuda_status(e);
+}
+
+int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigned short* out, const int nx[3],
+                             void* stream) {
+  if (!f || !disp || !out || !dims_ok(nx)) return CB_ERR_ARG;
+  if (!(nx[2] & 3) && (reinterpret_cast<uintptr_t>(f) & 7)) return CB_ERR_ARG;
+  Dims d{nx[0], nx[1], nx[2]};
+  cudaStream_t s = (cudaStream_t)stream;
+  int4* tab = nullptr;
+  if (cudaMallocAsync((void**)&tab, sizeof(int4) * tile_table_int4s(d), s) != cudaSuccess) return CB_ERR_ALLOC;
+  int e = launch_tile_table(disp, 0, tab, 0, 1, d, nullptr, s);
+  if (!e)
+    e = launch_interp16(reinterpret_cast<const bf16*>(f), 0, disp, 0, tab, 0, reinterpret_cast<bf16*>(out), 0, 1, d,
+                        nullptr, s);
   cudaFreeAsync(tab, s);
   note_launches(2);
   return cuda_status(e);

@@ -8,12 +8,17 @@
 // Spectral data is the r2c half spectrum N1 x N2 x (N3/2+1) float2, row-major.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #define CB_DEVICE __device__ __forceinline__
 
 namespace cb {
+
+// Storage type of image volumes in the bf16-image mode (mR, mT and the state
+// levels); arithmetic on them is FP32.
+using bf16 = __nv_bfloat16;
 
 // Set by a host thread while it records a CUDA graph: launchers skip
 // non-stream calls (function attributes are set by an earlier uncaptured run).

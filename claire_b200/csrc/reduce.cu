@@ -226,4 +226,100 @@ int launch_lincomb(float* y, long long yp, const float* a, long long ap, const d
   return (int)cudaGetLastError();
 }
 
+// ---- bf16 image volumes -------------------------------------------------------
+
+static dim3 stream_grid(long long work, int nprob, int nz = 1) {
+  long long blocks = (work + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
+  return dim3((unsigned)blocks, nprob, nz);
+}
+
+__global__ void k_to_bf16(const float* __restrict__ src, long long sp, bf16* __restrict__ dst, long long dp,
+                          long long len, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const float* a = src + p * sp;
+  bf16* y = dst + p * dp;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16_rn(a[i]);
+}
+
+__global__ void k_from_bf16(const bf16* __restrict__ src, long long sp, long long sl, float* __restrict__ dst,
+                            long long dp, long long dl, long long len, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const bf16* a = src + p * sp + blockIdx.z * sl;
+  float* y = dst + p * dp + blockIdx.z * dl;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[i] = __bfloat162float(a[i]);
+}
+
+// 8 bf16 per 16-byte unit
+__global__ void k_copy16(uint4* __restrict__ dst, long long dp, const uint4* __restrict__ src, long long sp,
+                         long long units, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < units;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[p * dp + i] = src[p * sp + i];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_diff_sumsq16(const bf16* __restrict__ a, long long ap,
+                                                               const bf16* __restrict__ b, long long bp,
+                                                               long long len, double* __restrict__ partials,
+                                                               int nparts, const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const bf16* pa = a + blockIdx.y * ap;
+  const bf16* pb = b + blockIdx.y * bp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double d = (double)__bfloat162float(pa[i]) - (double)__bfloat162float(pb[i]);
+    acc += d * d;
+  }
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+__global__ void k_diff16(float* __restrict__ y, long long yp, const bf16* __restrict__ a, long long ap,
+                         const bf16* __restrict__ b, long long bp, long long len, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[p * yp + i] = __bfloat162float(a[p * ap + i]) - __bfloat162float(b[p * bp + i]);
+}
+
+int launch_to_bf16(const float* src, long long sp, bf16* dst, long long dp, long long len, int nprob,
+                   const int* active, cudaStream_t s) {
+  k_to_bf16<<<stream_grid(len, nprob), 256, 0, s>>>(src, sp, dst, dp, len, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_from_bf16(const bf16* src, long long sp, long long sl, float* dst, long long dp, long long dl,
+                     long long len, int nlev, int nprob, const int* active, cudaStream_t s) {
+  k_from_bf16<<<stream_grid(len, nprob, nlev), 256, 0, s>>>(src, sp, sl, dst, dp, dl, len, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_copy_bf16(bf16* dst, long long dp, const bf16* src, long long sp, long long len, int nprob,
+                     const int* active, cudaStream_t s) {
+  if ((len & 7) || (dp & 7) || (sp & 7) || !aligned16(dst) || !aligned16(src)) return (int)cudaErrorInvalidValue;
+  k_copy16<<<stream_grid(len / 8, nprob), 256, 0, s>>>(reinterpret_cast<uint4*>(dst), dp / 8,
+                                                       reinterpret_cast<const uint4*>(src), sp / 8, len / 8, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_diff_sumsq16(const bf16* a, long long ap, const bf16* b, long long bp, long long len, int nprob,
+                        double* partials, int stride, const int* active, cudaStream_t s) {
+  dim3 grid(dot_partials(len), nprob);
+  k_diff_sumsq16<<<grid, kRedThreads, 0, s>>>(a, ap, b, bp, len, partials, stride, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_diff16(float* y, long long yp, const bf16* a, long long ap, const bf16* b, long long bp, long long len,
+                  int nprob, const int* active, cudaStream_t s) {
+  k_diff16<<<stream_grid(len, nprob), 256, 0, s>>>(y, yp, a, ap, b, bp, len, active);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace cb

@@ -61,4 +61,21 @@ int launch_fill(float* y, long long yp, float value, long long len, int nprob, c
 int launch_diff_sumsq(const float* a, long long ap, const float* b, long long bp, long long len,
                       int nprob, double* partials, int stride, const int* active, cudaStream_t s);
 
+// ---- bf16 image volumes (FP32 arithmetic, bf16 storage) -----------------------
+// dst[p][i] = bf16(src[p][i]) (round to nearest even)
+int launch_to_bf16(const float* src, long long sp, bf16* dst, long long dp, long long len, int nprob,
+                   const int* active, cudaStream_t s);
+// dst[p][l*dl + i] = float(src[p][l*sl + i]), l < nlev
+int launch_from_bf16(const bf16* src, long long sp, long long sl, float* dst, long long dp, long long dl,
+                     long long len, int nlev, int nprob, const int* active, cudaStream_t s);
+// dst[p][i] = src[p][i] (len % 8 == 0, 16-byte aligned rows)
+int launch_copy_bf16(bf16* dst, long long dp, const bf16* src, long long sp, long long len, int nprob,
+                     const int* active, cudaStream_t s);
+// dot layout partial sums of (a[p][i] - b[p][i])^2 in FP64
+int launch_diff_sumsq16(const bf16* a, long long ap, const bf16* b, long long bp, long long len, int nprob,
+                        double* partials, int stride, const int* active, cudaStream_t s);
+// y[p][i] = a[p][i] - b[p][i] in FP32
+int launch_diff16(float* y, long long yp, const bf16* a, long long ap, const bf16* b, long long bp, long long len,
+                  int nprob, const int* active, cudaStream_t s);
+
 }  // namespace cb

@@ -52,7 +52,7 @@ static bool same_pool(const claire_b200_opts& a, const claire_b200_opts& b) {
          a.maxit == b.maxit && a.opttol == b.opttol && a.gatol == b.gatol && a.krylovmaxit == b.krylovmaxit &&
          a.krylovtol[0] == b.krylovtol[0] && a.krylovtol[1] == b.krylovtol[1] &&
          a.krylovtol[2] == b.krylovtol[2] && a.krylovfseq == b.krylovfseq && a.precond == b.precond &&
-         a.iporder == b.iporder;
+         a.iporder == b.iporder && a.bf16_images == b.bf16_images;
 }
 
 struct Pool;
@@ -175,12 +175,21 @@ static std::vector<std::pair<int, long long>> admit_locked(claire_b200_server* s
 
 static int load_slot(Solver& sv, int b, const Request& r) {
   const long long n = sv.n;
-  if (cudaMemcpyAsync(sv.mR + b * n, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
-          cudaSuccess ||
-      cudaMemcpyAsync(sv.mT + b * n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
-          cudaSuccess ||
-      cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess)
+  if (sv.img16) {
+    // stage through the free slot's PCG work vector, then round to bf16
+    float* st = sv.x + b * 3 * n;
+    if (cudaMemcpyAsync(st, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess ||
+        cudaMemcpyAsync(st + n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+    if (int e = sv.load_images(b, st, st + n)) return e;
+    if (cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess) return CB_ERR_CUDA;
+  } else if (cudaMemcpyAsync(sv.mR + b * n, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+                 cudaSuccess ||
+             cudaMemcpyAsync(sv.mT + b * n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+                 cudaSuccess ||
+             cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess) {
     return CB_ERR_CUDA;
+  }
   sv.state_of[b] = 0;
   return sv.set_problem(b, r.opts);  // per-slot norm and weights (synchronises the stream)
 }

@@ -71,6 +71,15 @@ struct StoreEpi {
   }
 };
 
+// bf16 image output (round to nearest even)
+struct Store16Epi {
+  bf16* dst;
+  const float* aux = nullptr;
+  CB_DEVICE void operator()(const TileThread& tt, int a, float val, float) const {
+    if (tt.valid_idx(a)) dst[tt.idx(a)] = __float2bfloat16_rn(val);
+  }
+};
+
 // out = c * val (aux = c)
 struct ScaleEpi {
   float* out;
@@ -171,6 +180,18 @@ __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
   extern __shared__ __align__(16) float sbuf[];
   StoreEpi epi{out + p * op + (long long)blockIdx.z * of, nullptr};
   tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp + (long long)blockIdx.z * ff, d, epi);
+}
+
+// bf16 image field of problem p -> bf16 out (one state time step)
+__global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
+    k_interp16(const bf16* __restrict__ f, long long fp, const float* __restrict__ disp, long long dp,
+               const int4* __restrict__ tab, long long tp, bf16* __restrict__ out, long long op, Dims d,
+               const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  extern __shared__ __align__(16) float sbuf[];
+  Store16Epi epi{out + p * op, nullptr};
+  tile_gather_tab(sbuf, disp + p * dp, tab + p * tp, f + p * fp, d, epi);
 }
 
 __global__ void __launch_bounds__(kTileThreads, kGatherMinBlocks)
@@ -314,6 +335,17 @@ int launch_interp(const float* f, long long fp, long long ff, const float* disp,
   if (e) return e;
   k_interp<<<tile_grid(d, nprob, nf), kTileThreads, kGatherSmemBytes, s>>>(f, fp, ff, disp, dp, tab, tp, out, op,
                                                                            of, d, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_interp16(const bf16* f, long long fp, const float* disp, long long dp, const int4* tab, long long tp,
+                    bf16* out, long long op, int nprob, const Dims& d, const int* active, cudaStream_t s) {
+  // staged boxes load 4-element chunks as 8-byte words (only when N3 % 4 == 0)
+  if (!(d.n3 & 3) && ((reinterpret_cast<uintptr_t>(f) & 7) || (fp & 3))) return (int)cudaErrorInvalidValue;
+  int e = allow_smem(k_interp16);
+  if (e) return e;
+  k_interp16<<<tile_grid(d, nprob, 1), kTileThreads, kGatherSmemBytes, s>>>(f, fp, disp, dp, tab, tp, out, op, d,
+                                                                            active);
   return (int)cudaGetLastError();
 }
 

@@ -5,6 +5,11 @@
 
 namespace cb {
 
+// Field loads of the gathers: FP32 fields, or bf16 image volumes widened to
+// FP32 (the tricubic sums are always FP32).
+CB_DEVICE float ld_field(const float* p) { return __ldg(p); }
+CB_DEVICE float ld_field(const bf16* p) { return __bfloat162float(__ldg(p)); }
+
 // Tricubic Lagrange stencil at point i + disp (grid units), periodic.
 // Reference: src/interp3.cpp:2492-2719 (base = floor(q) - 1, t = q - base in
 // [1,2), w_k(t) = c_k prod_{l != k}(t - l)).  With s = t - 1 = frac(disp):
@@ -44,13 +49,14 @@ CB_DEVICE void make_stencil(int i1, int i2, int i3, float d1, float d2, float d3
 }
 
 // Sum over one x1 plane of the stencil (16 taps).
-CB_DEVICE float gather_plane(const float* __restrict__ plane, const Stencil& st) {
+template <class T>
+CB_DEVICE float gather_plane(const T* __restrict__ plane, const Stencil& st) {
   float acc = 0.f;
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
-    const float* row = plane + st.o2[b];
-    const float r = st.w3[0] * __ldg(row + st.o3[0]) + st.w3[1] * __ldg(row + st.o3[1]) +
-                    st.w3[2] * __ldg(row + st.o3[2]) + st.w3[3] * __ldg(row + st.o3[3]);
+    const T* row = plane + st.o2[b];
+    const float r = st.w3[0] * ld_field(row + st.o3[0]) + st.w3[1] * ld_field(row + st.o3[1]) +
+                    st.w3[2] * ld_field(row + st.o3[2]) + st.w3[3] * ld_field(row + st.o3[3]);
     acc += st.w2[b] * r;
   }
   return acc;
@@ -60,7 +66,8 @@ CB_DEVICE float gather_plane(const float* __restrict__ plane, const Stencil& st)
 // flight per thread) so the kernel stays at a register count that keeps 32+
 // warps resident per SM; the plane loop selects offsets and weights with
 // compile-time indices only.
-CB_DEVICE float gather(const float* __restrict__ f, const Stencil& st) {
+template <class T>
+CB_DEVICE float gather(const T* __restrict__ f, const Stencil& st) {
   float acc = st.w1[0] * gather_plane(f + st.o1[0], st);
   acc += st.w1[1] * gather_plane(f + st.o1[1], st);
   acc += st.w1[2] * gather_plane(f + st.o1[2], st);
@@ -91,6 +98,11 @@ long long tile_table_int4s(const Dims& d);
 int launch_interp(const float* f, long long fp, long long ff, const float* disp, long long dp, const int4* tab,
                   long long tp, float* out, long long op, long long of, int nf, int nprob, const Dims& d,
                   const int* active, cudaStream_t s);
+
+// Same for one bf16 image field per problem (state levels stored in bf16):
+// taps widened to FP32, sums in FP32, the result rounded to bf16.
+int launch_interp16(const bf16* f, long long fp, const float* disp, long long dp, const int4* tab, long long tp,
+                    bf16* out, long long op, int nprob, const Dims& d, const int* active, cudaStream_t s);
 
 // out[p] = c[p] * f[p](i + disp[p](i)): one backward RK2 step of the
 // (incremental) adjoint, lambda^{l-1} = c * lambda^l(X) with the per-point

@@ -244,6 +244,41 @@ CB_DEVICE void issue_box(float* __restrict__ sb, const float* __restrict__ f, co
   }
 }
 
+// bf16 image field: the same box, widened to FP32 while it is staged.  Each
+// 4-element chunk is one 8-byte load (x3 offsets are multiples of 4 and N3 %
+// 4 == 0, so every chunk is 8-byte aligned) and one 16-byte shared store; the
+// shared-memory layout, and so the gather that reads it, is the FP32 one.
+CB_DEVICE void issue_box(float* __restrict__ sb, const bf16* __restrict__ f, const TileBox& bx, const Dims& d) {
+  const int nck = bx.e3 >> 2;
+  const int rpi = small_div(32, nck);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lr = small_div(lane, nck), lc = lane - lr * nck;
+  if (lr >= rpi || lr >= bx.e2) return;
+  int g1 = wrap_near(bx.lo[0] + warp, d.n1);
+  const int w2 = wrap_near(bx.lo[1] + lr, d.n2);
+  int g3 = wrap_near(bx.lo[2], d.n3) + 4 * lc;
+  g3 -= (g3 >= d.n3) ? d.n3 : 0;
+  const bf16* fb = f + g3;
+  const unsigned row = (unsigned)d.n3, plane = (unsigned)d.n2 * (unsigned)d.n3;
+  constexpr int kWarps = kTileThreads / 32;
+  for (int l1 = warp; l1 < bx.e1; l1 += kWarps) {
+    const bf16* fp = fb + (unsigned)g1 * plane;
+    float* sp = sb + l1 * bx.Q + lr * bx.P + 4 * lc;
+    int g2 = w2;
+    for (int l2 = lr; l2 < bx.e2; l2 += rpi) {
+      const uint2 raw = __ldg(reinterpret_cast<const uint2*>(fp + (unsigned)g2 * row));
+      const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+      const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+      *reinterpret_cast<float4*>(sp) = make_float4(lo.x, lo.y, hi.x, hi.y);
+      sp += rpi * bx.P;
+      g2 += rpi;
+      while (g2 >= d.n2) g2 -= d.n2;
+    }
+    g1 += kWarps;
+    g1 -= (g1 >= d.n1) ? d.n1 : 0;
+  }
+}
+
 // Four consecutive floats at byte offset OFF from addr, weighted by w.
 template <int OFF>
 CB_DEVICE float row4(unsigned addr, const float (&w)[4]) {
@@ -335,10 +370,11 @@ CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ 
 // Tile gather of one field at a displacement field with a precomputed box
 // table: the box copy is issued first and the points' displacements (and the
 // epilogue's per-point operand epi.aux, when it has one) load while it is in
-// flight; epi(tt, a, value, aux_a) finishes point a.
-template <class Epi>
+// flight; epi(tt, a, value, aux_a) finishes point a.  T = bf16 stages an
+// image field synchronously (widened to FP32 on the way to shared memory).
+template <class Epi, class T = float>
 CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const int4* __restrict__ tab,
-                               const float* __restrict__ f, const Dims& d, const Epi& epi) {
+                               const T* __restrict__ f, const Dims& d, const Epi& epi) {
   const TileBox bx = box_from_table(tab, d);
   const bool staged = bx.within && bx.vol <= kGatherBudget;
   if (staged) {

@@ -100,7 +100,7 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 Solver::~Solver() {
   prof_clear();
   if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
-  void* ptrs[] = {mR, mT, v, vtrial, m, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
+  void* ptrs[] = {mR, mT, m, mR16, mT16, m16, v, vtrial, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
                   r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -132,9 +132,8 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   const long long n = d.n(), nc = d.nc();
   const int nt = o.nt;
   long long floats = 0;
-  floats += 2 * n;                    // mR, mT
+  const long long image_bytes = (nt + 3) * n * (o.bf16_images ? 2 : 4);  // mR, mT, state levels
   floats += 2 * 3 * n;                // v, vtrial
-  floats += (nt + 1) * n;             // state
   floats += 2 * 3 * n;                // trajectories
   floats += (nt + 1) * 3 * n;         // grad m cache
   floats += nt * 3 * n;               // grad m (X) cache
@@ -142,7 +141,7 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   floats += (nt + 1) * n;             // adjoint levels
   floats += nt * n;                   // incremental state sources
   floats += 3 * n * 9;                // bf, g, x, r, z, p, q, vtx, work3
-  long long bytes = floats * 4 + 3 * nc * 8;
+  long long bytes = floats * 4 + image_bytes + 3 * nc * 8;
   bytes += 2 * tile_table_int4s(d) * 16;  // box tables of the two characteristics
   bytes += (long long)max_parts(d) * 8;
   return bytes * B;
@@ -178,11 +177,19 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   }
   stream = own_stream;
   const size_t S = sizeof(float) * n * B, V = 3 * S;
-  CB_TRY(alloc((void**)&mR, S));
-  CB_TRY(alloc((void**)&mT, S));
+  img16 = o.bf16_images != 0;
+  if (img16) {
+    const size_t S16 = sizeof(bf16) * n * B;
+    CB_TRY(alloc((void**)&mR16, S16));
+    CB_TRY(alloc((void**)&mT16, S16));
+    CB_TRY(alloc((void**)&m16, S16 * (nt + 1)));
+  } else {
+    CB_TRY(alloc((void**)&mR, S));
+    CB_TRY(alloc((void**)&mT, S));
+    CB_TRY(alloc((void**)&m, S * (nt + 1)));
+  }
   CB_TRY(alloc((void**)&v, V));
   CB_TRY(alloc((void**)&vtrial, V));
-  CB_TRY(alloc((void**)&m, S * (nt + 1)));
   CB_TRY(alloc((void**)&disp_st, V));
   CB_TRY(alloc((void**)&disp_adj, V));
   TP = tile_table_int4s(d);
@@ -219,8 +226,13 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     return CB_ERR_ALLOC;
   }
   cudaMemsetAsync(v, 0, V, stream);
-  cudaMemsetAsync(mR, 0, S, stream);
-  cudaMemsetAsync(mT, 0, S, stream);
+  if (img16) {
+    cudaMemsetAsync(mR16, 0, sizeof(bf16) * n * B, stream);
+    cudaMemsetAsync(mT16, 0, sizeof(bf16) * n * B, stream);
+  } else {
+    cudaMemsetAsync(mR, 0, S, stream);
+    cudaMemsetAsync(mT, 0, S, stream);
+  }
   cudaMemsetAsync(dsc, 0, sizeof(double) * NSLOT * B, stream);
   cudaMemsetAsync(dint, 0, sizeof(int) * NISLOT * B, stream);
   ps.assign(B, ProbState());
@@ -309,15 +321,94 @@ int Solver::characteristic(const float* vel, float sign, const int* act) {
 }
 
 int Solver::state_solve(const float* vel, const int* act) {
-  const long long PM = (nt + 1) * n;
   CB_TRY(characteristic(vel, 1.f, act));
-  CB_TRY(launch_lincomb(m, PM, mT, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+  CB_TRY(state_init(nullptr, act));
+  return state_steps(act);
+}
+
+// ---- image state in its storage type ------------------------------------------
+// FP32 images: m, mR, mT.  bf16 images: m16, mR16, mT16, with every gather and
+// every reduction computed in FP32 / FP64 and only the stored values rounded.
+
+int Solver::state_init(const float* m0, const int* act) {
+  const long long PM = (nt + 1) * n;
+  if (img16) {
+    if (m0) CB_TRY(launch_to_bf16(m0, n, m16, PM, n, B, act, stream));
+    else CB_TRY(launch_copy_bf16(m16, PM, mT16, n, n, B, act, stream));
+  } else {
+    CB_TRY(launch_lincomb(m, PM, m0 ? m0 : mT, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+  }
+  note_launches(1);
+  return 0;
+}
+
+int Solver::state_steps(const int* act) {
+  const long long PM = (nt + 1) * n;
   for (int j = 0; j < nt; ++j) {
     CB_TRY(prof_mark(CB_PROF_STATE_STEP));
-    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, tab_st, TP, m + (j + 1) * n, PM, n, 1, B, d, act, stream));
+    if (img16)
+      CB_TRY(launch_interp16(m16 + j * n, PM, disp_st, 3 * n, tab_st, TP, m16 + (j + 1) * n, PM, B, d, act, stream));
+    else
+      CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, tab_st, TP, m + (j + 1) * n, PM, n, 1, B, d, act,
+                           stream));
     CB_TRY(prof_mark(CB_PROF_STATE_STEP));
   }
-  note_launches(2 + nt);
+  note_launches(nt);
+  return 0;
+}
+
+int Solver::state_out(float* m1, long long m1p, const int* act) {
+  const long long PM = (nt + 1) * n;
+  if (img16) CB_TRY(launch_from_bf16(m16 + nt * n, PM, 0, m1, m1p, 0, n, 1, B, act, stream));
+  else CB_TRY(launch_lincomb(m1, m1p, m + nt * n, PM, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+  note_launches(1);
+  return 0;
+}
+
+int Solver::image_diff_sumsq(bool template_image, const int* act) {
+  const long long PM = (nt + 1) * n;
+  if (img16) {
+    const bf16* b = template_image ? mT16 : m16 + nt * n;
+    CB_TRY(launch_diff_sumsq16(mR16, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
+  } else {
+    const float* b = template_image ? mT : m + nt * n;
+    CB_TRY(launch_diff_sumsq(mR, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
+  }
+  note_launches(1);
+  return 0;
+}
+
+int Solver::image_residual(float* y, long long yp, const int* act) {
+  const long long PM = (nt + 1) * n;
+  if (img16) CB_TRY(launch_diff16(y, yp, mR16, n, m16 + nt * n, PM, n, B, act, stream));
+  else CB_TRY(launch_lincomb(y, yp, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
+  note_launches(1);
+  return 0;
+}
+
+// grad m^j for j = 0..nt into gm.  bf16 levels are widened into gx first: gx
+// is free here (it caches (grad m^j)(X), rebuilt by hessian_prep after every
+// gradient) and holds 3nt >= nt+1 fields per problem.
+int Solver::image_grad(const int* act) {
+  const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n;
+  if (img16) {
+    CB_TRY(launch_from_bf16(m16, PM, n, gx, PGX, n, n, nt + 1, B, act, stream));
+    note_launches(1);
+    return grad_fields(gx, PGX, n, gm, PGM, 3 * n, nt + 1, act);
+  }
+  return grad_fields(m, PM, n, gm, PGM, 3 * n, nt + 1, act);
+}
+
+int Solver::load_images(int b, const float* mRd, const float* mTd) {
+  if (b < 0 || b >= B) return CB_ERR_ARG;
+  if (img16) {
+    CB_TRY(launch_to_bf16(mRd, 0, mR16 + b * n, 0, n, 1, nullptr, stream));
+    CB_TRY(launch_to_bf16(mTd, 0, mT16 + b * n, 0, n, 1, nullptr, stream));
+  } else if (cudaMemcpyAsync(mR + b * n, mRd, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||
+             cudaMemcpyAsync(mT + b * n, mTd, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess) {
+    return CB_ERR_CUDA;
+  }
+  state_of[b] = 0;
   return 0;
 }
 
@@ -374,11 +465,10 @@ void Solver::prof_clear() {
 
 // D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)
 int Solver::distance(const int* act) {
-  const long long PM = (nt + 1) * n;
   const int np = dot_partials(n);
-  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, act, stream));
+  CB_TRY(image_diff_sumsq(false, act));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_D), B, 0.5 * (double)hd, false, stream));
-  note_launches(2);
+  note_launches(1);
   return 0;
 }
 
@@ -586,12 +676,12 @@ int Solver::finish_with_reg(const float* vin, float* out, const int* act, const 
 int Solver::gradient(const int* act) {
   const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
   CB_TRY(characteristic(v, -1.f, act));
-  CB_TRY(grad_fields(m, PM, n, gm, PGM, 3 * n, nt + 1, act));
+  CB_TRY(image_grad(act));
   CB_TRY(divergence(v, divv, act));
   CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, tab_adj, TP, cadj, n, ht, B, d, act, stream));
   // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222)
-  CB_TRY(launch_lincomb(lamh + nt * n, PL, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
-  note_launches(3);
+  CB_TRY(image_residual(lamh + nt * n, PL, act));
+  note_launches(2);
   CB_TRY(finish_with_reg(v, g, act));
   CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, act));
   return 0;
@@ -731,14 +821,10 @@ int Solver::precond(const float* rin, float* zout, const std::vector<int>& sel) 
 int Solver::forward(const float* m0, float* m1, const std::vector<int>& sel) {
   // m0 / m1 are device arrays laid out like mT (problem stride n)
   CB_TRY(upload_mask(sel, dact));
-  const long long PM = (nt + 1) * n;
   CB_TRY(characteristic(v, 1.f, dact));
-  CB_TRY(launch_lincomb(m, PM, m0, n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
-  for (int j = 0; j < nt; ++j)
-    CB_TRY(launch_interp(m + j * n, PM, n, disp_st, 3 * n, tab_st, TP, m + (j + 1) * n, PM, n, 1, B, d, dact,
-                         stream));
-  CB_TRY(launch_lincomb(m1, n, m + nt * n, PM, nullptr, 1.0, nullptr, 0, nullptr, 0.0, n, B, dact, stream));
-  note_launches(3 + nt);
+  CB_TRY(state_init(m0, dact));
+  CB_TRY(state_steps(dact));
+  CB_TRY(state_out(m1, n, dact));
   for (int b = 0; b < B; ++b)
     if (sel[b]) state_of[b] = 0;  // state now belongs to m0, not mT
   return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
@@ -751,8 +837,12 @@ int Solver::final_state(float* m1, int b) {
     CB_TRY(objective_at(v, sel));
   }
   const long long PM = (nt + 1) * n;
-  if (cudaMemcpyAsync(m1, m + b * PM + nt * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+  if (img16) {
+    CB_TRY(launch_from_bf16(m16 + b * PM + nt * n, 0, 0, m1, 0, 0, n, 1, 1, nullptr, stream));
+  } else if (cudaMemcpyAsync(m1, m + b * PM + nt * n, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) !=
+             cudaSuccess) {
     return CB_ERR_CUDA;
+  }
   return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
 }
 
@@ -1041,13 +1131,12 @@ int Solver::finish(const std::vector<int>& sel) {
   if (!anysel) return 0;
   if (anyneed) CB_TRY(objective_at(v, need));
   CB_TRY(upload_mask(sel, dact));
-  const long long PM = (nt + 1) * n;
   const int np = dot_partials(n);
-  CB_TRY(launch_diff_sumsq(mR, n, m + nt * n, PM, n, B, partials, maxparts, dact, stream));
+  CB_TRY(image_diff_sumsq(false, dact));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_PQ), B, 1.0, false, stream));
-  CB_TRY(launch_diff_sumsq(mR, n, mT, n, n, B, partials, maxparts, dact, stream));
+  CB_TRY(image_diff_sumsq(true, dact));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream));
-  note_launches(4);
+  note_launches(2);
   CB_TRY(fetch_scalars());
   const auto t1 = std::chrono::steady_clock::now();
   for (int b = 0; b < B; ++b) {

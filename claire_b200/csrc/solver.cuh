@@ -55,6 +55,9 @@ class Solver {
   int forward(const float* m0, float* m1, const std::vector<int>& sel);
   int det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<double>& stats);
   int final_state(float* m1, int b);
+  // images of problem b from device arrays (n floats each), converted to the
+  // storage type; not synchronised
+  int load_images(int b, const float* mRd, const float* mTd);
   int set_problem(int b, const claire_b200_opts& o);
   long long footprint() const { return bytes_; }
 
@@ -77,6 +80,10 @@ class Solver {
   float *divv = nullptr, *cadj = nullptr, *lamh = nullptr, *bf = nullptr;
   float *g = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *q = nullptr;
   float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *sj = nullptr, *work3 = nullptr;
+  // bf16-image mode (opts.bf16_images): mR, mT and the state levels live in
+  // these arrays instead (same layout); mR / mT / m above stay null.
+  bool img16 = false;
+  bf16 *mR16 = nullptr, *mT16 = nullptr, *m16 = nullptr;
   float2* spec = nullptr;
   double* partials = nullptr;
   int maxparts = 0;
@@ -124,6 +131,13 @@ class Solver {
 
   // building blocks (act: device mask)
   int characteristic(const float* vel, float sign, const int* act);
+  // image-state steps in the storage type (FP32 or bf16)
+  int state_init(const float* m0, const int* act);  // m^0 = m0 (device, stride n), or mT if null
+  int state_steps(const int* act);                  // m^{j+1} = m^j(X_state), j < nt
+  int state_out(float* m1, long long m1p, const int* act);  // m1 = m^nt (FP32)
+  int image_diff_sumsq(bool template_image, const int* act);  // partials of (mR - m^nt or mT)^2
+  int image_residual(float* y, long long yp, const int* act);  // y = mR - m^nt
+  int image_grad(const int* act);                              // gm = grad m^j, j <= nt
   int state_solve(const float* vel, const int* act);
   int distance(const int* act);
   int reg_functional(const float* vel, const std::vector<int>& sel, const int* act);

@@ -139,6 +139,13 @@ int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt,
 /* SemiLagrangian::Interpolate (src/SemiLagrangian.cpp:536-727): out[k] =
  * f[k](i + disp) for k < dof (dof 1 or 3), tricubic (src/interp3.cpp:2492-2719). */
 int claire_b200_interp3(const float* f, const float* disp, float* out, const int nx[3], int dof, void* stream);
+/* The same gather of one bfloat16 volume (the -bf16images storage of the
+ * images and state levels): f and out hold bfloat16 bit patterns, the 64-tap
+ * sum is FP32 and rounded to nearest even.  No reference counterpart (the
+ * reference interpolates single or double precision images); f must be
+ * 8-byte aligned when nx[2] % 4 == 0. */
+int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigned short* out, const int nx[3],
+                             void* stream);
 /* accfft_grad_t: g (3n) = spectral gradient of f (n), Nyquist zeroed. */
 int claire_b200_fft_grad(const float* f, float* g, const int nx[3], void* stream);
 /* accfft_divergence_t: d (n) = spectral divergence of v (3n). */

@@ -413,6 +413,17 @@ def leray_projection(b: np.ndarray, model: str = "stokes", beta_v: float = 1e-2,
 # --------------------------------------------------------------------------
 
 
+def bf16_round(x: np.ndarray) -> np.ndarray:
+    """Values of x stored as bfloat16 (the upper 16 bits of the float32
+    pattern), rounded to nearest with ties to even, returned as float64.
+    x is first rounded to float32 (the device computes the stored values in
+    FP32).  This emulates the library's bf16 image storage; the reference has
+    no such format."""
+    u = np.asarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 class Problem:
     """One SL2 registration problem with the GN (single time level) storage layout.
 
@@ -421,8 +432,14 @@ class Problem:
     """
 
     def __init__(self, mR, mT, nt: int, reg: Regularization, dtype=np.float64,
-                 projection: Optional[str] = None):
+                 projection: Optional[str] = None, image_store=None):
+        # image_store: rounding applied to every stored image value (mR, mT
+        # and each state level), e.g. bf16_round; None keeps dtype values
         self.dtype = dtype
+        self.image_store = image_store
+        if image_store is not None:
+            mR = image_store(mR)
+            mT = image_store(mT)
         self.mR = np.asarray(mR, dtype=dtype)
         self.mT = np.asarray(mT, dtype=dtype)
         self.shape = self.mR.shape
@@ -467,6 +484,8 @@ class Problem:
         tr = self.traj_state()
         for j in range(self.nt):
             m[j + 1] = tr.interp(m[j])
+            if self.image_store is not None:
+                m[j + 1] = self.image_store(m[j + 1])
         self.m = m
         self.counters["pdesolve"] += 1
         return m

@@ -56,6 +56,8 @@ def test_parse_args():
     assert tuple(o.nx) == (64, 64, 64) and o.nt == 8
     assert o.regnorm == cb.NORMS["h2"] and o.model == cb.MODELS["compressible"]
     assert o.beta[0] == 1e-3 and o.maxit == 10 and o.opttol == 1e-2 and o.krylovfseq == 1
+    assert o.bf16_images == 0
+    assert cb.RegOpt(["-nx", "64", "-bf16images"]).opts.bf16_images == 1
     opt2 = cb.RegOpt(["-nx", "96", "-regnorm", "h1s-stokes"])
     assert tuple(opt2.opts.nx) == (96, 96, 96) and opt2.opts.model == cb.MODELS["stokes"]
 

@@ -209,3 +209,14 @@ def test_det_def_grad_known_answers():
     ji, _ = R.det_def_grad(vr, 8, inverse=True)
     assert np.abs(jf - 1).max() > 1e-3
     assert np.abs(jf * ji - 1).max() < 0.1 * np.abs(jf - 1).max()
+
+
+def test_bf16_round_known_answers():
+    # round to nearest, ties to even, on the float32 bit pattern
+    x = np.array([1 + 2 ** -8, 1 + 3 * 2 ** -8, 1 + 2 ** -7, 1 - 2 ** -10, -2.5, 0.0, 3.0e38], np.float32)
+    want = np.array([1.0, 1 + 2 ** -6, 1 + 2 ** -7, 1.0, -2.5, 0.0, 2.9996e38], np.float64)
+    got = R.bf16_round(x)
+    assert np.array_equal(got[:6], want[:6])
+    assert abs(got[6] / 3.0e38 - 1) < 2 ** -8
+    y = np.random.default_rng(0).standard_normal(1000)
+    assert np.max(np.abs(R.bf16_round(y) / y - 1)) <= 2 ** -8
