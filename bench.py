@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--requests", type=int, default=40, help="--serve: number of requests")
     ap.add_argument("--rate", type=float, default=20.0, help="--serve: arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="--serve: slots per pool")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default FFT variants (no measurement)")
     ap.add_argument("--mixed", action="store_true",
                     help="mixed batch instead: 12 x 64^3 + 12 x 96^3 + 8 x 128^3 (H1 beta=1e-2, nt=4) served "
                          "together against plain one-at-a-time runs")
@@ -171,6 +172,7 @@ def run_ours(a, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     B = a.batch
+    tuned = None if a.no_autotune else tune(cb, [a.n], B)
     # seeded inputs: problem index = rank*B + b
     probs = [synthetic.ellipsoid_problem(a.n, a.nt, 1, rank * B + b, dev) for b in range(B)]
     host = [(p[0].cpu().pin_memory(), p[1].cpu().pin_memory()) for p in probs]
@@ -277,7 +279,16 @@ def run_ours(a, rank, world, local):
     roof = roofline(cb, a, ci, load_device, B) if rank == 0 else None
     ci.close()
     return dict(total_ms=total_ms, lat=lat_all, lat_srv=lat_srv, stats=stats, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
-                launches=launches, clocks=clk.summary(), plain=plain, roof=roof)
+                launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned)
+
+
+def tune(cb, sizes, nbatch):
+    """FFT variant per grid size by measurement (claire_b200_autotune), before any timing."""
+    out = {}
+    for n in sizes:
+        v, times = cb.autotune(n, nbatch)
+        out[str(n)] = {"variant": v, "ms_per_candidate": {str(k): round(t, 4) for k, t in times.items()}}
+    return out
 
 
 def roofline(cb, a, ci, load_device, B):
@@ -507,6 +518,7 @@ def run_mixed(a, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     nt, norm, beta = 4, "h1", 1e-2
+    tuned = None if a.no_autotune else tune(cb, sorted(set(MIXED)), a.mixed_slots)
     probs = []
     for i, n in enumerate(MIXED):
         mR, mT, _ = synthetic.ellipsoid_problem(n, nt, 2, rank * len(MIXED) + i, dev)
@@ -583,7 +595,8 @@ def run_mixed(a, rank, world, local):
                                   "what": "per request, submit of host images to host velocity, all 32 "
                                           "submitted at once"},
                    "mean_gn_iterations": float(np.mean([r[1]["gn_iterations"] for r in res])),
-                   "mean_pcg_iterations": float(np.mean([r[1]["pcg_iterations"] for r in res]))},
+                   "mean_pcg_iterations": float(np.mean([r[1]["pcg_iterations"] for r in res])),
+                   "fft_variants": tuned or "defaults (--no-autotune)"},
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -610,6 +623,7 @@ def run_precision(a, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n, nt, norm, beta = 256, 8, "h2", 1e-4
+    tuned = None if a.no_autotune else tune(cb, [n], 1)
     mR, mT, vrec = synthetic.ellipsoid_problem(n, nt, 3, rank, dev)
     v = (0.5 * vrec).cpu().numpy()
     vt = np.random.default_rng(3).standard_normal(v.shape).astype(np.float32) * float(np.std(v))
@@ -676,6 +690,7 @@ def run_precision(a, rank, world, local):
                        "gradient_rel_l2": rel(h["g"], f["g"]),
                        "hessian_matvec_rel_l2": rel(h["H"], f["H"])},
                    "solve": {"fp32": solve(f), "bf16": solve(h)},
+                   "fft_variants": tuned or "defaults (--no-autotune)",
                    "reference_for_errors": "the FP32-image result on the same GPU (no FP64 device path)"},
     }
     print(json.dumps(line), flush=True)
@@ -742,7 +757,8 @@ def main():
                                              ("gn_iterations", "pcg_iterations", "hess_matvecs", "pc_matvecs",
                                               "obj_evals", "grad_evals")},
                    "hess_matvecs_per_s": float(sum(s["hess_matvecs"] for s in r["stats"]) * world * a.steps
-                                               / (r["total_ms"] / 1e3))},
+                                               / (r["total_ms"] / 1e3)),
+                   "fft_variants": r["tuned"] or "defaults (--no-autotune)"},
         "e2e": {"value": regs / (r["e2e_ms"] / 1e3), "unit": "registrations/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "path": "claire_b200_server_submit / _wait / _result (host buffers)"},

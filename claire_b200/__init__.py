@@ -57,7 +57,7 @@ class Opts(ctypes.Structure):
         ("gatol", ctypes.c_double), ("krylovmaxit", ctypes.c_int), ("krylovtol", ctypes.c_double * 3),
         ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int), ("betacont", ctypes.c_double),
-        ("presolvetol", ctypes.c_double),
+        ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int),
     ]
 
 
@@ -123,6 +123,9 @@ _signatures = {
     "claire_b200_interp3": (_I, [_P, _P, _P, _IA, _I, _P]),
     "claire_b200_interp3_bf16": (_I, [_P, _P, _P, _IA, _P]),
     "claire_b200_fft_grad": (_I, [_P, _P, _IA, _P]),
+    "claire_b200_autotune": (_I, [_I, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
+    "claire_b200_fft_variant": (_I, [_I]),
+    "claire_b200_set_fft_variant": (_I, [_I, _I]),
     "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
     "claire_b200_reg_apply": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
     "claire_b200_reg_functional": (_I, [_P, _DA, _IA, _I, _DA, _P]),
@@ -159,6 +162,29 @@ def _check(code: int, where: str, ctx=None):
             raw = lib.claire_b200_last_error(ctx)
             detail = raw.decode() if raw else ""
         raise ClaireError(code, where, detail)
+
+
+def autotune(n: int, nbatch: int = 1):
+    """Measure the FFT variants of n-point grids (claire_b200_autotune) and keep
+    the fastest for this process; returns (variant, {variant: ms})."""
+    v = ctypes.c_int()
+    ms = (ctypes.c_float * 4)()
+    _check(lib.claire_b200_autotune(int(n), int(nbatch), _stream(), ctypes.byref(v), ms), "autotune")
+    cand = fft_variant_candidates(n)
+    return v.value, {c: float(ms[i]) for i, c in enumerate(cand)}
+
+
+def fft_variant_candidates(n: int):
+    """FFT variants the autotuner tries for n-point grids (bit 0: radix plan, bit 1: lines per CTA)."""
+    return [0, 2] if n in (16, 256) else [0, 1, 2, 3]
+
+
+def fft_variant(n: int) -> int:
+    return int(lib.claire_b200_fft_variant(int(n)))
+
+
+def set_fft_variant(n: int, variant: int) -> None:
+    _check(lib.claire_b200_set_fft_variant(int(n), int(variant)), "set_fft_variant")
 
 
 def kernel_launches() -> int:

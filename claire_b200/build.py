@@ -21,6 +21,11 @@ NVCC_FLAGS = [
 ]
 
 
+# fft.cu instantiates every transform kernel for each grid size and FFT
+# variant: let nvcc split its device compilation over the host's cores
+EXTRA_FLAGS = {"fft.cu": ["--split-compile=0"]}
+
+
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
         if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
@@ -50,7 +55,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
         objs.append(obj)
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        extra = EXTRA_FLAGS.get(src, [])
+        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

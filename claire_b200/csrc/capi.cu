@@ -62,6 +62,7 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->iporder = 3;
   o->verbosity = 0;
   o->bf16_images = 0;
+  o->autotune = 0;
   return CB_OK;
 }
 
@@ -138,6 +139,8 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (next(&val)) return CB_ERR_ARG;
       o->iporder = std::atoi(val);
       if (o->iporder != 3) return CB_ERR_UNSUPPORTED;
+    } else if (!std::strcmp(a, "-autotune")) {
+      o->autotune = 1;
     } else if (!std::strcmp(a, "-bf16images")) {
       o->bf16_images = 1;  // no reference counterpart: bf16 storage of the image volumes
     } else if (!std::strcmp(a, "-verbosity")) {
@@ -452,6 +455,25 @@ int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigne
   cudaFreeAsync(tab, s);
   note_launches(2);
   return cuda_status(e);
+}
+
+int claire_b200_autotune(int n, int nbatch, void* stream, int* variant, float* ms) {
+  if (!fft_size_supported(n) || nbatch < 1) return CB_ERR_ARG;
+  float t[4] = {-1.f, -1.f, -1.f, -1.f};
+  int best = 0;
+  const int e = fft_autotune(n, nbatch, (cudaStream_t)stream, &best, t);
+  if (e) return e == (int)cudaErrorMemoryAllocation ? CB_ERR_ALLOC : CB_ERR_CUDA;
+  if (variant) *variant = best;
+  if (ms)
+    for (int i = 0; i < 4; ++i) ms[i] = t[i];
+  return CB_OK;
+}
+
+int claire_b200_fft_variant(int n) { return fft_size_supported(n) ? fft_variant(n) : -1; }
+
+int claire_b200_set_fft_variant(int n, int variant) {
+  if (!fft_size_supported(n)) return CB_ERR_ARG;
+  return set_fft_variant(n, variant) ? CB_ERR_ARG : CB_OK;
 }
 
 int claire_b200_fft_grad(const float* f, float* gout, const int nx[3], void* stream) {

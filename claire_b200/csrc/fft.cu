@@ -19,6 +19,7 @@
 // Every global->shared load is two-phase: a thread issues all of its loads
 // into registers (compile-time count) before it stores any of them, so each
 // thread keeps 8-32 independent loads in flight.
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 #include <vector>
@@ -62,16 +63,27 @@ bool fft_size_supported(int n) {
 }
 
 // Packed lines per CTA for row kernels, and columns per CTA for column kernels.
-// Lines per CTA.  With 256 threads and at least 32 lines a warp's lanes are
-// 32 consecutive lines at one element index in every radix stage, so the
-// split re / im arrays (odd line pitch) are read and written without bank
-// conflicts; grids of 192 and 256 points use 16 lines to keep two CTAs per SM.
-template <int N> struct RowCfg {
-  static constexpr int P = N <= 32 ? 64 : (N <= 128 ? 32 : 16);
+// With 256 threads and at least 32 lines a warp's lanes are 32 consecutive
+// lines at one element index in every radix stage, so the split re / im
+// arrays (odd line pitch) are read and written without bank conflicts; grids
+// of 192 and 256 points use 16 lines to keep two CTAs per SM.  Variant bit 1
+// selects the alternative line counts the autotuner tries (row chunks must
+// split into whole float4 per thread: P * N % 512 == 0; the 4-field pencil of
+// 256 points keeps 16 columns to fit shared memory).
+template <int N> struct RowLines {
+  static constexpr int base = N <= 32 ? 64 : (N <= 128 ? 32 : 16);
+  static constexpr int alt = N == 16 ? 32 : (N == 32 ? 32 : (N == 48 ? 64 : (N <= 128 ? 16 : 32)));
+};
+template <int N> struct ColLines {
+  static constexpr int base = N <= 128 ? 32 : 16;
+  static constexpr int alt = N <= 128 ? 16 : (N == 192 ? 32 : 16);
+};
+template <int N, int V = 0> struct RowCfg {
+  static constexpr int P = (V & 2) ? RowLines<N>::alt : RowLines<N>::base;
   static constexpr int PITCH = P + 1;
 };
-template <int N> struct ColCfg {
-  static constexpr int C = N <= 128 ? 32 : 16;
+template <int N, int V = 0> struct ColCfg {
+  static constexpr int C = (V & 2) ? ColLines<N>::alt : ColLines<N>::base;
   static constexpr int PITCH = C + 1;
 };
 
@@ -192,13 +204,13 @@ CB_DEVICE void load_row_chunk(float* re, float* im, const float* __restrict__ sr
 // rows: r2c along x3.  Two real rows a, b are packed as z = a + i b; after
 // the complex FFT Z, A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = (Z[k] - conj Z[N-k]) / 2i.
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_r2c_rows(const float* __restrict__ in, long long ip,
                                                         long long ifs, float2* __restrict__ out,
                                                         long long op, long long ofs, int nrows,
                                                         const float2* __restrict__ twg,
                                                         const int* __restrict__ active) {
-  constexpr int P = RowCfg<N>::P, PITCH = RowCfg<N>::PITCH, NH = N / 2 + 1;
+  constexpr int P = RowCfg<N, V>::P, PITCH = RowCfg<N, V>::PITCH, NH = N / 2 + 1;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -213,7 +225,7 @@ __global__ void __launch_bounds__(kThreads) k_r2c_rows(const float* __restrict__
   load_twiddles<N>(tw, twg);
   load_row_chunk<N, P, PITCH>(re, im, src + (long long)row0 * N, nr);
   __syncthreads();
-  fft_lines<N, false, P, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, false, P, PITCH, V>(re, im, sre, sim, tw);
   for (int idx = threadIdx.x; idx < 2 * P * NH; idx += kThreads) {
     const int r = idx / NH, k = idx - r * NH;
     if (r >= nr) continue;
@@ -233,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) k_r2c_rows(const float* __restrict__
 // conj(A[k]) + i conj(B[k]); the imaginary parts of the DC and Nyquist bins
 // are ignored (the c2r convention of FFTW / pocketfft).
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict__ in, long long ip,
                                                         long long ifs, float* __restrict__ out,
                                                         long long op, long long ofs, int nrows,
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
                                                         double* __restrict__ partials, int nparts,
                                                         const float* __restrict__ other,
                                                         const int* __restrict__ active) {
-  constexpr int P = RowCfg<N>::P, PITCH = RowCfg<N>::PITCH, NH = N / 2 + 1;
+  constexpr int P = RowCfg<N, V>::P, PITCH = RowCfg<N, V>::PITCH, NH = N / 2 + 1;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -304,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
     im[e * PITCH + line] = zi;
   }
   __syncthreads();
-  fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, true, P, PITCH, V>(re, im, sre, sim, tw);
   const float al = alpha ? alpha[blockIdx.z] : 1.f;
   const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, oth, row0, nr, epi, al);
   if (epi_reduces(epi)) {
@@ -316,12 +328,12 @@ __global__ void __launch_bounds__(kThreads) k_c2r_rows(const float2* __restrict_
 // complex column FFT along a strided axis, in place
 // column g starts at (g / cpg) * gs + (g % cpg); elements are es apart
 // ---------------------------------------------------------------------------
-template <int N, bool INV>
+template <int N, bool INV, int V>
 __global__ void __launch_bounds__(kThreads) k_cols(float2* __restrict__ data, long long pstr,
                                                     long long fstr, int ncols, int cpg, long long gs,
                                                     long long es, const float2* __restrict__ twg,
                                                     const int* __restrict__ active) {
-  constexpr int C = ColCfg<N>::C, PITCH = ColCfg<N>::PITCH;
+  constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -335,7 +347,7 @@ __global__ void __launch_bounds__(kThreads) k_cols(float2* __restrict__ data, lo
   load_twiddles<N>(tw, twg);
   load_col_tile<N, C, PITCH>(re, im, colp, es);
   __syncthreads();
-  fft_lines<N, INV, C, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, INV, C, PITCH, V>(re, im, sre, sim, tw);
   store_col_tile<N, C, PITCH>(re, im, colp, es);
 }
 
@@ -467,12 +479,12 @@ CB_DEVICE void apply_op3(int op, const SpecParams& q, const Dims& d, int i1, con
 
 // x1 pencil, one field per CTA (grid.y = field): forward FFT along x1, the
 // diagonal symbol, inverse FFT.
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec, long long pstr, long long fstr,
                                                        Dims d, int op, const SpecParams* __restrict__ params,
                                                        const float2* __restrict__ twg,
                                                        const int* __restrict__ active) {
-  constexpr int C = ColCfg<N>::C, PITCH = ColCfg<N>::PITCH;
+  constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
   constexpr int RSTEP = kThreads / C, K = N / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
@@ -492,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
   load_twiddles<N>(tw, twg);
   load_col_tile<N, C, PITCH>(re, im, colp, ncols);
   __syncthreads();
-  fft_lines<N, false, C, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, false, C, PITCH, V>(re, im, sre, sim, tw);
   // one copy of the symbol code (a rolled loop keeps the kernel small enough
   // for the instruction cache)
 #pragma unroll 1
@@ -504,17 +516,17 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
     im[a] = y.y;
   }
   __syncthreads();
-  fft_lines<N, true, C, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, true, C, PITCH, V>(re, im, sre, sim, tw);
   store_col_tile<N, C, PITCH>(re, im, colp, ncols);
 }
 
 // x1 pencil with the three fields in one CTA (coupled projections).
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec, long long pstr, long long fstr,
                                                        Dims d, int op, const SpecParams* __restrict__ params,
                                                        const float2* __restrict__ twg,
                                                        const int* __restrict__ active) {
-  constexpr int C = ColCfg<N>::C, PITCH = ColCfg<N>::PITCH;
+  constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
   constexpr int RSTEP = kThreads / C, K = N / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
@@ -541,7 +553,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
   for (int f = 0; f < 3; ++f) load_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
   __syncthreads();
 #pragma unroll 1
-  for (int f = 0; f < 3; ++f) fft_lines<N, false, C, PITCH>(fre[f], fim[f], sre, sim, tw);
+  for (int f = 0; f < 3; ++f) fft_lines<N, false, C, PITCH, V>(fre[f], fim[f], sre, sim, tw);
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
@@ -558,7 +570,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
   }
   __syncthreads();
 #pragma unroll 1
-  for (int f = 0; f < 3; ++f) fft_lines<N, true, C, PITCH>(fre[f], fim[f], sre, sim, tw);
+  for (int f = 0; f < 3; ++f) fft_lines<N, true, C, PITCH, V>(fre[f], fim[f], sre, sim, tw);
 #pragma unroll
   for (int f = 0; f < 3; ++f) store_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
 }
@@ -581,14 +593,14 @@ CB_DEVICE void mul_ik(float* re, float* im, float hscale) {
   }
 }
 
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict__ in, long long ip,
                                                           long long ifs, float* __restrict__ out,
                                                           long long op, long long ofs, int nrows,
                                                           const float2* __restrict__ twg, int epi,
                                                           double* __restrict__ partials, int nparts,
                                                           const int* __restrict__ active) {
-  constexpr int P = RowCfg<N>::P, PITCH = RowCfg<N>::PITCH;
+  constexpr int P = RowCfg<N, V>::P, PITCH = RowCfg<N, V>::PITCH;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -603,16 +615,16 @@ __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict
   load_twiddles<N>(tw, twg);
   load_row_chunk<N, P, PITCH>(re, im, src + (long long)row0 * N, nr);
   __syncthreads();
-  fft_lines<N, false, P, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, false, P, PITCH, V>(re, im, sre, sim, tw);
   mul_ik<N, P, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
-  fft_lines<N, true, P, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, true, P, PITCH, V>(re, im, sre, sim, tw);
   const double acc = rows_epilogue<N, P, PITCH>(re, im, dst, nullptr, row0, nr, epi, 1.f);
   if (epi == EPI_SUMSQ)
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
 }
 
-template <int N>
+template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict__ in, long long ip,
                                                           long long ifs, float* __restrict__ out,
                                                           long long op, long long ofs, int ncols,
@@ -620,9 +632,9 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
                                                           const float2* __restrict__ twg, int epi,
                                                           double* __restrict__ partials, int nparts,
                                                           const int* __restrict__ active) {
-  constexpr int L = ColCfg<N>::C;       // packed complex lines per CTA
+  constexpr int L = ColCfg<N, V>::C;       // packed complex lines per CTA
   constexpr int C = 2 * L;              // real columns per CTA
-  constexpr int PITCH = ColCfg<N>::PITCH;
+  constexpr int PITCH = ColCfg<N, V>::PITCH;
   constexpr int RSTEP = kThreads / C, K = N / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
@@ -647,10 +659,10 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
     for (int k = 0; k < K; ++k) lane[(e0 + k * RSTEP) * PITCH] = v[k];
   }
   __syncthreads();
-  fft_lines<N, false, L, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, false, L, PITCH, V>(re, im, sre, sim, tw);
   mul_ik<N, L, PITCH>(re, im, 1.f / (float)N);
   __syncthreads();
-  fft_lines<N, true, L, PITCH>(re, im, sre, sim, tw);
+  fft_lines<N, true, L, PITCH, V>(re, im, sre, sim, tw);
   double acc = 0.0;
   if (ok) {
     float old[K];
@@ -673,14 +685,14 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-template <int N> static size_t row_smem(bool c2r) {
-  const size_t scratch = 2 * N * RowCfg<N>::PITCH;           // sre + sim
-  const size_t staging = 2 * 2 * RowCfg<N>::P * (N / 2 + 1);  // c2r half-spectrum rows (shares scratch)
+template <int N, int V> static size_t row_smem(bool c2r) {
+  const size_t scratch = 2 * N * RowCfg<N, V>::PITCH;           // sre + sim
+  const size_t staging = 2 * 2 * RowCfg<N, V>::P * (N / 2 + 1);  // c2r half-spectrum rows (shares scratch)
   const size_t tail = (c2r && staging > scratch) ? staging : scratch;
-  return (2 * N + 2 * N * RowCfg<N>::PITCH + tail) * sizeof(float);
+  return (2 * N + 2 * N * RowCfg<N, V>::PITCH + tail) * sizeof(float);
 }
-template <int N> static size_t col_smem(int nbuf) {
-  return (2 * N + 2 * nbuf * N * ColCfg<N>::PITCH) * sizeof(float);
+template <int N, int V> static size_t col_smem(int nbuf) {
+  return (2 * N + 2 * nbuf * N * ColCfg<N, V>::PITCH) * sizeof(float);
 }
 
 template <typename K> static int set_smem(K kernel, size_t bytes) {
@@ -706,49 +718,131 @@ static bool aligned16(const void* p) { return (reinterpret_cast<unsigned long lo
     default: return (int)cudaErrorInvalidValue;        \
   }
 
-template <int N>
+// ---------------------------------------------------------------------------
+// FFT variants (plan factorization x lines per CTA) chosen per grid size.
+// The table is process-wide; the autotuner (fft_autotune) or
+// set_fft_variant change it, and every launch reads it, so it must only
+// change while no transform of that size is in flight (contexts tune when
+// they are created, before any of their work).
+// ---------------------------------------------------------------------------
+static std::atomic<int> g_fft_var[8];
+
+static int size_slot(int n) {
+  switch (n) {
+    case 16: return 0;
+    case 32: return 1;
+    case 48: return 2;
+    case 64: return 3;
+    case 96: return 4;
+    case 128: return 5;
+    case 192: return 6;
+    case 256: return 7;
+    default: return -1;
+  }
+}
+
+int fft_variant_candidates(int n, int* out) {
+  const int k = size_slot(n);
+  if (k < 0) return 0;
+  if (n == 16 || n == 256) {  // one factorization: line counts only
+    out[0] = 0;
+    out[1] = 2;
+    return 2;
+  }
+  for (int v = 0; v < 4; ++v) out[v] = v;
+  return 4;
+}
+
+int fft_variant(int n) {
+  const int k = size_slot(n);
+  return k < 0 ? 0 : g_fft_var[k].load(std::memory_order_relaxed);
+}
+
+int set_fft_variant(int n, int v) {
+  int cand[4];
+  const int nc = fft_variant_candidates(n, cand);
+  for (int i = 0; i < nc; ++i)
+    if (cand[i] == v) {
+      g_fft_var[size_slot(n)].store(v, std::memory_order_relaxed);
+      return 0;
+    }
+  return (int)cudaErrorInvalidValue;
+}
+
+#define CB_V(VV_, CALL) \
+  case VV_: {           \
+    constexpr int VV = VV_; \
+    CALL;               \
+  } break;
+#define CB_VSW4(N_, CALL)                                                                  \
+  {                                                                                        \
+    constexpr int NN = N_;                                                                 \
+    switch (fft_variant(N_)) { CB_V(0, CALL) CB_V(1, CALL) CB_V(2, CALL) CB_V(3, CALL)     \
+      default: return (int)cudaErrorInvalidValue; }                                        \
+  } break;
+#define CB_VSW2(N_, CALL)                                                                  \
+  {                                                                                        \
+    constexpr int NN = N_;                                                                 \
+    switch (fft_variant(N_)) { CB_V(0, CALL) CB_V(2, CALL)                                 \
+      default: return (int)cudaErrorInvalidValue; }                                        \
+  } break;
+// CB_DISPATCH_N with the size's current variant as the constexpr VV
+#define CB_DISPATCH_NV(n, CALL)      \
+  switch (n) {                       \
+    case 16: CB_VSW2(16, CALL)       \
+    case 32: CB_VSW4(32, CALL)       \
+    case 48: CB_VSW4(48, CALL)       \
+    case 64: CB_VSW4(64, CALL)       \
+    case 96: CB_VSW4(96, CALL)       \
+    case 128: CB_VSW4(128, CALL)     \
+    case 192: CB_VSW4(192, CALL)     \
+    case 256: CB_VSW2(256, CALL)     \
+    default: return (int)cudaErrorInvalidValue; \
+  }
+
+template <int N, int V>
 static int r2c_rows_impl(const float* in, long long ip, long long ifs, float2* out, long long op,
                          long long ofs, int nrows, int nf, int nprob, const int* active,
                          cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  size_t sm = row_smem<N>(false);
-  int e = set_smem(k_r2c_rows<N>, sm);
+  size_t sm = row_smem<N, V>(false);
+  int e = set_smem(k_r2c_rows<N, V>, sm);
   if (e) return e;
-  dim3 grid((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), nf, nprob);
-  k_r2c_rows<N><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op, ofs, nrows, tw, active);
+  dim3 grid((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), nf, nprob);
+  k_r2c_rows<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op, ofs, nrows, tw, active);
   return (int)cudaGetLastError();
 }
 
-template <int N>
+template <int N, int V>
 static int c2r_rows_impl(const float2* in, long long ip, long long ifs, float* out, long long op,
                          long long ofs, int nrows, int nf, int nprob, int epi, const float* alpha,
                          double* partials, int nparts, const float* other, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  size_t sm = row_smem<N>(true);
-  int e = set_smem(k_c2r_rows<N>, sm);
+  size_t sm = row_smem<N, V>(true);
+  int e = set_smem(k_c2r_rows<N, V>, sm);
   if (e) return e;
-  dim3 grid((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), nf, nprob);
-  k_c2r_rows<N><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op, ofs, nrows, tw, epi, alpha, partials,
+  dim3 grid((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), nf, nprob);
+  k_c2r_rows<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op, ofs, nrows, tw, epi, alpha, partials,
                                             nparts, other, active);
   return (int)cudaGetLastError();
 }
 
-template <int N, bool INV>
+template <int N, bool INV, int V>
 static int cols_impl(float2* data, long long pstr, long long fstr, int ncols, int cpg, long long gs,
                      long long es, int nf, int nprob, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  size_t sm = col_smem<N>(2);
-  int e = set_smem(k_cols<N, INV>, sm);
+  size_t sm = col_smem<N, V>(2);
+  int e = set_smem(k_cols<N, INV, V>, sm);
   if (e) return e;
-  dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, nf, nprob);
-  k_cols<N, INV><<<grid, kThreads, sm, s>>>(data, pstr, fstr, ncols, cpg, gs, es, tw, active);
+  dim3 grid((ncols + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, nf, nprob);
+  k_cols<N, INV, V><<<grid, kThreads, sm, s>>>(data, pstr, fstr, ncols, cpg, gs, es, tw, active);
   return (int)cudaGetLastError();
 }
 
-template <int N>
+template <int N, int V>
 static int pencil_impl(float2* spec, long long sp, long long fstr, int nprob, const Dims& d, int op,
                        const SpecParams* params, int nin, int nout, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
@@ -756,18 +850,18 @@ static int pencil_impl(float2* spec, long long sp, long long fstr, int nprob, co
   const int ncols = d.n2 * (d.n3 / 2 + 1);
   if (op == OP_LERAY || op == OP_LERAY_RELAXED) {
     if (nin != 3 || nout != 3) return (int)cudaErrorInvalidValue;
-    size_t sm = col_smem<N>(4);
-    int e = set_smem(k_pencil3<N>, sm);
+    size_t sm = col_smem<N, V>(4);
+    int e = set_smem(k_pencil3<N, V>, sm);
     if (e) return e;
-    dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, 1, nprob);
-    k_pencil3<N><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
+    dim3 grid((ncols + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, 1, nprob);
+    k_pencil3<N, V><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
   } else {
     if (nin != nout) return (int)cudaErrorInvalidValue;
-    size_t sm = col_smem<N>(2);
-    int e = set_smem(k_pencil1<N>, sm);
+    size_t sm = col_smem<N, V>(2);
+    int e = set_smem(k_pencil1<N, V>, sm);
     if (e) return e;
-    dim3 grid((ncols + ColCfg<N>::C - 1) / ColCfg<N>::C, nin, nprob);
-    k_pencil1<N><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
+    dim3 grid((ncols + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, nin, nprob);
+    k_pencil1<N, V><<<grid, kThreads, sm, s>>>(spec, sp, fstr, d, op, params, tw, active);
   }
   return (int)cudaGetLastError();
 }
@@ -782,10 +876,10 @@ int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, lon
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
-  CB_DISPATCH_N(d.n3, e = r2c_rows_impl<NN>(in, ip, ifs, spec, sp, nc, d.n1 * d.n2, nf, nprob, active, s));
+  CB_DISPATCH_NV(d.n3, e = (r2c_rows_impl<NN, VV>(in, ip, ifs, spec, sp, nc, d.n1 * d.n2, nf, nprob, active, s)));
   if (e) return e;
   // x2 columns: column g = (i1, k3) starts at i1*n2*n3h + k3, stride n3h
-  CB_DISPATCH_N(d.n2, e = (cols_impl<NN, false>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
+  CB_DISPATCH_NV(d.n2, e = (cols_impl<NN, false, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
                                                 nf, nprob, active, s)));
   return e;
 }
@@ -794,40 +888,48 @@ int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
                   const SpecParams* dparams, int nin, int nout, const int* active, cudaStream_t s) {
   if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
   int e = 0;
-  CB_DISPATCH_N(d.n1, e = pencil_impl<NN>(spec, sp, d.nc(), nprob, d, op, dparams, nin, nout, active, s));
+  CB_DISPATCH_NV(d.n1, e = (pencil_impl<NN, VV>(spec, sp, d.nc(), nprob, d, op, dparams, nin, nout, active, s)));
   return e;
 }
 
-static int row_lines(int n) {
+// Lines per CTA of the size's current variant (min_over_variants: the
+// smallest over its candidates, which sizes reduction buffers for any variant).
+static int row_lines(int n, bool min_over_variants = false) {
+  int base = 0, alt = 0;
   switch (n) {
-    case 16: return RowCfg<16>::P;
-    case 32: return RowCfg<32>::P;
-    case 48: return RowCfg<48>::P;
-    case 64: return RowCfg<64>::P;
-    case 96: return RowCfg<96>::P;
-    case 128: return RowCfg<128>::P;
-    case 192: return RowCfg<192>::P;
-    case 256: return RowCfg<256>::P;
+    case 16: base = RowLines<16>::base; alt = RowLines<16>::alt; break;
+    case 32: base = RowLines<32>::base; alt = RowLines<32>::alt; break;
+    case 48: base = RowLines<48>::base; alt = RowLines<48>::alt; break;
+    case 64: base = RowLines<64>::base; alt = RowLines<64>::alt; break;
+    case 96: base = RowLines<96>::base; alt = RowLines<96>::alt; break;
+    case 128: base = RowLines<128>::base; alt = RowLines<128>::alt; break;
+    case 192: base = RowLines<192>::base; alt = RowLines<192>::alt; break;
+    case 256: base = RowLines<256>::base; alt = RowLines<256>::alt; break;
     default: return 0;
   }
+  if (min_over_variants) return base < alt ? base : alt;
+  return (fft_variant(n) & 2) ? alt : base;
 }
 
-static int col_lines(int n) {
+static int col_lines(int n, bool min_over_variants = false) {
+  int base = 0, alt = 0;
   switch (n) {
-    case 16: return ColCfg<16>::C;
-    case 32: return ColCfg<32>::C;
-    case 48: return ColCfg<48>::C;
-    case 64: return ColCfg<64>::C;
-    case 96: return ColCfg<96>::C;
-    case 128: return ColCfg<128>::C;
-    case 192: return ColCfg<192>::C;
-    case 256: return ColCfg<256>::C;
+    case 16: base = ColLines<16>::base; alt = ColLines<16>::alt; break;
+    case 32: base = ColLines<32>::base; alt = ColLines<32>::alt; break;
+    case 48: base = ColLines<48>::base; alt = ColLines<48>::alt; break;
+    case 64: base = ColLines<64>::base; alt = ColLines<64>::alt; break;
+    case 96: base = ColLines<96>::base; alt = ColLines<96>::alt; break;
+    case 128: base = ColLines<128>::base; alt = ColLines<128>::alt; break;
+    case 192: base = ColLines<192>::base; alt = ColLines<192>::alt; break;
+    case 256: base = ColLines<256>::base; alt = ColLines<256>::alt; break;
     default: return 0;
   }
+  if (min_over_variants) return base < alt ? base : alt;
+  return (fft_variant(n) & 2) ? alt : base;
 }
 
-int c2r_partials(const Dims& d, int nf) {
-  const int P = row_lines(d.n3);
+int c2r_partials(const Dims& d, int nf, bool any_variant) {
+  const int P = row_lines(d.n3, any_variant);
   if (!P) return 0;
   const int nrows = d.n1 * d.n2;
   return ((nrows + 2 * P - 1) / (2 * P)) * nf;
@@ -841,31 +943,31 @@ int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long lon
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
-  CB_DISPATCH_N(d.n2, e = (cols_impl<NN, true>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
+  CB_DISPATCH_NV(d.n2, e = (cols_impl<NN, true, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
                                                nf, nprob, active, s)));
   if (e) return e;
-  CB_DISPATCH_N(d.n3, e = c2r_rows_impl<NN>(spec, sp, nc, out, op_, ofs, d.n1 * d.n2, nf, nprob, epi, alpha,
-                                            partials, nparts, other, active, s));
+  CB_DISPATCH_NV(d.n3, e = (c2r_rows_impl<NN, VV>(spec, sp, nc, out, op_, ofs, d.n1 * d.n2, nf, nprob, epi, alpha,
+                                            partials, nparts, other, active, s)));
   return e;
 }
 
-template <int N>
+template <int N, int V>
 static int deriv_impl(const float* in, long long ip, long long ifs, float* out, long long op_,
                       long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
                       double* partials, int nparts, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
   if (axis == 2) {
-    size_t sm = row_smem<N>(false);
-    int e = set_smem(k_deriv_rows<N>, sm);
+    size_t sm = row_smem<N, V>(false);
+    int e = set_smem(k_deriv_rows<N, V>, sm);
     if (e) return e;
     const int nrows = d.n1 * d.n2;
-    dim3 grid((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), nf, nprob);
-    k_deriv_rows<N><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, nrows, tw, epi, partials, nparts,
+    dim3 grid((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), nf, nprob);
+    k_deriv_rows<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, nrows, tw, epi, partials, nparts,
                                                 active);
   } else {
-    size_t sm = col_smem<N>(2);
-    int e = set_smem(k_deriv_cols<N>, sm);
+    size_t sm = col_smem<N, V>(2);
+    int e = set_smem(k_deriv_cols<N, V>, sm);
     if (e) return e;
     int ncols, cpg;
     long long gs, es;
@@ -874,22 +976,22 @@ static int deriv_impl(const float* in, long long ip, long long ifs, float* out, 
     } else {          // lines along x1: column (i2, i3)
       ncols = d.n2 * d.n3; cpg = ncols; gs = 0; es = (long long)d.n2 * d.n3;
     }
-    constexpr int C = 2 * ColCfg<N>::C;
+    constexpr int C = 2 * ColCfg<N, V>::C;
     dim3 grid((ncols + C - 1) / C, nf, nprob);
-    k_deriv_cols<N><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, ncols, cpg, gs, es, tw, epi,
+    k_deriv_cols<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, ncols, cpg, gs, es, tw, epi,
                                                 partials, nparts, active);
   }
   return (int)cudaGetLastError();
 }
 
-int deriv_partials(const Dims& d, int axis, int nf) {
+int deriv_partials(const Dims& d, int axis, int nf, bool any_variant) {
   const int n = (axis == 0) ? d.n1 : (axis == 1 ? d.n2 : d.n3);
   if (axis == 2) {
-    const int P = row_lines(n);
+    const int P = row_lines(n, any_variant);
     if (!P) return 0;
     return ((d.n1 * d.n2 + 2 * P - 1) / (2 * P)) * nf;
   }
-  const int C = col_lines(n);
+  const int C = col_lines(n, any_variant);
   if (!C) return 0;
   const int ncols = (axis == 1) ? d.n1 * d.n3 : d.n2 * d.n3;
   return ((ncols + 2 * C - 1) / (2 * C)) * nf;
@@ -902,37 +1004,37 @@ int launch_deriv(const float* in, long long ip, long long ifs, float* out, long 
   if (axis == 2 && (!aligned16(in) || ((ip | ifs) & 3))) return (int)cudaErrorInvalidValue;
   const int n = (axis == 0) ? d.n1 : (axis == 1 ? d.n2 : d.n3);
   int e = 0;
-  CB_DISPATCH_N(n, e = deriv_impl<NN>(in, ip, ifs, out, op_, ofs, nf, nprob, d, axis, epi, partials, nparts,
-                                      active, s));
+  CB_DISPATCH_NV(n, e = (deriv_impl<NN, VV>(in, ip, ifs, out, op_, ofs, nf, nprob, d, axis, epi, partials, nparts,
+                                      active, s)));
   return e;
 }
 
 // 3-field spectral operator (r2c, x1 op, c2r store) on caller-provided
 // spectrum workspace and twiddle table: the launches allocate nothing.
-template <int N>
+template <int N, int V>
 static int spectral3_explicit_impl(const float* in, float* out, float2* spec, const SpecParams* params,
                                    const Dims& d, int op, const float2* tw, cudaStream_t s) {
   const long long n = d.n(), nc = d.nc();
   const int n3h = N / 2 + 1;
   const int nrows = d.n1 * d.n2;
-  int e = set_smem(k_r2c_rows<N>, row_smem<N>(false));
-  if (!e) e = set_smem(k_cols<N, false>, col_smem<N>(2));
-  if (!e) e = set_smem(k_cols<N, true>, col_smem<N>(2));
-  if (!e) e = set_smem(k_pencil1<N>, col_smem<N>(2));
-  if (!e) e = set_smem(k_c2r_rows<N>, row_smem<N>(true));
+  int e = set_smem(k_r2c_rows<N, V>, row_smem<N, V>(false));
+  if (!e) e = set_smem(k_cols<N, false, V>, col_smem<N, V>(2));
+  if (!e) e = set_smem(k_cols<N, true, V>, col_smem<N, V>(2));
+  if (!e) e = set_smem(k_pencil1<N, V>, col_smem<N, V>(2));
+  if (!e) e = set_smem(k_c2r_rows<N, V>, row_smem<N, V>(true));
   if (e) return e;
-  const dim3 rows((nrows + 2 * RowCfg<N>::P - 1) / (2 * RowCfg<N>::P), 3, 1);
+  const dim3 rows((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), 3, 1);
   const int ncx2 = d.n1 * n3h;
-  const dim3 cols((ncx2 + ColCfg<N>::C - 1) / ColCfg<N>::C, 3, 1);
+  const dim3 cols((ncx2 + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, 3, 1);
   const int ncx1 = d.n2 * n3h;
-  const dim3 pen((ncx1 + ColCfg<N>::C - 1) / ColCfg<N>::C, 3, 1);
-  k_r2c_rows<N><<<rows, kThreads, row_smem<N>(false), s>>>(in, 0, n, spec, 0, nc, nrows, tw, nullptr);
-  k_cols<N, false><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+  const dim3 pen((ncx1 + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, 3, 1);
+  k_r2c_rows<N, V><<<rows, kThreads, row_smem<N, V>(false), s>>>(in, 0, n, spec, 0, nc, nrows, tw, nullptr);
+  k_cols<N, false, V><<<cols, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                           nullptr);
-  k_pencil1<N><<<pen, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, d, op, params, tw, nullptr);
-  k_cols<N, true><<<cols, kThreads, col_smem<N>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+  k_pencil1<N, V><<<pen, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, d, op, params, tw, nullptr);
+  k_cols<N, true, V><<<cols, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                          nullptr);
-  k_c2r_rows<N><<<rows, kThreads, row_smem<N>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
+  k_c2r_rows<N, V><<<rows, kThreads, row_smem<N, V>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
                                                            nullptr, 0, nullptr, nullptr);
   return (int)cudaGetLastError();
 }
@@ -941,7 +1043,105 @@ int launch_spectral3_explicit(const float* in, float* out, float2* spec, const S
                               int op, const float2* tw, cudaStream_t s) {
   if (!cubic_supported(d) || !aligned16(in)) return (int)cudaErrorInvalidValue;
   int e = 0;
-  CB_DISPATCH_N(d.n1, e = spectral3_explicit_impl<NN>(in, out, spec, params, d, op, tw, s));
+  CB_DISPATCH_N(d.n1, e = (spectral3_explicit_impl<NN, 0>(in, out, spec, params, d, op, tw, s)));
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner: CLAIRE plans its transforms by measurement (accfft_plan_dft_3d_r2c
+// with ACCFFT_MEASURE, src/RegOpt.cpp:993-994); here the candidates are the
+// variants above, timed on the work the solver does with them.
+// ---------------------------------------------------------------------------
+__global__ void k_tune_fill(float* x, long long len) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    x[i] = __sinf(0.001f * (float)(i % 100003));
+}
+
+static std::atomic<bool> g_fft_tuned[8];
+static std::mutex g_tune_mutex;
+
+bool fft_tuned(int n) {
+  const int k = size_slot(n);
+  return k >= 0 && g_fft_tuned[k].load();
+}
+
+int fft_autotune_once(int n, int nprob, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  if (fft_tuned(n)) return 0;
+  int best = 0;
+  return fft_autotune(n, nprob, s, &best, nullptr);
+}
+
+int fft_autotune(int n, int nprob, cudaStream_t s, int* best, float* ms) {
+  int cand[4];
+  const int ncand = fft_variant_candidates(n, cand);
+  if (!ncand || nprob < 1) return (int)cudaErrorInvalidValue;
+  const Dims d{n, n, n};
+  const long long nn = d.n(), nc = d.nc();
+  float *in = nullptr, *out = nullptr;
+  float2* spec = nullptr;
+  SpecParams* par = nullptr;
+  int e = 0;
+  if (cudaMalloc(&in, sizeof(float) * 3 * nn * nprob) != cudaSuccess ||
+      cudaMalloc(&out, sizeof(float) * 3 * nn * nprob) != cudaSuccess ||
+      cudaMalloc(&spec, sizeof(float2) * 3 * nc * nprob) != cudaSuccess ||
+      cudaMalloc(&par, sizeof(SpecParams) * nprob) != cudaSuccess)
+    e = (int)cudaErrorMemoryAllocation;
+  std::vector<SpecParams> hp(nprob);
+  for (auto& p : hp) {
+    p.norm = NORM_H2;
+    p.beta0 = 1e-3f;
+    p.beta1 = 1e-4f;
+    p.beta2 = 1e-4f;
+    p.hd = 1.f;
+    p.sigma[0] = p.sigma[1] = p.sigma[2] = 1.f;
+  }
+  if (!e) e = (int)cudaMemcpyAsync(par, hp.data(), sizeof(SpecParams) * nprob, cudaMemcpyHostToDevice, s);
+  if (!e) {
+    k_tune_fill<<<148 * 4, 256, 0, s>>>(in, 3 * nn * nprob);
+    e = (int)cudaGetLastError();
+  }
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (!e && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess)) e = (int)cudaErrorUnknown;
+  const int old = fft_variant(n);
+  float best_ms = 0.f;
+  int best_v = old;
+  auto work = [&]() -> int {
+    int r = launch_r2c3d(in, 3 * nn, nn, spec, 3 * nc, 3, nprob, d, nullptr, s);
+    if (!r) r = launch_pencil(spec, 3 * nc, nprob, d, OP_REG_INV, par, 3, 3, nullptr, s);
+    if (!r) r = launch_c2r3d(spec, 3 * nc, out, 3 * nn, nn, 3, nprob, d, EPI_STORE, nullptr, nullptr, 0, nullptr, s);
+    for (int a = 0; a < 3 && !r; ++a)
+      r = launch_deriv(in, 3 * nn, nn, out + a * nn, 3 * nn, 3 * nn, 1, nprob, d, a, EPI_STORE, nullptr, 0, nullptr,
+                       s);
+    return r;
+  };
+  for (int i = 0; i < ncand && !e; ++i) {
+    g_fft_var[size_slot(n)].store(cand[i], std::memory_order_relaxed);
+    for (int w = 0; w < 2 && !e; ++w) e = work();
+    constexpr int kReps = 5;
+    if (!e) e = (int)cudaEventRecord(t0, s);
+    for (int r = 0; r < kReps && !e; ++r) e = work();
+    if (!e) e = (int)cudaEventRecord(t1, s);
+    if (!e) e = (int)cudaEventSynchronize(t1);
+    float t = 0.f;
+    if (!e) e = (int)cudaEventElapsedTime(&t, t0, t1);
+    t /= kReps;
+    if (ms) ms[i] = t;
+    if (!e && (i == 0 || t < best_ms)) {
+      best_ms = t;
+      best_v = cand[i];
+    }
+  }
+  g_fft_var[size_slot(n)].store(e ? old : best_v, std::memory_order_relaxed);
+  if (!e) g_fft_tuned[size_slot(n)].store(true);
+  if (best) *best = e ? old : best_v;
+  cudaStreamSynchronize(s);
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  cudaFree(in);
+  cudaFree(out);
+  cudaFree(spec);
+  cudaFree(par);
   return e;
 }
 

@@ -123,16 +123,32 @@ template <int R, bool INV> struct Dft {
   }
 };
 
-// Two-stage plans N = R0 * R1.
-template <int N> struct Plan;
-template <> struct Plan<16> { static constexpr int R0 = 4, R1 = 4; };
-template <> struct Plan<32> { static constexpr int R0 = 4, R1 = 8; };
-template <> struct Plan<48> { static constexpr int R0 = 12, R1 = 4; };
-template <> struct Plan<64> { static constexpr int R0 = 8, R1 = 8; };
-template <> struct Plan<96> { static constexpr int R0 = 12, R1 = 8; };
-template <> struct Plan<128> { static constexpr int R0 = 16, R1 = 8; };
-template <> struct Plan<192> { static constexpr int R0 = 12, R1 = 16; };
-template <> struct Plan<256> { static constexpr int R0 = 16, R1 = 16; };
+// Two-stage plans N = R0 * R1.  Variant bit 0 selects the alternative
+// factorization (the other factor order, or 16 x 4 for 64); the autotuner
+// picks per grid size whichever runs faster (Plan0 where there is none).
+template <int N> struct Plan0;
+template <> struct Plan0<16> { static constexpr int R0 = 4, R1 = 4; };
+template <> struct Plan0<32> { static constexpr int R0 = 4, R1 = 8; };
+template <> struct Plan0<48> { static constexpr int R0 = 12, R1 = 4; };
+template <> struct Plan0<64> { static constexpr int R0 = 8, R1 = 8; };
+template <> struct Plan0<96> { static constexpr int R0 = 12, R1 = 8; };
+template <> struct Plan0<128> { static constexpr int R0 = 16, R1 = 8; };
+template <> struct Plan0<192> { static constexpr int R0 = 12, R1 = 16; };
+template <> struct Plan0<256> { static constexpr int R0 = 16, R1 = 16; };
+template <int N> struct Plan1;
+template <> struct Plan1<16> { static constexpr int R0 = 4, R1 = 4; };
+template <> struct Plan1<32> { static constexpr int R0 = 8, R1 = 4; };
+template <> struct Plan1<48> { static constexpr int R0 = 4, R1 = 12; };
+template <> struct Plan1<64> { static constexpr int R0 = 16, R1 = 4; };
+template <> struct Plan1<96> { static constexpr int R0 = 8, R1 = 12; };
+template <> struct Plan1<128> { static constexpr int R0 = 8, R1 = 16; };
+template <> struct Plan1<192> { static constexpr int R0 = 16, R1 = 12; };
+template <> struct Plan1<256> { static constexpr int R0 = 16, R1 = 16; };
+template <int N, int V = 0> struct Plan {
+  static constexpr int R0 = (V & 1) ? Plan1<N>::R0 : Plan0<N>::R0;
+  static constexpr int R1 = (V & 1) ? Plan1<N>::R1 : Plan0<N>::R1;
+  static_assert(R0 * R1 == N, "plan must factor N");
+};
 
 constexpr int kFftThreads = 256;  // threads per CTA of every FFT kernel
 
@@ -174,9 +190,9 @@ CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict_
 // Transform nlines lines held in (re, im); (sre, sim) is scratch of the same
 // size.  The result is back in (re, im).  Caller synchronises before; this
 // function synchronises after each stage.
-template <int N, bool INV, int NL, int PITCH>
+template <int N, bool INV, int NL, int PITCH, int V = 0>
 CB_DEVICE void fft_lines(float* re, float* im, float* sre, float* sim, const float2* tw) {
-  using P = Plan<N>;
+  using P = Plan<N, V>;
   fft_stage<N, P::R0, 1, INV, NL, PITCH>(re, im, sre, sim, tw);
   __syncthreads();
   fft_stage<N, P::R1, P::R0, INV, NL, PITCH>(sre, sim, re, im, tw);

@@ -121,8 +121,8 @@ int Solver::alloc(void** p, size_t bytes) {
 
 static int max_parts(const Dims& d) {
   int mp = dot_partials(3 * d.n());
-  for (int a = 0; a < 3; ++a) mp = std::max(mp, deriv_partials(d, a, 3));
-  mp = std::max(mp, c2r_partials(d, 3));
+  for (int a = 0; a < 3; ++a) mp = std::max(mp, deriv_partials(d, a, 3, true));
+  mp = std::max(mp, c2r_partials(d, 3, true));
   mp = std::max(mp, 3 * field_stats_parts(d.n()));
   return mp;
 }
@@ -176,6 +176,10 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     return CB_ERR_CUDA;
   }
   stream = own_stream;
+  if (o.autotune && !fft_tuned(d.n1) && fft_autotune_once(d.n1, B, stream)) {
+    err = "FFT autotuning failed";
+    return CB_ERR_CUDA;
+  }
   const size_t S = sizeof(float) * n * B, V = 3 * S;
   img16 = o.bf16_images != 0;
   if (img16) {

@@ -60,9 +60,26 @@ int launch_deriv(const float* in, long long ip, long long ifs, float* out, long 
                  long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
                  double* partials, int nparts, const int* active, cudaStream_t s);
 
-// Number of reduction partials a launch with these arguments writes per problem.
-int deriv_partials(const Dims& d, int axis, int nf);
-int c2r_partials(const Dims& d, int nf);
+// Number of reduction partials a launch with these arguments writes per problem
+// (any_variant: the largest count over the size's FFT variants, for sizing).
+int deriv_partials(const Dims& d, int axis, int nf, bool any_variant = false);
+int c2r_partials(const Dims& d, int nf, bool any_variant = false);
+
+// FFT variant of an N-point axis: bit 0 the alternative two-stage radix plan,
+// bit 1 the alternative lines per CTA.  Process-wide, default 0; change it
+// only while no transform of that size is in flight.
+int fft_variant(int n);
+int set_fft_variant(int n, int v);
+// candidate variants of size n into out[0..3]; returns their count (0: unsupported)
+int fft_variant_candidates(int n, int* out);
+// Time every candidate on a batch of nprob problems (a 3-field regularisation
+// operator and a 3-field gradient per problem) and keep the fastest.  ms[i]
+// receives the time of candidate i (ms may be null).  Allocates its own
+// buffers; synchronises the stream.
+int fft_autotune(int n, int nprob, cudaStream_t s, int* best, float* ms);
+// whether size n was tuned in this process; tune it once (serialised)
+bool fft_tuned(int n);
+int fft_autotune_once(int n, int nprob, cudaStream_t s);
 
 bool fft_size_supported(int n);
 

@@ -62,6 +62,8 @@ typedef struct claire_b200_opts {
   int bf16_images;      /* store transported images in bf16 (gathers accumulate in fp32) */
   double betacont;      /* -betacont beta*: regularisation-parameter continuation to beta* (0: off) */
   double presolvetol;   /* relative gradient tolerance of the continuation levels (1e-1) */
+  int autotune;         /* -autotune: measure the FFT variants of this grid size when the first
+                           context of that size is created (claire_b200_autotune) */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {
@@ -146,6 +148,20 @@ int claire_b200_interp3(const float* f, const float* disp, float* out, const int
  * 8-byte aligned when nx[2] % 4 == 0. */
 int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigned short* out, const int nx[3],
                              void* stream);
+/* FFT planning by measurement, the counterpart of the reference's
+ * accfft_plan_dft_3d_r2c(..., ACCFFT_MEASURE) (src/RegOpt.cpp:993-994): times
+ * every variant of the n-point transforms (two-stage radix plan x lines per
+ * CTA) on nbatch problems of the solver's spectral work (a 3-field
+ * regularisation operator and a 3-field gradient) and keeps the fastest for
+ * this process.  variant receives the choice; ms[i] the time of candidate i
+ * (4 entries, -1 where a size has fewer candidates; may be NULL).  Variants
+ * differ only in rounding (each within the FFT tolerance of the others).
+ * The choice is process-wide: tune, or set a variant, only while no
+ * transform of that size is in flight.  Allocates scratch; synchronises. */
+int claire_b200_autotune(int n, int nbatch, void* stream, int* variant, float* ms);
+/* Current FFT variant of size n (-1: unsupported), and a stored choice. */
+int claire_b200_fft_variant(int n);
+int claire_b200_set_fft_variant(int n, int variant);
 /* accfft_grad_t: g (3n) = spectral gradient of f (n), Nyquist zeroed. */
 int claire_b200_fft_grad(const float* f, float* g, const int nx[3], void* stream);
 /* accfft_divergence_t: d (n) = spectral divergence of v (3n). */
