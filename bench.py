@@ -278,8 +278,46 @@ def run_ours(a, rank, world, local):
 
     roof = roofline(cb, a, ci, load_device, B) if rank == 0 else None
     ci.close()
+    fixed = fixed_work(cb, a, probs, stream, zero_v) if rank == 0 else None
     return dict(total_ms=total_ms, lat=lat_all, lat_srv=lat_srv, stats=stats, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
-                launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned)
+                launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned, fixed=fixed)
+
+
+def fixed_work(cb, a, probs, stream, zero_v, matvecs=10):
+    """Time of one GN iteration with a fixed amount of work: PCG forced to
+    `matvecs` iterations (no forcing sequence, relative tolerance 1e-30), no
+    early stop; the difference of 2- and 1-iteration solves on the same
+    problems.  Unlike registrations/s on this workload it does not move with
+    the GN path, so kernel changes compare."""
+    import torch
+    out = {}
+    for B in (len(probs), 1):
+        ms, st = {}, {}
+        for maxit in (1, 2):
+            opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", a.norm, "-beta", repr(a.beta),
+                             "-krylovfseq", "none", "-krylovtol", "1e-30", "-krylovmaxit", str(matvecs + 1),
+                             "-opttol", "0", "-gabs", "0", "-maxit", str(maxit)])
+            ci = cb.CLAIREInterface(opt, nbatch=B)
+            ci.set_stream(stream)
+            for rep in range(2):  # warm-up, then timed
+                for b in range(B):
+                    ci.set_images(probs[b][0], probs[b][1], b)
+                    ci.SetInitialGuess(zero_v, b)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ci.Run()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms[maxit] = e0.elapsed_time(e1)
+            st[maxit] = ci.stats(0)
+            ci.close()
+        out["batch_%d" % B] = {
+            "gn_iteration_ms": ms[2] - ms[1],
+            "hess_matvecs_in_iteration": st[2]["hess_matvecs"] - st[1]["hess_matvecs"],
+            "obj_evals_in_iteration": st[2]["obj_evals"] - st[1]["obj_evals"]}
+    return out
 
 
 def tune(cb, sizes, nbatch):
@@ -758,7 +796,8 @@ def main():
                                               "obj_evals", "grad_evals")},
                    "hess_matvecs_per_s": float(sum(s["hess_matvecs"] for s in r["stats"]) * world * a.steps
                                                / (r["total_ms"] / 1e3)),
-                   "fft_variants": r["tuned"] or "defaults (--no-autotune)"},
+                   "fft_variants": r["tuned"] or "defaults (--no-autotune)",
+                   "fixed_work": r["fixed"]},
         "e2e": {"value": regs / (r["e2e_ms"] / 1e3), "unit": "registrations/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "path": "claire_b200_server_submit / _wait / _result (host buffers)"},

@@ -334,6 +334,106 @@ CB_DEVICE float gather_staged(unsigned sb, const BoxPoint& bp, const TileBox& bx
   return bx.P == 32 ? gather_box<32>(base, qb, bp.w1, bp.w2, bp.w3) : gather_box<64>(base, qb, bp.w1, bp.w2, bp.w3);
 }
 
+// ---- two points per instruction: packed FP32 pairs (fma.rn.f32x2) ------------
+// The thread's points a and a+1 are gathered together: their weights and
+// partial sums live in 64-bit register pairs and every multiply-add of the
+// tensor product is one f32x2 instruction for both points (each lane an
+// ordinary round-to-nearest FP32 FMA, in the scalar code's order).
+typedef unsigned long long f32x2;
+
+CB_DEVICE f32x2 pk2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+CB_DEVICE float2 upk2(f32x2 r) {
+  float2 o;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+  return o;
+}
+CB_DEVICE f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+CB_DEVICE f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+CB_DEVICE f32x2 dup2(float c) { return pk2(c, c); }
+
+// lagrange4 of two fractions at once (same Horner steps)
+CB_DEVICE void lagrange4x2(f32x2 s, f32x2 (&w)[4]) {
+  w[0] = mul2(s, fma2(s, fma2(s, dup2(-1.f / 6.f), dup2(0.5f)), dup2(-1.f / 3.f)));
+  w[1] = fma2(s, fma2(s, fma2(s, dup2(0.5f), dup2(-1.f)), dup2(-0.5f)), dup2(1.f));
+  w[2] = mul2(s, fma2(s, fma2(s, dup2(-0.5f), dup2(0.5f)), dup2(1.f)));
+  w[3] = mul2(s, fma2(mul2(s, s), dup2(1.f / 6.f), dup2(-1.f / 6.f)));
+}
+
+// Four consecutive floats at OFF from each of two addresses, weighted.
+template <int OFF>
+CB_DEVICE f32x2 row4x2(unsigned pa, unsigned pb, const f32x2 (&w)[4]) {
+  float a0, a1, a2, a3, b0, b1, b2, b3;
+  asm volatile(
+      "ld.shared.f32 %0, [%8+%10];\n\t"
+      "ld.shared.f32 %1, [%8+%11];\n\t"
+      "ld.shared.f32 %2, [%8+%12];\n\t"
+      "ld.shared.f32 %3, [%8+%13];\n\t"
+      "ld.shared.f32 %4, [%9+%10];\n\t"
+      "ld.shared.f32 %5, [%9+%11];\n\t"
+      "ld.shared.f32 %6, [%9+%12];\n\t"
+      "ld.shared.f32 %7, [%9+%13];\n"
+      : "=f"(a0), "=f"(a1), "=f"(a2), "=f"(a3), "=f"(b0), "=f"(b1), "=f"(b2), "=f"(b3)
+      : "r"(pa), "r"(pb), "n"(OFF), "n"(OFF + 4), "n"(OFF + 8), "n"(OFF + 12));
+  f32x2 r = mul2(w[0], pk2(a0, b0));
+  r = fma2(w[1], pk2(a1, b1), r);
+  r = fma2(w[2], pk2(a2, b2), r);
+  return fma2(w[3], pk2(a3, b3), r);
+}
+
+template <int P>
+CB_DEVICE f32x2 gather_box_x2(unsigned ba, unsigned bb, unsigned qb, const f32x2 (&w1)[4], const f32x2 (&w2)[4],
+                              const f32x2 (&w3)[4]) {
+  f32x2 acc = 0ull;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const unsigned pa = ba + a * qb, pb = bb + a * qb;
+    f32x2 t = mul2(w2[0], row4x2<0>(pa, pb, w3));
+    t = fma2(w2[1], row4x2<P * 4>(pa, pb, w3), t);
+    t = fma2(w2[2], row4x2<P * 8>(pa, pb, w3), t);
+    t = fma2(w2[3], row4x2<P * 12>(pa, pb, w3), t);
+    acc = (a == 0) ? mul2(w1[0], t) : fma2(w1[a], t, acc);
+  }
+  return acc;
+}
+
+// Staged gather of the thread's points a and a+1: values (x, y).
+CB_DEVICE float2 gather_staged_pair(unsigned sb, const float (&da)[3], const float (&db)[3], int a,
+                                    const TileThread& tt, const TileBox& bx) {
+  float fa[3], fb[3];
+  int oa[3], ob[3];
+  const int xa[3] = {tt.x1(a), tt.i2, tt.i3}, xb[3] = {tt.x1(a + 1), tt.i2, tt.i3};
+  const bool okA = tt.valid_idx(a), okB = tt.valid_idx(a + 1);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float la = floorf(da[k]), lb = floorf(db[k]);
+    fa[k] = da[k] - la;
+    fb[k] = db[k] - lb;
+    oa[k] = okA ? xa[k] + (int)la - 1 - bx.lo[k] : 0;
+    ob[k] = okB ? xb[k] + (int)lb - 1 - bx.lo[k] : 0;
+  }
+  f32x2 w1[4], w2[4], w3[4];
+  lagrange4x2(pk2(fa[0], fb[0]), w1);
+  lagrange4x2(pk2(fa[1], fb[1]), w2);
+  lagrange4x2(pk2(fa[2], fb[2]), w3);
+  const unsigned ba = sb + 4u * (unsigned)(oa[0] * bx.Q + oa[1] * bx.P + oa[2]);
+  const unsigned bb = sb + 4u * (unsigned)(ob[0] * bx.Q + ob[1] * bx.P + ob[2]);
+  const unsigned qb = (unsigned)bx.Q * 4u;
+  const f32x2 r = bx.P == 32 ? gather_box_x2<32>(ba, bb, qb, w1, w2, w3) : gather_box_x2<64>(ba, bb, qb, w1, w2, w3);
+  return upk2(r);
+}
+
 // Tile gather of one field at the displacements Src loads; epi(tt, a, value)
 // consumes the value at the thread's point a.  sb holds kGatherBudget floats
 // (16-byte aligned).  Tiles whose box does not fit gather from global memory.
@@ -399,9 +499,10 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
     __syncthreads();
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
 #pragma unroll
-    for (int a = 0; a < kTilePts; ++a) {
-      const BoxPoint bp = box_point(dd[a], tt.x1(a), tt, tt.valid_idx(a), bx);
-      epi(tt, a, gather_staged(sbase, bp, bx), aux[a]);
+    for (int a = 0; a < kTilePts; a += 2) {
+      const float2 r = gather_staged_pair(sbase, dd[a], dd[a + 1], a, tt, bx);
+      epi(tt, a, r.x, aux[a]);
+      epi(tt, a + 1, r.y, aux[a + 1]);
     }
   } else {
 #pragma unroll
