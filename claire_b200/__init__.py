@@ -57,7 +57,7 @@ class Opts(ctypes.Structure):
         ("gatol", ctypes.c_double), ("krylovmaxit", ctypes.c_int), ("krylovtol", ctypes.c_double * 3),
         ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int), ("betacont", ctypes.c_double),
-        ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int),
+        ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int), ("distance", ctypes.c_int),
     ]
 
 

@@ -63,6 +63,7 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->verbosity = 0;
   o->bf16_images = 0;
   o->autotune = 0;
+  o->distance = CB_DIST_SL2;  // src/RegOpt.cpp:1079
   return CB_OK;
 }
 
@@ -139,6 +140,12 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (next(&val)) return CB_ERR_ARG;
       o->iporder = std::atoi(val);
       if (o->iporder != 3) return CB_ERR_UNSUPPORTED;
+    } else if (!std::strcmp(a, "-distance")) {
+      // src/RegOpt.cpp:680-690
+      if (next(&val)) return CB_ERR_ARG;
+      if (!std::strcmp(val, "sl2")) o->distance = CB_DIST_SL2;
+      else if (!std::strcmp(val, "ncc")) o->distance = CB_DIST_NCC;
+      else return CB_ERR_ARG;
     } else if (!std::strcmp(a, "-autotune")) {
       o->autotune = 1;
     } else if (!std::strcmp(a, "-bf16images")) {
@@ -226,7 +233,7 @@ int claire_b200_set_images(claire_b200_ctx* c, int b, const float* mR, const flo
   }
   int e = copy_in(s, s.mR + b * s.n, mR, s.n, on_device);
   if (!e) e = copy_in(s, s.mT + b * s.n, mT, s.n, on_device);
-  s.state_of[b] = 0;
+  s.images_changed(b);
   return e;
 }
 

@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(kRedThreads) k_diff_sumsq(const float* __restr
 }
 
 __global__ void k_finalize(const double* __restrict__ partials, int stride, int nparts,
-                           double* __restrict__ out, double scale, int accumulate) {
+                           double* __restrict__ out, double scale, int accumulate, const int* __restrict__ active) {
+  if (active && !active[blockIdx.x]) return;  // other problems' results stay as they are
   const double* p = partials + (long long)blockIdx.x * stride;
   double acc = 0.0;
   // fixed-order: thread t sums entries t, t+32, ...; then a fixed shuffle tree
@@ -119,8 +120,8 @@ __global__ void k_finalize(const double* __restrict__ partials, int stride, int 
 }
 
 int launch_finalize(const double* partials, int stride, int count, double* out, int nprob, double scale,
-                    bool accumulate, cudaStream_t s) {
-  k_finalize<<<nprob, 32, 0, s>>>(partials, stride, count, out, scale, accumulate ? 1 : 0);
+                    bool accumulate, cudaStream_t s, const int* active) {
+  k_finalize<<<nprob, 32, 0, s>>>(partials, stride, count, out, scale, accumulate ? 1 : 0, active);
   return (int)cudaGetLastError();
 }
 

@@ -36,9 +36,10 @@ CB_DEVICE void block_reduce_store(double v, double* dst, int idx) {
 }
 
 // Host launchers.  Problem p's partials start at partials + p*stride.
-// out[p] = scale * sum(partials[p][0..count)) (+ out[p] when accumulate).
+// out[p] = scale * sum(partials[p][0..count)) (+ out[p] when accumulate), for the
+// problems whose active entry is nonzero (all when active is null).
 int launch_finalize(const double* partials, int stride, int count, double* out, int nprob, double scale,
-                    bool accumulate, cudaStream_t s);
+                    bool accumulate, cudaStream_t s, const int* active = nullptr);
 
 // Partials written by the dot / norm kernels for vectors of length len.
 int dot_partials(long long len);

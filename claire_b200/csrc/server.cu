@@ -52,7 +52,7 @@ static bool same_pool(const claire_b200_opts& a, const claire_b200_opts& b) {
          a.maxit == b.maxit && a.opttol == b.opttol && a.gatol == b.gatol && a.krylovmaxit == b.krylovmaxit &&
          a.krylovtol[0] == b.krylovtol[0] && a.krylovtol[1] == b.krylovtol[1] &&
          a.krylovtol[2] == b.krylovtol[2] && a.krylovfseq == b.krylovfseq && a.precond == b.precond &&
-         a.iporder == b.iporder && a.bf16_images == b.bf16_images;
+         a.iporder == b.iporder && a.bf16_images == b.bf16_images && a.distance == b.distance;
 }
 
 struct Pool;
@@ -190,7 +190,7 @@ static int load_slot(Solver& sv, int b, const Request& r) {
              cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess) {
     return CB_ERR_CUDA;
   }
-  sv.state_of[b] = 0;
+  sv.images_changed(b);
   return sv.set_problem(b, r.opts);  // per-slot norm and weights (synchronises the stream)
 }
 

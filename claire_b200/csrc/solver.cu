@@ -50,6 +50,37 @@ __global__ void k_pcg_init(double* __restrict__ sc, int* __restrict__ isc, int* 
   }
 }
 
+// NCC distance scalars (src/DistanceMeasureNCC.cpp), FP64, one thread per problem.
+// which 0: scale = (1/2 hd |mT - mR|^2) / (1/2 - 1/2 I^2/(A R))     (:78-166)
+// which 1: D = scale (1/2 - 1/2 I^2/(A R))                         (:171-245)
+// which 2: lambda(1) = CA mR + CB m1, CA = s I/(hd A R), CB = -s I^2/(hd A^2 R)   (:251-366)
+// which 3: lambda~(1) = CA mR + CB m1 + CC m~ with the linearised coefficients    (:368-510)
+// A = <x,x> (x = mT for the scale, else m1), R = <mR,mR>, I = <x,mR>.
+__global__ void k_ncc(double* __restrict__ sc, const int* __restrict__ act, int B, int which, double hd) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B || (act && !act[p])) return;
+  const double A = sc[Solver::S_NA * B + p], R = sc[Solver::S_NRR * B + p], I = sc[Solver::S_NI * B + p];
+  const double s = sc[Solver::S_NS * B + p];
+  if (which == 0) {
+    sc[Solver::S_NS * B + p] = (0.5 * hd * sc[Solver::S_NL2 * B + p]) / (0.5 - 0.5 * I * I / (A * R));
+  } else if (which == 1) {
+    sc[Solver::S_D * B + p] = s * (0.5 - 0.5 * I * I / (A * R));
+  } else if (which == 2) {
+    sc[Solver::S_CA * B + p] = s * I / (hd * A * R);
+    sc[Solver::S_CB * B + p] = -s * I * I / (hd * A * A * R);
+  } else {
+    const double IM = sc[Solver::S_NIM * B + p], RM = sc[Solver::S_NRM * B + p];
+    const double c1 = s * RM / (hd * A * R);
+    const double c2 = 2.0 * s * I * IM / (hd * A * A * R);
+    const double c3 = 4.0 * s * I * I * IM / (hd * A * A * A * R);
+    const double c4 = 2.0 * s * I * RM / (hd * A * A * R);
+    const double c5 = s * I * I / (hd * A * A * R);
+    sc[Solver::S_CA * B + p] = c1 - c2;
+    sc[Solver::S_CB * B + p] = c3 - c4;
+    sc[Solver::S_CC * B + p] = -c5;
+  }
+}
+
 // alpha = rz / pq, stop on non-positive curvature
 __global__ void k_pcg_alpha(double* __restrict__ sc, int* __restrict__ isc, int* __restrict__ act, int B) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -182,6 +213,11 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   }
   const size_t S = sizeof(float) * n * B, V = 3 * S;
   img16 = o.bf16_images != 0;
+  ncc = o.distance == CB_DIST_NCC;
+  if (ncc && img16) {
+    err = "the NCC distance needs FP32 images";
+    return CB_ERR_UNSUPPORTED;
+  }
   if (img16) {
     const size_t S16 = sizeof(bf16) * n * B;
     CB_TRY(alloc((void**)&mR16, S16));
@@ -248,6 +284,7 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     ps[b].beta2 = o.beta[2];
   }
   state_of.assign(B, 0);
+  ncc_scale_ok.assign(B, 0);
   CB_TRY(upload_params());
   if (cudaStreamSynchronize(stream) != cudaSuccess) {
     err = "initialisation failed";
@@ -305,7 +342,7 @@ int Solver::dot(const float* a, long long ap, const float* b, long long bp, long
                 const int* act, double scale) {
   const int np = dot_partials(len);
   CB_TRY(launch_dot(a, ap, b, bp, len, B, partials, maxparts, act, stream));
-  CB_TRY(launch_finalize(partials, maxparts, np, slot(s), B, scale, false, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(s), B, scale, false, stream, act));
   note_launches(2);
   return 0;
 }
@@ -467,12 +504,76 @@ void Solver::prof_clear() {
   prof_pool.clear();
 }
 
-// D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)
-int Solver::distance(const int* act) {
+// D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155), or the NCC
+// distance (src/DistanceMeasureNCC.cpp:171-245)
+int Solver::distance(const std::vector<int>& sel, const int* act) {
   const int np = dot_partials(n);
+  if (ncc) {
+    const long long PM = (nt + 1) * n;
+    CB_TRY(ncc_setup_scale(sel));
+    const float* m1 = m + nt * n;
+    CB_TRY(dot(m1, PM, m1, PM, n, S_NA, act));
+    CB_TRY(dot(mR, n, mR, n, n, S_NRR, act));
+    CB_TRY(dot(m1, PM, mR, n, n, S_NI, act));
+    k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 1, (double)hd);
+    note_launches(1);
+    return (int)cudaGetLastError();
+  }
   CB_TRY(image_diff_sumsq(false, act));
-  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_D), B, 0.5 * (double)hd, false, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_D), B, 0.5 * (double)hd, false, stream, act));
   note_launches(1);
+  return 0;
+}
+
+// DistanceMeasureNCC::SetupScale for the selected problems whose images
+// changed since their scale was set (src/CLAIREBase.cpp:686-689 calls it once
+// the images are known).
+int Solver::ncc_setup_scale(const std::vector<int>& sel) {
+  std::vector<int> need(B, 0);
+  bool any = false;
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && !ncc_scale_ok[b]) { need[b] = 1; any = true; }
+  if (!any) return 0;
+  int* m3 = dact + 2 * B;
+  CB_TRY(upload_mask(need, m3));
+  CB_TRY(dot(mT, n, mT, n, n, S_NA, m3));
+  CB_TRY(dot(mR, n, mR, n, n, S_NRR, m3));
+  CB_TRY(dot(mT, n, mR, n, n, S_NI, m3));
+  CB_TRY(launch_diff_sumsq(mT, n, mR, n, n, B, partials, maxparts, m3, stream));
+  CB_TRY(launch_finalize(partials, maxparts, dot_partials(n), slot(S_NL2), B, 1.0, false, stream, m3));
+  k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, m3, B, 0, (double)hd);
+  note_launches(3);
+  CB_TRY((int)cudaGetLastError());
+  for (int b = 0; b < B; ++b)
+    if (need[b]) ncc_scale_ok[b] = 1;
+  return 0;
+}
+
+int Solver::ncc_final_condition(float* lam, long long lp, const int* act) {
+  const long long PM = (nt + 1) * n;
+  const float* m1 = m + nt * n;
+  CB_TRY(dot(m1, PM, m1, PM, n, S_NA, act));
+  CB_TRY(dot(mR, n, mR, n, n, S_NRR, act));
+  CB_TRY(dot(m1, PM, mR, n, n, S_NI, act));
+  k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 2, (double)hd);
+  CB_TRY((int)cudaGetLastError());
+  CB_TRY(launch_lincomb(lam, lp, mR, n, slot(S_CA), 1.0, m1, PM, slot(S_CB), 1.0, n, B, act, stream));
+  note_launches(2);
+  return 0;
+}
+
+// lam holds m~(1) on entry and lambda~(1) on exit; the sums of m1 and mR are
+// those of the last gradient (the GN iterate).
+int Solver::ncc_inc_final_condition(float* lam, long long lp, const int* act) {
+  const long long PM = (nt + 1) * n;
+  const float* m1 = m + nt * n;
+  CB_TRY(dot(m1, PM, lam, lp, n, S_NIM, act));
+  CB_TRY(dot(mR, n, lam, lp, n, S_NRM, act));
+  k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 3, (double)hd);
+  CB_TRY((int)cudaGetLastError());
+  CB_TRY(launch_lincomb(lam, lp, lam, lp, slot(S_CC), 1.0, mR, n, slot(S_CA), 1.0, n, B, act, stream));
+  CB_TRY(launch_lincomb(lam, lp, lam, lp, nullptr, 1.0, m1, PM, slot(S_CB), 1.0, n, B, act, stream));
+  note_launches(3);
   return 0;
 }
 
@@ -494,7 +595,7 @@ int Solver::reg_functional(const float* vel, const std::vector<int>& sel, const 
     for (int a = 0; a < 3; ++a) {
       const int np = deriv_partials(d, a, 3);
       CB_TRY(launch_deriv(vel, 3 * n, n, nullptr, 0, 0, 3, B, d, a, EPI_SUMSQ, partials, maxparts, dma, stream));
-      CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, a > 0, stream));
+      CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, a > 0, stream, dma));
     }
     note_launches(6);
     CB_TRY(dot(vel, 3 * n, vel, 3 * n, 3 * n, S_RV, dma));
@@ -506,7 +607,7 @@ int Solver::reg_functional(const float* vel, const std::vector<int>& sel, const 
     const int np = c2r_partials(d, 3);
     CB_TRY(launch_c2r3d(spec, 3 * nc, nullptr, 0, 0, 3, B, d, EPI_SUMSQ, nullptr, partials, maxparts, dmb, stream));
     // finalize only the selected problems' slots: unselected keep stale values
-    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, false, stream));
+    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_R), B, 1.0, false, stream, dmb));
     note_launches(6);
     (void)any_a;
   }
@@ -524,7 +625,7 @@ int Solver::div_penalty(const float* vel, const int* act) {
   for (int a = 0; a < 3; ++a) {
     const int np = deriv_partials(d, a, 1);
     CB_TRY(launch_deriv(dv, n, n, nullptr, 0, 0, 1, B, d, a, EPI_SUMSQ, partials, maxparts, act, stream));
-    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RW), B, 1.0, true, stream));
+    CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RW), B, 1.0, true, stream, act));
   }
   note_launches(6);
   return 0;
@@ -546,7 +647,7 @@ static double reg_factor(const ProbState& s, double hd, double sumsq, double vv)
 int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
   CB_TRY(upload_mask(sel, dact));
   CB_TRY(state_solve(vel, dact));
-  CB_TRY(distance(dact));
+  CB_TRY(distance(sel, dact));
   // mixed-class batches run reg_functional's two passes with their own masks;
   // the finalize of the second pass must not clobber the first, so run classes
   // one after another and read back in between.
@@ -597,7 +698,7 @@ int Solver::reg_op(const float* vin, float* out, int op, int epi, const int* act
     const int e2 = (epi == EPI_ADD) ? EPI_ADD_DOT : EPI_STORE_DOT;
     CB_TRY(launch_c2r3d(spec, 3 * nc, out, 3 * n, n, 3, B, d, e2, nullptr, partials, maxparts, act, stream,
                         dot_with));
-    CB_TRY(launch_finalize(partials, maxparts, c2r_partials(d, 3), slot(dot_slot), B, 1.0, false, stream));
+    CB_TRY(launch_finalize(partials, maxparts, c2r_partials(d, 3), slot(dot_slot), B, 1.0, false, stream, act));
     note_launches(6);
     return 0;
   }
@@ -683,8 +784,9 @@ int Solver::gradient(const int* act) {
   CB_TRY(image_grad(act));
   CB_TRY(divergence(v, divv, act));
   CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, tab_adj, TP, cadj, n, ht, B, d, act, stream));
-  // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222)
-  CB_TRY(image_residual(lamh + nt * n, PL, act));
+  // lambda(t=1) = mR - m1 (src/DistanceMeasureSL2.cpp:156-222), or NCC's
+  if (ncc) CB_TRY(ncc_final_condition(lamh + nt * n, PL, act));
+  else CB_TRY(image_residual(lamh + nt * n, PL, act));
   note_launches(2);
   CB_TRY(finish_with_reg(v, g, act));
   CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, act));
@@ -708,8 +810,10 @@ int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) 
   CB_TRY(launch_incstate_source(gx, PGX, vtx, 3 * n, gm, PGM, vin, 3 * n, sj, PS, nt, ht, B, n, act, stream));
   note_launches(2);
   float* lam_end = lamh + nt * n;
+  // SL2: lambda~(1) = -m~(1), written by the last step; NCC: m~(1) there first
+  const float fin = ncc ? 1.f : -1.f;
   if (nt == 1) {
-    CB_TRY(launch_lincomb(lam_end, PL, sj, PS, nullptr, -1.0, nullptr, 0, nullptr, 0.0, n, B, act, stream));
+    CB_TRY(launch_lincomb(lam_end, PL, sj, PS, nullptr, fin, nullptr, 0, nullptr, 0.0, n, B, act, stream));
     note_launches(1);
   }
   const float* cur = sj;  // m~^1 = s_0
@@ -720,12 +824,13 @@ int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) 
     float* out = last ? lam_end : bufs[j & 1];
     CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
     CB_TRY(launch_gather_add(cur, cp, disp_st, 3 * n, tab_st, TP, sj + j * n, PS, out, last ? PL : n,
-                             last ? -1.f : 1.f, B, d, act, stream));
+                             last ? fin : 1.f, B, d, act, stream));
     CB_TRY(prof_mark(CB_PROF_INCSTATE_STEP));
     cur = out;
     cp = n;
   }
   note_launches(nt - 1);
+  if (ncc) CB_TRY(ncc_inc_final_condition(lam_end, PL, act));
   CB_TRY(finish_with_reg(vin, hout, act, pq_slot >= 0 ? vin : nullptr, pq_slot));
   return 0;
 }
@@ -785,6 +890,7 @@ int Solver::det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<
 // public single-shot operations
 // ---------------------------------------------------------------------------
 int Solver::gradient_at_current(const std::vector<int>& sel) {
+  if (ncc) CB_TRY(ncc_setup_scale(sel));
   std::vector<int> need(B, 0);
   bool any = false;
   for (int b = 0; b < B; ++b)
@@ -885,7 +991,7 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
     k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
     // x += alpha p, r -= alpha q and the new r.r in one pass
     CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
-    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream));
+    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream, act));
     k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
     note_launches(4);
     CB_TRY(apply_pc(S_RZNEW));
@@ -1137,9 +1243,9 @@ int Solver::finish(const std::vector<int>& sel) {
   CB_TRY(upload_mask(sel, dact));
   const int np = dot_partials(n);
   CB_TRY(image_diff_sumsq(false, dact));
-  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_PQ), B, 1.0, false, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_PQ), B, 1.0, false, stream, dact));
   CB_TRY(image_diff_sumsq(true, dact));
-  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream));
+  CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream, dact));
   note_launches(2);
   CB_TRY(fetch_scalars());
   const auto t1 = std::chrono::steady_clock::now();

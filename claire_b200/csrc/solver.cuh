@@ -96,11 +96,21 @@ class Solver {
   int* hint = nullptr;     // pinned host mirror of dint
 
   enum Slot { S_D = 0, S_R, S_RV, S_GG, S_PQ, S_RR, S_RZ, S_RZNEW, S_ALPHA, S_BETA, S_TOL,
-              S_RN0, S_GD, S_RTOL, S_RW, NSLOT };
+              S_RN0, S_GD, S_RTOL, S_RW,
+              // NCC: sums <x,x> of m1 (or mT), <mR,mR>, <x,mR>, |mT - mR|^2, the
+              // scale, <m1,m~>, <mR,m~>, and final-condition coefficients
+              S_NA, S_NRR, S_NI, S_NL2, S_NS, S_NIM, S_NRM, S_CA, S_CB, S_CC, NSLOT };
   enum ISlot { I_IT = 0, I_REASON, NISLOT };
 
   // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
   std::vector<int> state_of;
+  // NCC distance (opts.distance == CB_DIST_NCC): scale set up per image pair
+  bool ncc = false;
+  std::vector<char> ncc_scale_ok;
+  void images_changed(int b) {
+    state_of[b] = 0;
+    if (b >= 0 && b < (int)ncc_scale_ok.size()) ncc_scale_ok[b] = 0;
+  }
 
   // PCG iteration recorded as a CUDA graph (built on the second iteration the
   // solver runs; graphs = false switches replay off)
@@ -139,7 +149,10 @@ class Solver {
   int image_residual(float* y, long long yp, const int* act);  // y = mR - m^nt
   int image_grad(const int* act);                              // gm = grad m^j, j <= nt
   int state_solve(const float* vel, const int* act);
-  int distance(const int* act);
+  int distance(const std::vector<int>& sel, const int* act);
+  int ncc_setup_scale(const std::vector<int>& sel);   // DistanceMeasureNCC::SetupScale where needed
+  int ncc_final_condition(float* lam, long long lp, const int* act);       // lambda(1)
+  int ncc_inc_final_condition(float* lam, long long lp, const int* act);   // lambda~(1) from m~(1) in lam
   int reg_functional(const float* vel, const std::vector<int>& sel, const int* act);
   int reg_op(const float* vin, float* out, int op, int epi, const int* act, const float* dot_with = nullptr,
              int dot_slot = -1);

@@ -35,6 +35,9 @@ enum {
 };
 /* Registration models: CLAIRE (no projection), Stokes, relaxed Stokes. */
 enum { CB_MODEL_COMPRESSIBLE = 0, CB_MODEL_STOKES = 1, CB_MODEL_RELAXEDSTOKES = 2 };
+/* Distance measures (-distance): squared L2 (DistanceMeasureSL2) or
+ * normalised cross-correlation (DistanceMeasureNCC). */
+enum { CB_DIST_SL2 = 0, CB_DIST_NCC = 1 };
 /* Krylov forcing sequences (-krylovfseq). */
 enum { CB_FSEQ_NONE = 0, CB_FSEQ_QUADRATIC = 1, CB_FSEQ_SUPERLINEAR = 2 };
 /* Regularisation operator kinds for claire_b200_reg_apply. */
@@ -64,6 +67,7 @@ typedef struct claire_b200_opts {
   double presolvetol;   /* relative gradient tolerance of the continuation levels (1e-1) */
   int autotune;         /* -autotune: measure the FFT variants of this grid size when the first
                            context of that size is created (claire_b200_autotune) */
+  int distance;         /* -distance sl2|ncc (CB_DIST_SL2); NCC needs FP32 images */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {

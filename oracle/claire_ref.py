@@ -432,7 +432,7 @@ class Problem:
     """
 
     def __init__(self, mR, mT, nt: int, reg: Regularization, dtype=np.float64,
-                 projection: Optional[str] = None, image_store=None):
+                 projection: Optional[str] = None, image_store=None, distance: str = "sl2"):
         # image_store: rounding applied to every stored image value (mR, mT
         # and each state level), e.g. bf16_round; None keeps dtype values
         self.dtype = dtype
@@ -443,9 +443,13 @@ class Problem:
         self.mR = np.asarray(mR, dtype=dtype)
         self.mT = np.asarray(mT, dtype=dtype)
         self.shape = self.mR.shape
+        self.distance_type = distance
+        if distance not in ("sl2", "ncc"):
+            raise ValueError(distance)
         self.nt = nt
         self.ht = 1.0 / nt
         self.hd = lebesgue_measure(self.shape)
+        self.ncc_scale = self._ncc_setup_scale() if distance == "ncc" else None
         self.reg = reg
         self.projection = projection
         self.beta_w = 1e-4  # -beta-div (src/RegOpt.cpp:729-731, default 1e-4)
@@ -503,10 +507,65 @@ class Problem:
             self._divv = (dv, dvx)
         return self._divv
 
+    # --- NCC distance (src/DistanceMeasureNCC.cpp, no mask, one component) -
+    def _ncc_setup_scale(self) -> float:
+        """DistanceMeasureNCC::SetupScale (src/DistanceMeasureNCC.cpp:78-166):
+        scale = (1/2 hd sum (mT - mR)^2) / (1/2 - 1/2 <mT,mR>^2 / (|mT|^2 |mR|^2))."""
+        mT = self.mT.astype(np.float64).ravel()
+        mR = self.mR.astype(np.float64).ravel()
+        l2 = 0.5 * self.hd * float(np.sum((mT - mR) ** 2))
+        ncc = 0.5 - 0.5 * float(np.dot(mT, mR)) ** 2 / (float(np.dot(mT, mT)) * float(np.dot(mR, mR)))
+        return l2 / ncc
+
+    def _ncc_sums(self):
+        m1 = self.solve_state()[self.nt].astype(np.float64).ravel()
+        mR = self.mR.astype(np.float64).ravel()
+        return m1, mR, float(np.dot(m1, m1)), float(np.dot(mR, mR)), float(np.dot(m1, mR))
+
+    def final_condition(self) -> np.ndarray:
+        """Adjoint final condition lambda(1): mR - m1 for SL2
+        (src/DistanceMeasureSL2.cpp:156-222); for NCC
+        c1 mR - c2 m1, c1 = s I / (hd A R), c2 = s I^2 / (hd A^2 R), with
+        A = <m1,m1>, R = <mR,mR>, I = <m1,mR> (src/DistanceMeasureNCC.cpp:251-366)."""
+        m = self.solve_state()
+        if self.distance_type == "sl2":
+            return (self.mR - m[self.nt]).astype(self.dtype)
+        m1, mR, A, Rr, I = self._ncc_sums()
+        s, hd = self.ncc_scale, self.hd
+        c1 = s * I / (hd * A * Rr)
+        c2 = s * I * I / (hd * A * A * Rr)
+        return (c1 * mR - c2 * m1).reshape(self.shape).astype(self.dtype)
+
+    def inc_final_condition(self, mt1) -> np.ndarray:
+        """Incremental adjoint final condition: -m~(1) for SL2
+        (src/DistanceMeasureSL2.cpp:223-283); for NCC the linearisation of the
+        adjoint final condition (src/DistanceMeasureNCC.cpp:368-510):
+        (c1 - c2) mR + (c3 - c4) m1 - c5 m~ with c1 = s<mR,m~>/(hd A R),
+        c2 = 2 s I <m1,m~>/(hd A^2 R), c3 = 4 s I^2 <m1,m~>/(hd A^3 R),
+        c4 = 2 s I <mR,m~>/(hd A^2 R), c5 = s I^2/(hd A^2 R)."""
+        if self.distance_type == "sl2":
+            return (-mt1).astype(self.dtype)
+        m1, mR, A, Rr, I = self._ncc_sums()
+        mt = np.asarray(mt1, np.float64).ravel()
+        IM, RM = float(np.dot(m1, mt)), float(np.dot(mR, mt))
+        s, hd = self.ncc_scale, self.hd
+        c1 = s * RM / (hd * A * Rr)
+        c2 = 2.0 * s * I * IM / (hd * A * A * Rr)
+        c3 = 4.0 * s * I * I * IM / (hd * A ** 3 * Rr)
+        c4 = 2.0 * s * I * RM / (hd * A * A * Rr)
+        c5 = s * I * I / (hd * A * A * Rr)
+        out = (c1 - c2) * mR + (c3 - c4) * m1 - c5 * mt
+        return out.reshape(self.shape).astype(self.dtype)
+
     # --- objective (src/CLAIRE.cpp:793-863) --------------------------------
     def distance(self) -> float:
-        """D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155)."""
+        """D = 1/2 hd sum (mR - m1)^2 (src/DistanceMeasureSL2.cpp:93-155), or
+        D = s (1/2 - 1/2 <m1,mR>^2 / (|m1|^2 |mR|^2)) for NCC
+        (src/DistanceMeasureNCC.cpp:171-245)."""
         m = self.solve_state()
+        if self.distance_type == "ncc":
+            _, _, A, Rr, I = self._ncc_sums()
+            return self.ncc_scale * (0.5 - 0.5 * I * I / (A * Rr))
         dr = self.mR.astype(np.float64) - m[self.nt].astype(np.float64)
         return 0.5 * self.hd * float(np.sum(dr * dr))
 
@@ -563,8 +622,7 @@ class Problem:
         return leray_projection(b, self.projection, self.reg.beta0)
 
     def body_force(self):
-        m = self.solve_state()
-        lam1 = (self.mR - m[self.nt]).astype(self.dtype)
+        lam1 = self.final_condition()
         b, lam0 = self._backward_sl(lam1)
         b = self._project(b)
         self.lambda0 = lam0
@@ -594,7 +652,7 @@ class Problem:
         return mt
 
     def inc_body_force(self, mt1) -> np.ndarray:
-        bt, _ = self._backward_sl((-mt1).astype(self.dtype))
+        bt, _ = self._backward_sl(self.inc_final_condition(mt1))
         bt = self._project(bt)
         return (self.hd * bt).astype(self.dtype)
 

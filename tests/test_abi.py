@@ -59,6 +59,7 @@ def test_parse_args():
     assert o.bf16_images == 0
     assert cb.RegOpt(["-nx", "64", "-bf16images"]).opts.bf16_images == 1
     assert o.autotune == 0 and cb.RegOpt(["-nx", "64", "-autotune"]).opts.autotune == 1
+    assert o.distance == 0 and cb.RegOpt(["-nx", "64", "-distance", "ncc"]).opts.distance == 1
     opt2 = cb.RegOpt(["-nx", "96", "-regnorm", "h1s-stokes"])
     assert tuple(opt2.opts.nx) == (96, 96, 96) and opt2.opts.model == cb.MODELS["stokes"]
 

@@ -220,3 +220,58 @@ def test_bf16_round_known_answers():
     assert abs(got[6] / 3.0e38 - 1) < 2 ** -8
     y = np.random.default_rng(0).standard_normal(1000)
     assert np.max(np.abs(R.bf16_round(y) / y - 1)) <= 2 ** -8
+
+
+def test_ncc_scale_matches_sl2_at_zero_velocity():
+    # src/DistanceMeasureNCC.cpp:78-166: the scale makes D_ncc(m1 = mT) = D_sl2(m1 = mT)
+    n, nt = 16, 4
+    mR, mT, _ = R.synthetic_c1(n, np.float64, nt)
+    reg = R.Regularization("h1s", 1e-2)
+    z = np.zeros((3, n, n, n))
+    d_ncc = R.Problem(mR, mT, nt, reg, distance="ncc").objective(z)
+    d_sl2 = R.Problem(mR, mT, nt, reg).objective(z)
+    assert abs(d_ncc - d_sl2) <= 1e-12 * d_sl2
+
+
+def test_ncc_final_conditions_are_derivatives_of_the_distance():
+    # lambda(1) = -(1/hd) dD/dm1 and lambda~(1) = d lambda(1)/dm1 [m~]
+    # (src/DistanceMeasureNCC.cpp:251-510), checked by central differences in m1
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2), distance="ncc")
+    prob.set_velocity(0.3 * vs)
+    m = prob.solve_state()
+    m1 = m[nt].copy()
+    rng = np.random.default_rng(9)
+    w = rng.standard_normal(m1.shape)
+    lam = prob.final_condition()
+    lt = prob.inc_final_condition(w)
+
+    def with_m1(x):
+        prob.m = m.copy()
+        prob.m[nt] = x
+        return prob.distance(), prob.final_condition()
+
+    h = 1e-5
+    (dp, lp), (dm, lm) = with_m1(m1 + h * w), with_m1(m1 - h * w)
+    fd = (dp - dm) / (2 * h)
+    assert abs(fd + prob.hd * R.dot(lam, w)) <= 1e-6 * abs(fd)
+    assert np.linalg.norm(((lp - lm) / (2 * h) - lt).ravel()) <= 1e-6 * np.linalg.norm(lt.ravel())
+
+
+def test_ncc_taylor_gradient_and_hessian_symmetry():
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2), distance="ncc")
+    v = 0.3 * vs
+    J0 = prob.objective(v)
+    gw = R.dot(prob.gradient(v), vs)
+    for h in (1e-3, 1e-4):
+        fd = (prob.objective(v + h * vs) - J0) / h
+        assert abs(fd - gw) < 1e-2 * abs(gw)
+    prob.objective(v)
+    prob.gradient(v)
+    w2 = np.roll(vs, 3, axis=1)
+    a = prob.hessian_matvec(vs)
+    b = prob.hessian_matvec(w2)
+    assert abs(R.dot(a, w2) - R.dot(vs, b)) <= 1e-10 * np.linalg.norm(a) * np.linalg.norm(w2)
