@@ -125,6 +125,9 @@ _signatures = {
     "claire_b200_fft_grad": (_I, [_P, _P, _IA, _P]),
     "claire_b200_autotune": (_I, [_I, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
     "claire_b200_fft_variant": (_I, [_I]),
+    "claire_b200_read_nifti": (_I, [ctypes.c_char_p, _IA, _P, ctypes.c_longlong]),
+    "claire_b200_write_nifti": (_I, [ctypes.c_char_p, _IA, _P]),
+    "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
     "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
     "claire_b200_reg_apply": (_I, [_P, _P, _IA, _I, _DA, _I, _P]),
@@ -177,6 +180,38 @@ def autotune(n: int, nbatch: int = 1):
 def fft_variant_candidates(n: int):
     """FFT variants the autotuner tries for n-point grids (bit 0: radix plan, bit 1: lines per CTA)."""
     return [0, 2] if n in (16, 256) else [0, 1, 2, 3]
+
+
+def read_nifti(path: str):
+    """ReadWriteReg::ReadNII: the volume of a single-file NIfTI-1 image as a
+    float32 array of shape (nx[0], nx[1], nx[2]) = (nz, ny, nx) of the file."""
+    import numpy as np
+    nx = (ctypes.c_int * 3)()
+    _check(lib.claire_b200_read_nifti(os.fsencode(path), nx, None, 0), "read_nifti")
+    out = np.empty((nx[0], nx[1], nx[2]), dtype=np.float32)
+    _check(lib.claire_b200_read_nifti(os.fsencode(path), nx, out.ctypes.data_as(ctypes.c_void_p), out.size),
+           "read_nifti")
+    return out
+
+
+def write_nifti(path: str, arr) -> None:
+    """ReadWriteReg::WriteNII: float32 single-file NIfTI-1 (.nii, or .nii.gz compressed)."""
+    import numpy as np
+    a = np.ascontiguousarray(arr, dtype=np.float32)
+    if a.ndim != 3:
+        raise ValueError("expected a 3D volume")
+    _check(lib.claire_b200_write_nifti(os.fsencode(path), _nx(a.shape), a.ctypes.data_as(ctypes.c_void_p)),
+           "write_nifti")
+
+
+def preprocess(m, rescale: bool = True, sigma=(1.0, 1.0, 1.0)):
+    """Image preparation of the file path, in place on a CUDA tensor:
+    Normalize (rescale) then Gaussian smoothing with sigma grid cells
+    (sigma None: no smoothing)."""
+    sig = None if sigma is None else (ctypes.c_double * 3)(*[float(x) for x in sigma])
+    _check(lib.claire_b200_preprocess(_dev_ptr(m), _nx(m.shape), int(bool(rescale)), sig, _stream()),
+           "preprocess")
+    return m
 
 
 def fft_variant(n: int) -> int:

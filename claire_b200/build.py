@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libclaire_b200.so")
-SOURCES = ["fft.cu", "sl.cu", "reduce.cu", "solver.cu", "capi.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["fft.cu", "sl.cu", "reduce.cu", "solver.cu", "capi.cu", "noalloc.cu", "server.cu", "nifti.cu"]
 HEADERS = ["common.cuh", "fft_engine.cuh", "spectral.cuh", "reduce.cuh", "sl.cuh", "sl_tile.cuh", "solver.cuh"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
@@ -65,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if p.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{out.decode()}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp]
+    cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-lz", "-o", tmp]
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout.decode())

@@ -166,6 +166,27 @@ int claire_b200_autotune(int n, int nbatch, void* stream, int* variant, float* m
 /* Current FFT variant of size n (-1: unsupported), and a stored choice. */
 int claire_b200_fft_variant(int n);
 int claire_b200_set_fft_variant(int n, int variant);
+/* ---- file input / output (the path before and after the registration) ----- */
+/* ReadWriteReg::ReadNII (src/ReadWriteReg.cpp:794-1128): one scalar volume of
+ * a single-file NIfTI-1 image (.nii or .nii.gz; uint8/int8/int16/uint16/
+ * int32/uint32/int64/uint64/float32/float64).  nx receives CLAIRE's grid
+ * (nx[0] = NIfTI nz, nx[2] = NIfTI nx, src/ReadWriteReg.cpp:813-815); data
+ * (host, at least nx[0]*nx[1]*nx[2] floats = capacity, or NULL to query the
+ * size) receives the raw voxel values as float, in file order (x3 fastest).
+ * CB_ERR_UNSUPPORTED for two-file (.hdr/.img) images, several volumes or
+ * components, or other data types. */
+int claire_b200_read_nifti(const char* path, int nx[3], float* data, long long capacity);
+/* ReadWriteReg::WriteNII (src/ReadWriteReg.cpp:1130-1475): float32 single-file
+ * NIfTI-1, gzip-compressed when the path ends in .gz; pixdim = 2*pi/nx. */
+int claire_b200_write_nifti(const char* path, const int nx[3], const float* data);
+/* Image preparation of the file path on a device field (one problem):
+ * rescale != 0 applies Normalize (src/CLAIREUtils.cpp:492-525, called by
+ * CLAIREInterface::SetReferenceImage / SetTemplateImage,
+ * src/CLAIREInterface.cpp:254-320): negatives to zero, x <- (x - min) / max;
+ * sigma != NULL then applies the Gaussian smoothing of
+ * CLAIREInterface::SetupData (src/CLAIREInterface.cpp:594-626) with sigma
+ * grid cells per axis.  Synchronises the stream. */
+int claire_b200_preprocess(float* m, const int nx[3], int rescale, const double sigma[3], void* stream);
 /* accfft_grad_t: g (3n) = spectral gradient of f (n), Nyquist zeroed. */
 int claire_b200_fft_grad(const float* f, float* g, const int nx[3], void* stream);
 /* accfft_divergence_t: d (n) = spectral divergence of v (3n). */

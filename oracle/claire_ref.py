@@ -861,6 +861,19 @@ def relative_mismatch(mR, m1, mT) -> float:
 # --------------------------------------------------------------------------
 
 
+def normalize(x: np.ndarray) -> np.ndarray:
+    """Normalize for one component (src/CLAIREUtils.cpp:492-525): negative
+    values are set to zero (the shift is then zero), then x <- (x - xmin) / xmax
+    with xmin / xmax taken before the change (the division is by xmax, not by
+    the range, as written)."""
+    x = np.asarray(x, np.float64)
+    xmin, xmax = float(x.min()), float(x.max())
+    if xmin < 0.0:
+        x = np.where(x < 0.0, 0.0, x)
+        xmin = 0.0
+    return (x - xmin) / xmax
+
+
 def rescale(x: np.ndarray, xminout=0.0, xmaxout=1.0) -> np.ndarray:
     """Single-component Rescale (src/CLAIREUtils.cpp:691-725): shift only when
     min < -1e-6, then scale by xmaxout/(max-min)."""

@@ -175,3 +175,23 @@ def test_kernel_launch_counter_moves(cb):
     before = cb.kernel_launches()
     cb.fft_grad(to_dev(np.zeros((n, n, n), np.float32)))
     assert cb.kernel_launches() >= before + 3
+
+
+def test_file_path_preprocess_matches_oracle(cb, tmp_path):
+    # read (NIfTI, int16 with a negative outlier) -> Normalize -> Gaussian smoothing
+    # (src/CLAIREUtils.cpp:492-525, src/CLAIREInterface.cpp:594-626)
+    n = 32
+    rng = np.random.default_rng(77)
+    vol = (1000 * smooth_field((n, n, n), rng) + 2500).astype(np.int16)
+    vol[3, 4, 5] = -40
+    p = str(tmp_path / "img.nii.gz")
+    cb.write_nifti(p, vol.astype(np.float32))
+    img = cb.read_nifti(p)
+    assert np.array_equal(img, vol.astype(np.float32))
+    dev = to_dev(img)
+    cb.preprocess(dev, rescale=True, sigma=(1.0, 1.0, 1.0))
+    ref = R.gaussian_smooth(R.normalize(img.astype(np.float64)), 1.0)
+    assert rel(dev.cpu().numpy(), ref) < TOL
+    dev2 = to_dev(img)
+    cb.preprocess(dev2, rescale=True, sigma=None)
+    assert rel(dev2.cpu().numpy(), R.normalize(img.astype(np.float64))) < 1e-6
