@@ -58,6 +58,7 @@ class Opts(ctypes.Structure):
         ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int), ("betacont", ctypes.c_double),
         ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int), ("distance", ctypes.c_int),
+        ("scalecont", ctypes.c_int), ("gridcont", ctypes.c_int),
     ]
 
 
@@ -125,6 +126,7 @@ _signatures = {
     "claire_b200_fft_grad": (_I, [_P, _P, _IA, _P]),
     "claire_b200_autotune": (_I, [_I, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
     "claire_b200_fft_variant": (_I, [_I]),
+    "claire_b200_grid_change": (_I, [_P, _I, _P, _I, _I, _P]),
     "claire_b200_read_nifti": (_I, [ctypes.c_char_p, _IA, _P, ctypes.c_longlong]),
     "claire_b200_write_nifti": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
@@ -212,6 +214,19 @@ def preprocess(m, rescale: bool = True, sigma=(1.0, 1.0, 1.0)):
     _check(lib.claire_b200_preprocess(_dev_ptr(m), _nx(m.shape), int(bool(rescale)), sig, _stream()),
            "preprocess")
     return m
+
+
+def grid_change(f, nt: int):
+    """Preprocessing::Restrict / Prolong of a cubic CUDA field, or of a stack of
+    them (leading dimension), to nt^3 points."""
+    torch = _torch()
+    ns = f.shape[-1]
+    nf = 1
+    for k in f.shape[:-3]:
+        nf *= int(k)
+    out = torch.empty(tuple(f.shape[:-3]) + (nt, nt, nt), device=f.device, dtype=torch.float32)
+    _check(lib.claire_b200_grid_change(_dev_ptr(f), int(ns), _dev_ptr(out), int(nt), nf, _stream()), "grid_change")
+    return out
 
 
 def fft_variant(n: int) -> int:

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libclaire_b200.so")
-SOURCES = ["fft.cu", "sl.cu", "reduce.cu", "solver.cu", "capi.cu", "noalloc.cu", "server.cu", "nifti.cu"]
+SOURCES = ["fft.cu", "sl.cu", "reduce.cu", "solver.cu", "capi.cu", "noalloc.cu", "server.cu", "nifti.cu", "grid.cu"]
 HEADERS = ["common.cuh", "fft_engine.cuh", "spectral.cuh", "reduce.cuh", "sl.cuh", "sl_tile.cuh", "solver.cuh"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

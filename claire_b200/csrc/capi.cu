@@ -5,10 +5,12 @@
 // operator functions mirror the inner seams SemiLagrangian, Regularization,
 // DistanceMeasureSL2 and the AccFFT spectral calls so each piece can be
 // swapped and tested on its own.  No exception crosses the ABI.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -64,6 +66,8 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->bf16_images = 0;
   o->autotune = 0;
   o->distance = CB_DIST_SL2;  // src/RegOpt.cpp:1079
+  o->scalecont = 0;
+  o->gridcont = 0;
   return CB_OK;
 }
 
@@ -146,6 +150,10 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (!std::strcmp(val, "sl2")) o->distance = CB_DIST_SL2;
       else if (!std::strcmp(val, "ncc")) o->distance = CB_DIST_NCC;
       else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-scalecont")) {
+      o->scalecont = 1;  // src/RegOpt.cpp:769-770
+    } else if (!std::strcmp(a, "-gridcont")) {
+      o->gridcont = 1;  // src/RegOpt.cpp:771-772
     } else if (!std::strcmp(a, "-autotune")) {
       o->autotune = 1;
     } else if (!std::strcmp(a, "-bf16images")) {
@@ -250,16 +258,189 @@ int claire_b200_get_velocity(const claire_b200_ctx* c, int b, float* v, int on_d
   return copy_out(s, v, s.v + b * 3 * s.n, 3 * s.n, on_device);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Device buffer freed on scope exit.
+struct DevBuf {
+  float* p = nullptr;
+  int alloc(long long floats) { return cudaMalloc((void**)&p, sizeof(float) * (size_t)floats) == cudaSuccess ? 0 : CB_ERR_ALLOC; }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+// Carry the per-problem options (norm, weights) of `from` to a level solver.
+int copy_problem_opts(const Solver& from, Solver& to) {
+  for (int b = 0; b < from.B; ++b) {
+    claire_b200_opts o = to.opts;
+    o.regnorm = from.ps[b].norm;
+    o.beta[0] = from.ps[b].beta0;
+    o.beta[1] = from.ps[b].beta1;
+    o.beta[2] = from.ps[b].beta2;
+    if (int e = to.set_problem(b, o)) return e;
+  }
+  return 0;
+}
+
+// CLAIREInterface::RunSolverScaleCont (src/CLAIREInterface.cpp:1387-1505): the
+// original images are smoothed with sigma = 32, 16, ..., 1 grid cells (levels
+// with n/2 <= sigma skipped, sigmas of src/RegOpt.cpp:1241-1246); every level
+// re-initialises ||g0|| at v = 0 and warm-starts from the current velocity.
+int run_scalecont(Solver& s, const std::vector<int>& sel) {
+  if (s.img16) {
+    s.err = "scale continuation needs FP32 images";
+    return CB_ERR_UNSUPPORTED;
+  }
+  const long long n = s.n;
+  DevBuf orig;
+  if (int e = orig.alloc(2 * n * s.B)) return e;
+  if (cudaMemcpyAsync(orig.p, s.mR, sizeof(float) * n * s.B, cudaMemcpyDeviceToDevice, s.stream) != cudaSuccess ||
+      cudaMemcpyAsync(orig.p + n * s.B, s.mT, sizeof(float) * n * s.B, cudaMemcpyDeviceToDevice, s.stream) !=
+          cudaSuccess)
+    return CB_ERR_CUDA;
+  SpecParams* par = nullptr;
+  if (cudaMalloc((void**)&par, sizeof(SpecParams) * s.B) != cudaSuccess) return CB_ERR_ALLOC;
+  static const double kSigmas[6] = {32.0, 16.0, 8.0, 4.0, 2.0, 1.0};
+  int e = 0;
+  bool first = true;
+  for (int l = 0; l < 6 && !e; ++l) {
+    const double sig = kSigmas[l];
+    if (0.5 * s.d.n1 <= sig) continue;
+    std::vector<SpecParams> hp(s.B);
+    for (auto& p : hp) {
+      p = SpecParams{};
+      p.hd = s.hd;
+      p.sigma[0] = p.sigma[1] = p.sigma[2] = (float)sig;
+    }
+    e = cudaMemcpyAsync(par, hp.data(), sizeof(SpecParams) * s.B, cudaMemcpyHostToDevice, s.stream) ? CB_ERR_CUDA : 0;
+    // Preprocessing::Smooth of both originals (2B fields through the 3-field spectrum workspace)
+    for (int img = 0; img < 2 && !e; ++img) {
+      const float* src = orig.p + img * n * s.B;
+      float* dst = img == 0 ? s.mR : s.mT;
+      e = launch_r2c3d(src, n, n, s.spec, 3 * s.nc, 1, s.B, s.d, nullptr, s.stream);
+      if (!e) e = launch_pencil(s.spec, 3 * s.nc, s.B, s.d, OP_GAUSS, par, 1, 1, nullptr, s.stream);
+      if (!e) e = launch_c2r3d(s.spec, 3 * s.nc, dst, n, n, 1, s.B, s.d, EPI_STORE, nullptr, nullptr, 0, nullptr,
+                               s.stream);
+    }
+    if (e) break;
+    for (int b = 0; b < s.B; ++b) s.images_changed(b);
+    if (!first) {
+      s.carry_krylov_g0.assign(s.B, -1.0);
+      for (int b = 0; b < s.B; ++b) s.carry_krylov_g0[b] = s.ps[b].krylov_g0;
+    }
+    e = s.run(sel);
+    first = false;
+  }
+  s.carry_krylov_g0.clear();
+  cudaFree(par);
+  return e;
+}
+
+// CLAIREInterface::RunSolverGridCont (src/CLAIREInterface.cpp:1510-1705):
+// levels of RegOpt::SetupGridCont (src/RegOpt.cpp:1844-1930), images
+// restricted from the finest grid to each level, v = 0 on the coarsest level
+// and prolonged to the next, the gradient tolerance 10x looser below the
+// finest level when it is under 0.01, the Krylov reference norm of the first
+// solve kept.  The finest level is the context's own solver.
+int run_gridcont(Solver& s, const std::vector<int>& sel) {
+  if (s.img16) {
+    s.err = "grid continuation needs FP32 images";
+    return CB_ERR_UNSUPPORTED;
+  }
+  const int nf = s.d.n1;
+  int nlev = (int)std::ceil(std::log2((double)nf)) - 3;
+  if (nlev < 1) nlev = 1;
+  std::vector<int> sizes(nlev);
+  sizes[nlev - 1] = nf;
+  for (int l = nlev - 2; l >= 0; --l) sizes[l] = (sizes[l + 1] + 1) / 2;
+  const double greltol = s.opts.opttol;
+  DevBuf vprev, work;
+  long long wmax = 0;
+  for (int l = 0; l < nlev; ++l) {
+    wmax = std::max(wmax, grid_change_work(nf, sizes[l], s.B));
+    if (l + 1 < nlev) wmax = std::max(wmax, grid_change_work(sizes[l], sizes[l + 1], 3 * s.B));
+  }
+  if (int e = work.alloc(std::max(wmax, 1LL))) return e;
+  int prev = 0;  // size of the last solved level (0: none yet)
+  std::vector<double> kg0;
+  for (int l = 0; l < nlev; ++l) {
+    const int nl = sizes[l];
+    const bool last = l == nlev - 1;
+    if (!last && !fft_size_supported(nl)) continue;  // no FFT plan for this size here
+    std::unique_ptr<Solver> own;
+    Solver* lv = &s;
+    if (!last) {
+      claire_b200_opts o = s.opts;
+      o.nx[0] = o.nx[1] = o.nx[2] = nl;
+      o.gridcont = 0;
+      if (greltol < 0.01) o.opttol = 10.0 * greltol;
+      own.reset(new (std::nothrow) Solver());
+      if (!own) return CB_ERR_ALLOC;
+      if (int e = own->init(o, s.B)) {
+        s.err = own->err;
+        return e;
+      }
+      own->stream = s.stream;
+      if (int e = copy_problem_opts(s, *own)) return e;
+      lv = own.get();
+      const long long nn = (long long)nl * nl * nl;
+      if (int e = launch_grid_change(s.mR, s.n, nf, lv->mR, nn, nl, s.B, work.p, s.stream)) return CB_ERR_CUDA;
+      if (int e = launch_grid_change(s.mT, s.n, nf, lv->mT, nn, nl, s.B, work.p, s.stream)) return CB_ERR_CUDA;
+      for (int b = 0; b < s.B; ++b) lv->images_changed(b);
+    }
+    const long long nn = (long long)nl * nl * nl;
+    if (prev) {
+      const long long np = (long long)prev * prev * prev;
+      if (launch_grid_change(vprev.p, np, prev, lv->v, nn, nl, 3 * s.B, work.p, s.stream)) return CB_ERR_CUDA;
+    } else if (cudaMemsetAsync(lv->v, 0, sizeof(float) * 3 * nn * s.B, s.stream) != cudaSuccess) {
+      return CB_ERR_CUDA;
+    }
+    for (int b = 0; b < s.B; ++b) lv->state_of[b] = 0;
+    lv->carry_krylov_g0 = kg0;
+    if (int e = lv->run(sel)) {
+      if (lv != &s) s.err = lv->err;
+      return e;
+    }
+    lv->carry_krylov_g0.clear();
+    kg0.assign(s.B, -1.0);
+    for (int b = 0; b < s.B; ++b) kg0[b] = lv->ps[b].krylov_g0;
+    if (!last) {
+      DevBuf nv;
+      if (int e = nv.alloc(3 * nn * s.B)) return e;
+      if (cudaMemcpyAsync(nv.p, lv->v, sizeof(float) * 3 * nn * s.B, cudaMemcpyDeviceToDevice, s.stream) !=
+              cudaSuccess ||
+          cudaStreamSynchronize(s.stream) != cudaSuccess)
+        return CB_ERR_CUDA;
+      std::swap(vprev.p, nv.p);
+      prev = nl;
+    }
+  }
+  return 0;
+}
+
+int run_dispatch(Solver& s, const std::vector<int>& sel) {
+  if (s.opts.betacont > 0.0) return s.run(sel);  // RunSolverRegParaCont first (src/CLAIREInterface.cpp:729-753)
+  if (s.opts.scalecont) return run_scalecont(s, sel);
+  if (s.opts.gridcont) return run_gridcont(s, sel);
+  return s.run(sel);
+}
+
+}  // namespace
+
+extern "C" {
+
 int claire_b200_run(claire_b200_ctx* c) {
   if (!c) return CB_ERR_ARG;
   std::vector<int> sel(c->solver.B, 1);
-  return cuda_status(c->solver.run(sel));
+  return cuda_status(run_dispatch(c->solver, sel));
 }
 
 int claire_b200_run_masked(claire_b200_ctx* c, const int* mask) {
   if (!c || !mask) return CB_ERR_ARG;
   std::vector<int> sel(mask, mask + c->solver.B);
-  return cuda_status(c->solver.run(sel));
+  return cuda_status(run_dispatch(c->solver, sel));
 }
 
 int claire_b200_get_final_state(claire_b200_ctx* c, int b, float* m1, int on_device) {
@@ -481,6 +662,19 @@ int claire_b200_fft_variant(int n) { return fft_size_supported(n) ? fft_variant(
 int claire_b200_set_fft_variant(int n, int variant) {
   if (!fft_size_supported(n)) return CB_ERR_ARG;
   return set_fft_variant(n, variant) ? CB_ERR_ARG : CB_OK;
+}
+
+int claire_b200_grid_change(const float* in, int ns, float* out, int nt, int nf, void* stream) {
+  if (!in || !out || ns < 2 || nt < 2 || nf < 1 || ns > 1024 || nt > 1024) return CB_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* work = nullptr;
+  const long long w = std::max(grid_change_work(ns, nt, nf), 1LL);
+  if (cudaMallocAsync((void**)&work, sizeof(float) * (size_t)w, st) != cudaSuccess) return CB_ERR_ALLOC;
+  const long long ni = (long long)ns * ns * ns, no = (long long)nt * nt * nt;
+  const int e = launch_grid_change(in, ni, ns, out, no, nt, nf, work, st);
+  cudaFreeAsync(work, st);
+  note_launches(3);
+  return cuda_status(e);
 }
 
 int claire_b200_fft_grad(const float* f, float* gout, const int nx[3], void* stream) {

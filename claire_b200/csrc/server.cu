@@ -347,6 +347,9 @@ int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_serv
 int claire_b200_server_submit(claire_b200_server* s, const claire_b200_opts* o, const float* mR, const float* mT,
                               long long* id) {
   if (!s || !o || !mR || !mT || !id) return CB_ERR_ARG;
+  // a pool advances its slots one GN iteration at a time: the continuation
+  // drivers (several solves per request) run through claire_b200_run instead
+  if (o->betacont > 0.0 || o->scalecont || o->gridcont) return CB_ERR_UNSUPPORTED;
   if (o->nx[0] <= 0 || o->nx[1] <= 0 || o->nx[2] <= 0 || o->nt < 1) return CB_ERR_ARG;
   const long long n = (long long)o->nx[0] * o->nx[1] * o->nx[2];
   cb::srv::Request r;

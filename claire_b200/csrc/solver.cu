@@ -1157,8 +1157,25 @@ int Solver::begin(const std::vector<int>& sel) {
       ps[b].beta2 = keep.beta2;
       ps[b].running = true;
       ps[b].t0 = std::chrono::steady_clock::now();
+      if ((int)carry_krylov_g0.size() == B) ps[b].krylov_g0 = carry_krylov_g0[b];
       state_of[b] = 0;
     }
+  // InitializeOptimization (src/CLAIRE.cpp:227-357): D0, J0 and ||g0|| at the
+  // zero velocity; a nonzero initial guess is set aside meanwhile and the GN
+  // loop then starts from it.
+  CB_TRY(upload_mask(sel, dact2));
+  CB_TRY(dot(v, 3 * n, v, 3 * n, 3 * n, S_GD, dact2));
+  CB_TRY(fetch_scalars());
+  std::vector<int> guess(B, 0);
+  bool any_guess = false;
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && hsc[S_GD * B + b] > 0.0) { guess[b] = 1; any_guess = true; }
+  if (any_guess) {
+    CB_TRY(upload_mask(guess, dact2));
+    CB_TRY(launch_lincomb(x, 3 * n, v, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact2, stream));
+    CB_TRY(launch_fill(v, 3 * n, 0.f, 3 * n, B, dact2, stream));
+    note_launches(2);
+  }
   CB_TRY(objective_at(v, sel));
   CB_TRY(gradient_at_current(sel));
   for (int b = 0; b < B; ++b)
@@ -1167,6 +1184,15 @@ int Solver::begin(const std::vector<int>& sel) {
       ps[b].D0 = ps[b].D;
       ps[b].gnorm0 = ps[b].gnorm > 0.0 ? ps[b].gnorm : 1.0;
     }
+  if (any_guess) {
+    CB_TRY(upload_mask(guess, dact2));
+    CB_TRY(launch_lincomb(v, 3 * n, x, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact2, stream));
+    note_launches(1);
+    for (int b = 0; b < B; ++b)
+      if (guess[b]) state_of[b] = 0;
+    CB_TRY(objective_at(v, guess));
+    CB_TRY(gradient_at_current(guess));
+  }
   return 0;
 }
 

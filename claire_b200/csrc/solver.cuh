@@ -102,6 +102,9 @@ class Solver {
               S_NA, S_NRR, S_NI, S_NL2, S_NS, S_NIM, S_NRM, S_CA, S_CB, S_CC, NSLOT };
   enum ISlot { I_IT = 0, I_REASON, NISLOT };
 
+  // Krylov reference norms handed to the next begin() (continuation levels keep
+  // the first solve's, src/KrylovInterface.cpp:125-134); empty: fresh
+  std::vector<double> carry_krylov_g0;
   // velocity for which m / disp_st are valid, per problem: 0 none, 1 v, 2 vtrial
   std::vector<int> state_of;
   // NCC distance (opts.distance == CB_DIST_NCC): scale set up per image pair

@@ -83,6 +83,12 @@ int fft_autotune_once(int n, int nprob, cudaStream_t s);
 
 bool fft_size_supported(int n);
 
+// Spectral grid change (restriction / prolongation) of nf cubic fields, ns^3
+// (ip apart) -> nt^3 (op apart); work: grid_change_work(ns, nt, nf) floats.
+long long grid_change_work(int ns, int nt, int nf);
+int launch_grid_change(const float* in, long long ip, int ns, float* out, long long op, int nt, int nf, float* work,
+                       cudaStream_t s);
+
 // 3-field op (forward r2c, op in the x1 pass, inverse c2r stored to out) using
 // a caller-provided spectrum workspace (3 * nc float2) and twiddle table
 // (W_N^m, m < N); allocates nothing.

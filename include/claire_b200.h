@@ -68,6 +68,8 @@ typedef struct claire_b200_opts {
   int autotune;         /* -autotune: measure the FFT variants of this grid size when the first
                            context of that size is created (claire_b200_autotune) */
   int distance;         /* -distance sl2|ncc (CB_DIST_SL2); NCC needs FP32 images */
+  int scalecont;        /* -scalecont: continuation over image smoothing widths */
+  int gridcont;         /* -gridcont: continuation over grid sizes */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {
@@ -107,7 +109,15 @@ int claire_b200_set_images(claire_b200_ctx* ctx, int b, const float* mR, const f
 /* SetInitialGuess (src/CLAIREInterface.cpp: copy semantics). */
 int claire_b200_set_velocity(claire_b200_ctx* ctx, int b, const float* v, int on_device);
 int claire_b200_get_velocity(const claire_b200_ctx* ctx, int b, float* v, int on_device);
-/* Run: GN-Krylov solve of every problem in the context (RunSolver). */
+/* Run: GN-Krylov solve of every problem in the context (CLAIREInterface::Run,
+ * src/CLAIREInterface.cpp:709-885): with -betacont the parameter
+ * continuation, else with -scalecont the smoothing continuation
+ * (RunSolverScaleCont, :1387-1505: sigma = 32, 16, ..., 1 cells while below
+ * n/2), else with -gridcont the grid continuation (RunSolverGridCont,
+ * :1510-1705: ceil(log2 n) - 3 levels of halved grids, images restricted,
+ * velocity prolonged; sizes without an FFT plan here are skipped), else
+ * RunSolver.  Continuation runs end with the images of their last level in
+ * the context (smoothed with sigma = 1 for -scalecont). */
 int claire_b200_run(claire_b200_ctx* ctx);
 /* Solve only the problems whose mask entry is nonzero. */
 int claire_b200_run_masked(claire_b200_ctx* ctx, const int* mask);
@@ -187,6 +197,11 @@ int claire_b200_write_nifti(const char* path, const int nx[3], const float* data
  * CLAIREInterface::SetupData (src/CLAIREInterface.cpp:594-626) with sigma
  * grid cells per axis.  Synchronises the stream. */
 int claire_b200_preprocess(float* m, const int nx[3], int rescale, const double sigma[3], void* stream);
+/* Preprocessing::Restrict / Prolong (src/Preprocessing.cpp:733-917,
+ * 1605-1786): nf cubic fields of ns^3 points (consecutive) to nt^3 points
+ * (consecutive) by spectral truncation / zero padding, coefficients
+ * |w| < min(ns, nt)/2 per axis.  Scratch from the stream-ordered allocator. */
+int claire_b200_grid_change(const float* in, int ns, float* out, int nt, int nf, void* stream);
 /* accfft_grad_t: g (3n) = spectral gradient of f (n), Nyquist zeroed. */
 int claire_b200_fft_grad(const float* f, float* g, const int nx[3], void* stream);
 /* accfft_divergence_t: d (n) = spectral divergence of v (3n). */

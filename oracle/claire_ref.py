@@ -752,8 +752,19 @@ def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None
     Returns a dict with the velocity, iteration counts and monitor values.
     """
     v = np.zeros((3,) + prob.shape, dtype=prob.dtype) if v0 is None else np.asarray(v0, prob.dtype).copy()
-    J = prob.objective(v)
-    D0 = prob.last_D
+    if g0 is None and np.any(v):
+        # InitializeOptimization (src/CLAIRE.cpp:227-357): D0, J0 and ||g0|| at
+        # the zero velocity, then the loop starts from the initial guess
+        z = np.zeros_like(v)
+        prob.objective(z)
+        D0 = prob.last_D
+        gz = prob.gradient(z)
+        g0 = math.sqrt(dot(gz, gz))
+        g0 = g0 if g0 > 0 else 1.0
+        J = prob.objective(v)
+    else:
+        J = prob.objective(v)
+        D0 = prob.last_D
     g = prob.gradient(v)
     gnorm = math.sqrt(dot(g, g))
     if g0 is None:
@@ -846,6 +857,88 @@ def beta_continuation(prob: Problem, beta_star: float, opts: GNOptions = GNOptio
     res = gauss_newton(prob, opts, v0=v, log=log, g0=g0, krylov_g0=kg0, miniter=1)
     levels.append(res["iters"])
     res["levels"] = levels
+    return res
+
+
+def grid_transfer(f: np.ndarray, nt: int) -> np.ndarray:
+    """Restriction / prolongation of a cubic field to nt^3 points
+    (Preprocessing::Restrict / Prolong, src/Preprocessing.cpp:765-917,
+    1636-1786, index map of ComputeGridChangeIndices :918-1057): the
+    coefficients of the wavenumbers |w| < min(ns, nt)/2 on every axis, scaled
+    by 1/ns^3, transformed back unnormalised on the target grid."""
+    f = np.asarray(f, np.float64)
+    ns = f.shape[0]
+    if ns == nt:
+        return f.copy()
+    nc = min(ns, nt)
+    w = np.arange(-((nc + 1) // 2 - 1), (nc + 1) // 2)
+    src, dst = w % ns, w % nt
+    fh = np.fft.fftn(f)
+    out = np.zeros((nt, nt, nt), dtype=complex)
+    out[np.ix_(dst, dst, dst)] = fh[np.ix_(src, src, src)] / float(ns) ** 3
+    return np.real(np.fft.ifftn(out)) * float(nt) ** 3
+
+
+def grid_levels(n: int):
+    """Grid sizes of the continuation levels (RegOpt::SetupGridCont,
+    src/RegOpt.cpp:1844-1930): ceil(log2 n) - 3 levels, each half the next
+    (rounded up), the finest n."""
+    nlev = max(1, int(math.ceil(math.log2(n))) - 3)
+    sizes = [n]
+    for _ in range(nlev - 1):
+        sizes.insert(0, int(math.ceil(sizes[0] / 2.0)))
+    return sizes
+
+
+def grid_continuation(mR, mT, nt: int, reg: Regularization, opts: GNOptions = GNOptions(),
+                      supported=lambda n: True, **problem_kw):
+    """CLAIREInterface::RunSolverGridCont (src/CLAIREInterface.cpp:1510-1705):
+    images restricted from the finest grid to every level; v = 0 on the
+    coarsest level, prolonged to the next; the gradient tolerance is 10x
+    looser below the finest level when it is under 0.01; each level's
+    InitializeOptimization sets ||g0|| at v = 0, while the Krylov reference
+    norm is the first level's (set once per run, src/KrylovInterface.cpp:125-134).
+    Levels whose size `supported` rejects are skipped and the velocity goes
+    on from the last solved level."""
+    import dataclasses
+    sizes = grid_levels(mR.shape[0])
+    v, vsize, kg0, res, levels = None, None, None, None, []
+    for l, nl in enumerate(sizes):
+        if not supported(nl):
+            continue
+        last = l == len(sizes) - 1
+        prob = Problem(grid_transfer(mR, nl), grid_transfer(mT, nl), nt, reg, **problem_kw)
+        v0 = None if v is None else np.stack([grid_transfer(v[k], nl) for k in range(3)])
+        tol = opts.gttol * 10.0 if (opts.gttol < 0.01 and not last) else opts.gttol
+        res = gauss_newton(prob, dataclasses.replace(opts, gttol=tol), v0=v0, krylov_g0=kg0)
+        v, vsize, kg0 = res["v"], nl, res["krylov_g0"]
+        levels.append((nl, res["iters"]))
+    res["levels"] = levels
+    res["prob"] = prob
+    return res
+
+
+SCALE_SIGMAS = (32.0, 16.0, 8.0, 4.0, 2.0, 1.0)  # src/RegOpt.cpp:1241-1246
+
+
+def scale_continuation(mR, mT, nt: int, reg: Regularization, opts: GNOptions = GNOptions(), **problem_kw):
+    """CLAIREInterface::RunSolverScaleCont (src/CLAIREInterface.cpp:1387-1505):
+    for sigma = 32, 16, ..., 1 grid cells (skipped when n/2 <= sigma) the
+    original images are smoothed with sigma, ||g0|| is set at v = 0 and the GN
+    solve warm-starts from the previous level's velocity (Krylov reference
+    norm from the first level)."""
+    n = mR.shape[0]
+    v, kg0, res, levels = None, None, None, []
+    for sig in SCALE_SIGMAS:
+        if n / 2.0 <= sig:
+            continue
+        prob = Problem(gaussian_smooth(np.asarray(mR, np.float64), sig),
+                       gaussian_smooth(np.asarray(mT, np.float64), sig), nt, reg, **problem_kw)
+        res = gauss_newton(prob, opts, v0=v, krylov_g0=kg0)
+        v, kg0 = res["v"], res["krylov_g0"]
+        levels.append((sig, res["iters"]))
+    res["levels"] = levels
+    res["prob"] = prob
     return res
 
 

@@ -275,3 +275,28 @@ def test_ncc_taylor_gradient_and_hessian_symmetry():
     a = prob.hessian_matvec(vs)
     b = prob.hessian_matvec(w2)
     assert abs(R.dot(a, w2) - R.dot(vs, b)) <= 1e-10 * np.linalg.norm(a) * np.linalg.norm(w2)
+
+
+def test_grid_transfer_known_answers():
+    # band-limited fields are carried exactly; restriction after prolongation
+    # is the identity; modes at or above the coarse Nyquist index are dropped
+    n = 16
+    x1, x2, x3 = R.grid_coords((n, n, n))
+    f = np.sin(2 * x1) * np.cos(3 * x2) + 0.5 * np.cos(x3) + 0.25
+    fine = R.grid_transfer(f, 32)
+    y1, y2, y3 = R.grid_coords((32, 32, 32))
+    assert np.max(np.abs(fine - (np.sin(2 * y1) * np.cos(3 * y2) + 0.5 * np.cos(y3) + 0.25))) < 1e-12
+    assert np.max(np.abs(R.grid_transfer(fine, 16) - f)) < 1e-12
+    g = np.cos(8 * y1) + np.cos(7 * y2)   # 8 = the Nyquist wavenumber of 16 points
+    assert np.max(np.abs(R.grid_transfer(g, 16) - np.cos(7 * x2))) < 1e-12
+    assert R.grid_levels(128) == [16, 32, 64, 128] and R.grid_levels(96) == [12, 24, 48, 96]
+    assert R.grid_levels(32) == [16, 32]
+
+
+def test_initialization_uses_zero_velocity_for_g0():
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    prob = R.Problem(mR, mT, nt, R.Regularization("h1s", 1e-2))
+    g = prob.gradient(np.zeros_like(vs))
+    res = R.gauss_newton(prob, R.GNOptions(maxit=1, gttol=1e-2), v0=0.2 * vs)
+    assert abs(res["g0"] - np.sqrt(R.dot(g, g))) <= 1e-12 * res["g0"]
