@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=20.0, help="--serve: arrivals per second")
     ap.add_argument("--slots", type=int, default=4, help="--serve: slots per pool")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default FFT variants (no measurement)")
+    ap.add_argument("--fft-variant", type=int, default=-1,
+                    help="use this FFT variant for the workload's grid instead of measuring (profiling runs)")
     ap.add_argument("--mixed", action="store_true",
                     help="mixed batch instead: 12 x 64^3 + 12 x 96^3 + 8 x 128^3 (H1 beta=1e-2, nt=4) served "
                          "together against plain one-at-a-time runs")
@@ -172,7 +174,11 @@ def run_ours(a, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     B = a.batch
-    tuned = None if a.no_autotune else tune(cb, [a.n], B)
+    if a.fft_variant >= 0:
+        cb.set_fft_variant(a.n, a.fft_variant)
+        tuned = {str(a.n): {"variant": a.fft_variant, "set_by": "--fft-variant"}}
+    else:
+        tuned = None if a.no_autotune else tune(cb, [a.n], B)
     # seeded inputs: problem index = rank*B + b
     probs = [synthetic.ellipsoid_problem(a.n, a.nt, 1, rank * B + b, dev) for b in range(B)]
     host = [(p[0].cpu().pin_memory(), p[1].cpu().pin_memory()) for p in probs]
