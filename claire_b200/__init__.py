@@ -107,6 +107,7 @@ _signatures = {
     "claire_b200_set_problem_opts": (_I, [_P, _I, ctypes.POINTER(Opts)]),
     "claire_b200_set_images": (_I, [_P, _I, _P, _P, _I]),
     "claire_b200_set_velocity": (_I, [_P, _I, _P, _I]),
+    "claire_b200_set_mask": (_I, [_P, _I, _P, _I]),
     "claire_b200_get_velocity": (_I, [_P, _I, _P, _I]),
     "claire_b200_run": (_I, [_P]),
     "claire_b200_run_masked": (_I, [_P, _IA]),
@@ -402,6 +403,14 @@ class CLAIREInterface:
     def _set_images(self, b):
         self.set_images(self._mR[1], self._mT[1], b)
         self._mR = self._mT = None
+
+    def SetMask(self, w, b: int = 0):
+        """Distance-measure weights of problem b (None removes the mask)."""
+        if w is None:
+            _check(lib.claire_b200_set_mask(self._ctx, b, None, 0), "SetMask", self._ctx)
+            return
+        p, dev, keep = self._src(w, self._n())
+        _check(lib.claire_b200_set_mask(self._ctx, b, p, dev), "SetMask", self._ctx)
 
     def SetInitialGuess(self, v, b: int = 0):
         p, dev, keep = self._src(v, 3 * self._n())

@@ -245,6 +245,18 @@ int claire_b200_set_images(claire_b200_ctx* c, int b, const float* mR, const flo
   return e;
 }
 
+int claire_b200_set_mask(claire_b200_ctx* c, int b, const float* w, int on_device) {
+  if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  const float* src = w;
+  if (w && !on_device) {
+    float* st = s.x + b * 3 * s.n;  // problem b's PCG work vector, idle between solver calls
+    if (int e = copy_in(s, st, w, s.n, 0)) return e;
+    src = st;
+  }
+  return cuda_status(s.set_mask(b, src));
+}
+
 int claire_b200_set_velocity(claire_b200_ctx* c, int b, const float* v, int on_device) {
   if (!c || !v || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

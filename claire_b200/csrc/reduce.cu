@@ -323,4 +323,100 @@ int launch_diff16(float* y, long long yp, const bf16* a, long long ap, const bf1
   return (int)cudaGetLastError();
 }
 
+// ---- mask-weighted distance terms (DistanceMeasure with SetMask) --------------
+
+CB_DEVICE float ldv(const float* p, long long i) { return p[i]; }
+CB_DEVICE float ldv(const bf16* p, long long i) { return __bfloat162float(p[i]); }
+
+template <class T>
+__global__ void __launch_bounds__(kRedThreads) k_wdiff_sumsq(const T* __restrict__ a, long long ap,
+                                                              const T* __restrict__ b, long long bp,
+                                                              const float* __restrict__ w, long long wp,
+                                                              long long len, double* __restrict__ partials,
+                                                              int nparts, const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const T* pa = a + blockIdx.y * ap;
+  const T* pb = b + blockIdx.y * bp;
+  const float* pw = w + blockIdx.y * wp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double d = (double)ldv(pa, i) - (double)ldv(pb, i);
+    acc += (double)pw[i] * d * d;
+  }
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+template <class T>
+__global__ void k_wdiff(float* __restrict__ y, long long yp, const T* __restrict__ a, long long ap,
+                        const T* __restrict__ b, long long bp, const float* __restrict__ w, long long wp,
+                        long long len, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[p * yp + i] = w[p * wp + i] * (ldv(a + p * ap, i) - ldv(b + p * bp, i));
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_wdot(const float* __restrict__ a, long long ap,
+                                                       const float* __restrict__ b, long long bp,
+                                                       const float* __restrict__ w, long long wp, long long len,
+                                                       double* __restrict__ partials, int nparts,
+                                                       const int* __restrict__ active) {
+  if (active && !active[blockIdx.y]) return;
+  const float* pa = a + blockIdx.y * ap;
+  const float* pb = b + blockIdx.y * bp;
+  const float* pw = w + blockIdx.y * wp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x)
+    acc += (double)pw[i] * (double)pa[i] * (double)pb[i];
+  block_reduce_store(acc, partials + (long long)blockIdx.y * nparts, blockIdx.x);
+}
+
+__global__ void k_mulw(float* __restrict__ y, long long yp, const float* __restrict__ w, long long wp, long long len,
+                       const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+    y[p * yp + i] *= w[p * wp + i];
+}
+
+int launch_wdiff_sumsq(const float* a, long long ap, const float* b, long long bp, const float* w, long long wp,
+                       long long len, int nprob, double* partials, int stride, const int* active, cudaStream_t s) {
+  k_wdiff_sumsq<float><<<dim3(dot_partials(len), nprob), kRedThreads, 0, s>>>(a, ap, b, bp, w, wp, len, partials,
+                                                                              stride, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_wdiff_sumsq(const bf16* a, long long ap, const bf16* b, long long bp, const float* w, long long wp,
+                       long long len, int nprob, double* partials, int stride, const int* active, cudaStream_t s) {
+  k_wdiff_sumsq<bf16><<<dim3(dot_partials(len), nprob), kRedThreads, 0, s>>>(a, ap, b, bp, w, wp, len, partials,
+                                                                             stride, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_wdiff(float* y, long long yp, const float* a, long long ap, const float* b, long long bp, const float* w,
+                 long long wp, long long len, int nprob, const int* active, cudaStream_t s) {
+  k_wdiff<float><<<stream_grid(len, nprob), 256, 0, s>>>(y, yp, a, ap, b, bp, w, wp, len, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_wdiff(float* y, long long yp, const bf16* a, long long ap, const bf16* b, long long bp, const float* w,
+                 long long wp, long long len, int nprob, const int* active, cudaStream_t s) {
+  k_wdiff<bf16><<<stream_grid(len, nprob), 256, 0, s>>>(y, yp, a, ap, b, bp, w, wp, len, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_wdot(const float* a, long long ap, const float* b, long long bp, const float* w, long long wp, long long len,
+                int nprob, double* partials, int stride, const int* active, cudaStream_t s) {
+  k_wdot<<<dim3(dot_partials(len), nprob), kRedThreads, 0, s>>>(a, ap, b, bp, w, wp, len, partials, stride, active);
+  return (int)cudaGetLastError();
+}
+
+int launch_mulw(float* y, long long yp, const float* w, long long wp, long long len, int nprob, const int* active,
+                cudaStream_t s) {
+  k_mulw<<<stream_grid(len, nprob), 256, 0, s>>>(y, yp, w, wp, len, active);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace cb

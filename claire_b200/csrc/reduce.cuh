@@ -79,4 +79,18 @@ int launch_diff_sumsq16(const bf16* a, long long ap, const bf16* b, long long bp
 int launch_diff16(float* y, long long yp, const bf16* a, long long ap, const bf16* b, long long bp, long long len,
                   int nprob, const int* active, cudaStream_t s);
 
+// ---- mask weights w (SetMask): sum w (a - b)^2, y = w (a - b), sum w a b, y *= w
+int launch_wdiff_sumsq(const float* a, long long ap, const float* b, long long bp, const float* w, long long wp,
+                       long long len, int nprob, double* partials, int stride, const int* active, cudaStream_t s);
+int launch_wdiff_sumsq(const bf16* a, long long ap, const bf16* b, long long bp, const float* w, long long wp,
+                       long long len, int nprob, double* partials, int stride, const int* active, cudaStream_t s);
+int launch_wdiff(float* y, long long yp, const float* a, long long ap, const float* b, long long bp, const float* w,
+                 long long wp, long long len, int nprob, const int* active, cudaStream_t s);
+int launch_wdiff(float* y, long long yp, const bf16* a, long long ap, const bf16* b, long long bp, const float* w,
+                 long long wp, long long len, int nprob, const int* active, cudaStream_t s);
+int launch_wdot(const float* a, long long ap, const float* b, long long bp, const float* w, long long wp, long long len,
+                int nprob, double* partials, int stride, const int* active, cudaStream_t s);
+int launch_mulw(float* y, long long yp, const float* w, long long wp, long long len, int nprob, const int* active,
+                cudaStream_t s);
+
 }  // namespace cb

@@ -131,7 +131,7 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 Solver::~Solver() {
   prof_clear();
   if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
-  void* ptrs[] = {mR, mT, m, mR16, mT16, m16, v, vtrial, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
+  void* ptrs[] = {mR, mT, m, mR16, mT16, m16, wmask, v, vtrial, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
                   r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -406,22 +406,59 @@ int Solver::state_out(float* m1, long long m1p, const int* act) {
   return 0;
 }
 
-int Solver::image_diff_sumsq(bool template_image, const int* act) {
+int Solver::image_diff_sumsq(bool template_image, const int* act, bool weighted) {
   const long long PM = (nt + 1) * n;
+  const bool w = weighted && wmask;
   if (img16) {
     const bf16* b = template_image ? mT16 : m16 + nt * n;
-    CB_TRY(launch_diff_sumsq16(mR16, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
+    if (w) CB_TRY(launch_wdiff_sumsq(mR16, n, b, template_image ? n : PM, wmask, n, n, B, partials, maxparts, act, stream));
+    else CB_TRY(launch_diff_sumsq16(mR16, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
   } else {
     const float* b = template_image ? mT : m + nt * n;
-    CB_TRY(launch_diff_sumsq(mR, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
+    if (w) CB_TRY(launch_wdiff_sumsq(mR, n, b, template_image ? n : PM, wmask, n, n, B, partials, maxparts, act, stream));
+    else CB_TRY(launch_diff_sumsq(mR, n, b, template_image ? n : PM, n, B, partials, maxparts, act, stream));
   }
   note_launches(1);
   return 0;
 }
 
+int Solver::wdot(const float* a, long long ap, const float* b, long long bp, int s, const int* act) {
+  if (!wmask) return dot(a, ap, b, bp, n, s, act);
+  CB_TRY(launch_wdot(a, ap, b, bp, wmask, n, n, B, partials, maxparts, act, stream));
+  CB_TRY(launch_finalize(partials, maxparts, dot_partials(n), slot(s), B, 1.0, false, stream, act));
+  note_launches(2);
+  return 0;
+}
+
+int Solver::set_mask(int b, const float* w) {
+  if (b < 0 || b >= B) return CB_ERR_ARG;
+  if (!wmask) {
+    if (!w) return 0;  // no mask anywhere: nothing to do
+    CB_TRY(alloc((void**)&wmask, sizeof(float) * n * B));
+    CB_TRY(launch_fill(wmask, n, 1.f, n, B, nullptr, stream));
+  }
+  if (w) {
+    if (cudaMemcpyAsync(wmask + b * n, w, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+  } else {
+    CB_TRY(launch_fill(wmask + b * n, 0, 1.f, n, 1, nullptr, stream));
+  }
+  images_changed(b);
+  // the recorded PCG iteration may lack the weighting: record it again
+  if (pcg_exec) {
+    cudaGraphExecDestroy(pcg_exec);
+    pcg_exec = nullptr;
+  }
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
 int Solver::image_residual(float* y, long long yp, const int* act) {
   const long long PM = (nt + 1) * n;
-  if (img16) CB_TRY(launch_diff16(y, yp, mR16, n, m16 + nt * n, PM, n, B, act, stream));
+  if (wmask) {
+    // DistanceMeasureSL2::SetFinalConditionAE with a mask: w (mR - m1)
+    if (img16) CB_TRY(launch_wdiff(y, yp, mR16, n, m16 + nt * n, PM, wmask, n, n, B, act, stream));
+    else CB_TRY(launch_wdiff(y, yp, mR, n, m + nt * n, PM, wmask, n, n, B, act, stream));
+  } else if (img16) CB_TRY(launch_diff16(y, yp, mR16, n, m16 + nt * n, PM, n, B, act, stream));
   else CB_TRY(launch_lincomb(y, yp, mR, n, nullptr, 1.0, m + nt * n, PM, nullptr, -1.0, n, B, act, stream));
   note_launches(1);
   return 0;
@@ -512,14 +549,14 @@ int Solver::distance(const std::vector<int>& sel, const int* act) {
     const long long PM = (nt + 1) * n;
     CB_TRY(ncc_setup_scale(sel));
     const float* m1 = m + nt * n;
-    CB_TRY(dot(m1, PM, m1, PM, n, S_NA, act));
-    CB_TRY(dot(mR, n, mR, n, n, S_NRR, act));
-    CB_TRY(dot(m1, PM, mR, n, n, S_NI, act));
+    CB_TRY(wdot(m1, PM, m1, PM, S_NA, act));
+    CB_TRY(wdot(mR, n, mR, n, S_NRR, act));
+    CB_TRY(wdot(m1, PM, mR, n, S_NI, act));
     k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 1, (double)hd);
     note_launches(1);
     return (int)cudaGetLastError();
   }
-  CB_TRY(image_diff_sumsq(false, act));
+  CB_TRY(image_diff_sumsq(false, act, true));
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_D), B, 0.5 * (double)hd, false, stream, act));
   note_launches(1);
   return 0;
@@ -536,10 +573,11 @@ int Solver::ncc_setup_scale(const std::vector<int>& sel) {
   if (!any) return 0;
   int* m3 = dact + 2 * B;
   CB_TRY(upload_mask(need, m3));
-  CB_TRY(dot(mT, n, mT, n, n, S_NA, m3));
-  CB_TRY(dot(mR, n, mR, n, n, S_NRR, m3));
-  CB_TRY(dot(mT, n, mR, n, n, S_NI, m3));
-  CB_TRY(launch_diff_sumsq(mT, n, mR, n, n, B, partials, maxparts, m3, stream));
+  CB_TRY(wdot(mT, n, mT, n, S_NA, m3));
+  CB_TRY(wdot(mR, n, mR, n, S_NRR, m3));
+  CB_TRY(wdot(mT, n, mR, n, S_NI, m3));
+  if (wmask) CB_TRY(launch_wdiff_sumsq(mT, n, mR, n, wmask, n, n, B, partials, maxparts, m3, stream));
+  else CB_TRY(launch_diff_sumsq(mT, n, mR, n, n, B, partials, maxparts, m3, stream));
   CB_TRY(launch_finalize(partials, maxparts, dot_partials(n), slot(S_NL2), B, 1.0, false, stream, m3));
   k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, m3, B, 0, (double)hd);
   note_launches(3);
@@ -552,13 +590,14 @@ int Solver::ncc_setup_scale(const std::vector<int>& sel) {
 int Solver::ncc_final_condition(float* lam, long long lp, const int* act) {
   const long long PM = (nt + 1) * n;
   const float* m1 = m + nt * n;
-  CB_TRY(dot(m1, PM, m1, PM, n, S_NA, act));
-  CB_TRY(dot(mR, n, mR, n, n, S_NRR, act));
-  CB_TRY(dot(m1, PM, mR, n, n, S_NI, act));
+  CB_TRY(wdot(m1, PM, m1, PM, S_NA, act));
+  CB_TRY(wdot(mR, n, mR, n, S_NRR, act));
+  CB_TRY(wdot(m1, PM, mR, n, S_NI, act));
   k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 2, (double)hd);
   CB_TRY((int)cudaGetLastError());
   CB_TRY(launch_lincomb(lam, lp, mR, n, slot(S_CA), 1.0, m1, PM, slot(S_CB), 1.0, n, B, act, stream));
-  note_launches(2);
+  if (wmask) CB_TRY(launch_mulw(lam, lp, wmask, n, n, B, act, stream));
+  note_launches(3);
   return 0;
 }
 
@@ -567,13 +606,14 @@ int Solver::ncc_final_condition(float* lam, long long lp, const int* act) {
 int Solver::ncc_inc_final_condition(float* lam, long long lp, const int* act) {
   const long long PM = (nt + 1) * n;
   const float* m1 = m + nt * n;
-  CB_TRY(dot(m1, PM, lam, lp, n, S_NIM, act));
-  CB_TRY(dot(mR, n, lam, lp, n, S_NRM, act));
+  CB_TRY(wdot(m1, PM, lam, lp, S_NIM, act));
+  CB_TRY(wdot(mR, n, lam, lp, S_NRM, act));
   k_ncc<<<pgrid(B), 128, 0, stream>>>(dsc, act, B, 3, (double)hd);
   CB_TRY((int)cudaGetLastError());
   CB_TRY(launch_lincomb(lam, lp, lam, lp, slot(S_CC), 1.0, mR, n, slot(S_CA), 1.0, n, B, act, stream));
   CB_TRY(launch_lincomb(lam, lp, lam, lp, nullptr, 1.0, m1, PM, slot(S_CB), 1.0, n, B, act, stream));
-  note_launches(3);
+  if (wmask) CB_TRY(launch_mulw(lam, lp, wmask, n, n, B, act, stream));
+  note_launches(4);
   return 0;
 }
 
@@ -831,6 +871,8 @@ int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) 
   }
   note_launches(nt - 1);
   if (ncc) CB_TRY(ncc_inc_final_condition(lam_end, PL, act));
+  // DistanceMeasureSL2::SetFinalConditionIAE with a mask: -w m~(1)
+  else if (wmask) CB_TRY(launch_mulw(lam_end, PL, wmask, n, n, B, act, stream));
   CB_TRY(finish_with_reg(vin, hout, act, pq_slot >= 0 ? vin : nullptr, pq_slot));
   return 0;
 }

@@ -58,6 +58,9 @@ class Solver {
   // images of problem b from device arrays (n floats each), converted to the
   // storage type; not synchronised
   int load_images(int b, const float* mRd, const float* mTd);
+  // SetMask (src/CLAIREInterface.cpp:277-286): weights w (device, n floats) of
+  // problem b's distance, or none (w = null: weight 1)
+  int set_mask(int b, const float* w);
   int set_problem(int b, const claire_b200_opts& o);
   long long footprint() const { return bytes_; }
 
@@ -83,6 +86,8 @@ class Solver {
   // bf16-image mode (opts.bf16_images): mR, mT and the state levels live in
   // these arrays instead (same layout); mR / mT / m above stay null.
   bool img16 = false;
+  // distance weights (n per problem), allocated by the first set_mask
+  float* wmask = nullptr;
   bf16 *mR16 = nullptr, *mT16 = nullptr, *m16 = nullptr;
   float2* spec = nullptr;
   double* partials = nullptr;
@@ -148,7 +153,9 @@ class Solver {
   int state_init(const float* m0, const int* act);  // m^0 = m0 (device, stride n), or mT if null
   int state_steps(const int* act);                  // m^{j+1} = m^j(X_state), j < nt
   int state_out(float* m1, long long m1p, const int* act);  // m1 = m^nt (FP32)
-  int image_diff_sumsq(bool template_image, const int* act);  // partials of (mR - m^nt or mT)^2
+  // partials of (mR - m^nt or mT)^2, mask-weighted when `weighted` and a mask is set
+  int image_diff_sumsq(bool template_image, const int* act, bool weighted = false);
+  int wdot(const float* a, long long ap, const float* b, long long bp, int slot, const int* act);  // mask-weighted dot
   int image_residual(float* y, long long yp, const int* act);  // y = mR - m^nt
   int image_grad(const int* act);                              // gm = grad m^j, j <= nt
   int state_solve(const float* vel, const int* act);

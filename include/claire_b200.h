@@ -106,6 +106,10 @@ long long claire_b200_estimate_bytes(const claire_b200_opts* opts, int nbatch);
 int claire_b200_set_problem_opts(claire_b200_ctx* ctx, int b, const claire_b200_opts* opts);
 /* SetReferenceImage / SetTemplateImage (src/CLAIREInterface.cpp:594-660). */
 int claire_b200_set_images(claire_b200_ctx* ctx, int b, const float* mR, const float* mT, int on_device);
+/* SetMask (src/CLAIREInterface.cpp:277-286): weights w (n floats, host or
+ * device) of problem b's distance measure (DistanceMeasureSL2 / NCC with a
+ * mask: weighted sums and final conditions); w = NULL removes the mask. */
+int claire_b200_set_mask(claire_b200_ctx* ctx, int b, const float* w, int on_device);
 /* SetInitialGuess (src/CLAIREInterface.cpp: copy semantics). */
 int claire_b200_set_velocity(claire_b200_ctx* ctx, int b, const float* v, int on_device);
 int claire_b200_get_velocity(const claire_b200_ctx* ctx, int b, float* v, int on_device);

@@ -432,7 +432,7 @@ class Problem:
     """
 
     def __init__(self, mR, mT, nt: int, reg: Regularization, dtype=np.float64,
-                 projection: Optional[str] = None, image_store=None, distance: str = "sl2"):
+                 projection: Optional[str] = None, image_store=None, distance: str = "sl2", mask=None):
         # image_store: rounding applied to every stored image value (mR, mT
         # and each state level), e.g. bf16_round; None keeps dtype values
         self.dtype = dtype
@@ -444,6 +444,8 @@ class Problem:
         self.mT = np.asarray(mT, dtype=dtype)
         self.shape = self.mR.shape
         self.distance_type = distance
+        # SetMask weights of the distance measure (None: weight 1)
+        self.mask = None if mask is None else np.asarray(mask, np.float64)
         if distance not in ("sl2", "ncc"):
             raise ValueError(distance)
         self.nt = nt
@@ -513,14 +515,16 @@ class Problem:
         scale = (1/2 hd sum (mT - mR)^2) / (1/2 - 1/2 <mT,mR>^2 / (|mT|^2 |mR|^2))."""
         mT = self.mT.astype(np.float64).ravel()
         mR = self.mR.astype(np.float64).ravel()
-        l2 = 0.5 * self.hd * float(np.sum((mT - mR) ** 2))
-        ncc = 0.5 - 0.5 * float(np.dot(mT, mR)) ** 2 / (float(np.dot(mT, mT)) * float(np.dot(mR, mR)))
+        w = np.ones_like(mT) if self.mask is None else self.mask.ravel()
+        l2 = 0.5 * self.hd * float(np.sum(w * (mT - mR) ** 2))
+        ncc = 0.5 - 0.5 * float(np.sum(w * mT * mR)) ** 2 / (float(np.sum(w * mT * mT)) * float(np.sum(w * mR * mR)))
         return l2 / ncc
 
     def _ncc_sums(self):
         m1 = self.solve_state()[self.nt].astype(np.float64).ravel()
         mR = self.mR.astype(np.float64).ravel()
-        return m1, mR, float(np.dot(m1, m1)), float(np.dot(mR, mR)), float(np.dot(m1, mR))
+        w = np.ones_like(m1) if self.mask is None else self.mask.ravel()
+        return m1, mR, float(np.sum(w * m1 * m1)), float(np.sum(w * mR * mR)), float(np.sum(w * m1 * mR))
 
     def final_condition(self) -> np.ndarray:
         """Adjoint final condition lambda(1): mR - m1 for SL2
@@ -528,13 +532,14 @@ class Problem:
         c1 mR - c2 m1, c1 = s I / (hd A R), c2 = s I^2 / (hd A^2 R), with
         A = <m1,m1>, R = <mR,mR>, I = <m1,mR> (src/DistanceMeasureNCC.cpp:251-366)."""
         m = self.solve_state()
+        w = 1.0 if self.mask is None else self.mask
         if self.distance_type == "sl2":
-            return (self.mR - m[self.nt]).astype(self.dtype)
+            return (w * (self.mR - m[self.nt])).astype(self.dtype)
         m1, mR, A, Rr, I = self._ncc_sums()
         s, hd = self.ncc_scale, self.hd
         c1 = s * I / (hd * A * Rr)
         c2 = s * I * I / (hd * A * A * Rr)
-        return (c1 * mR - c2 * m1).reshape(self.shape).astype(self.dtype)
+        return (w * (c1 * mR - c2 * m1).reshape(self.shape)).astype(self.dtype)
 
     def inc_final_condition(self, mt1) -> np.ndarray:
         """Incremental adjoint final condition: -m~(1) for SL2
@@ -543,11 +548,13 @@ class Problem:
         (c1 - c2) mR + (c3 - c4) m1 - c5 m~ with c1 = s<mR,m~>/(hd A R),
         c2 = 2 s I <m1,m~>/(hd A^2 R), c3 = 4 s I^2 <m1,m~>/(hd A^3 R),
         c4 = 2 s I <mR,m~>/(hd A^2 R), c5 = s I^2/(hd A^2 R)."""
+        w = 1.0 if self.mask is None else self.mask
         if self.distance_type == "sl2":
-            return (-mt1).astype(self.dtype)
+            return (-w * mt1).astype(self.dtype)
         m1, mR, A, Rr, I = self._ncc_sums()
         mt = np.asarray(mt1, np.float64).ravel()
-        IM, RM = float(np.dot(m1, mt)), float(np.dot(mR, mt))
+        wf = np.ones_like(mt) if self.mask is None else self.mask.ravel()
+        IM, RM = float(np.sum(wf * m1 * mt)), float(np.sum(wf * mR * mt))
         s, hd = self.ncc_scale, self.hd
         c1 = s * RM / (hd * A * Rr)
         c2 = 2.0 * s * I * IM / (hd * A * A * Rr)
@@ -555,7 +562,7 @@ class Problem:
         c4 = 2.0 * s * I * RM / (hd * A * A * Rr)
         c5 = s * I * I / (hd * A * A * Rr)
         out = (c1 - c2) * mR + (c3 - c4) * m1 - c5 * mt
-        return out.reshape(self.shape).astype(self.dtype)
+        return (w * out.reshape(self.shape)).astype(self.dtype)
 
     # --- objective (src/CLAIRE.cpp:793-863) --------------------------------
     def distance(self) -> float:
@@ -567,7 +574,8 @@ class Problem:
             _, _, A, Rr, I = self._ncc_sums()
             return self.ncc_scale * (0.5 - 0.5 * I * I / (A * Rr))
         dr = self.mR.astype(np.float64) - m[self.nt].astype(np.float64)
-        return 0.5 * self.hd * float(np.sum(dr * dr))
+        w = 1.0 if self.mask is None else self.mask
+        return 0.5 * self.hd * float(np.sum(w * dr * dr))
 
     def div_penalty(self, v) -> float:
         """CLAIREDivReg::EvaluteRegularizationDIV (src/CLAIREDivReg.cpp:165-245):

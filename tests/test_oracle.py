@@ -300,3 +300,24 @@ def test_initialization_uses_zero_velocity_for_g0():
     g = prob.gradient(np.zeros_like(vs))
     res = R.gauss_newton(prob, R.GNOptions(maxit=1, gttol=1e-2), v0=0.2 * vs)
     assert abs(res["g0"] - np.sqrt(R.dot(g, g))) <= 1e-12 * res["g0"]
+
+
+@pytest.mark.parametrize("distance", ["sl2", "ncc"])
+def test_masked_distance_taylor_gradient_and_unit_mask(distance):
+    # src/DistanceMeasureSL2.cpp / DistanceMeasureNCC.cpp with m_Mask: weighted
+    # sums and final conditions; the gradient stays consistent with J
+    n, nt = 16, 4
+    mR, mT, vs = R.synthetic_c1(n, np.float64, nt)
+    x1, x2, x3 = R.grid_coords((n, n, n))
+    w = 0.5 + 0.5 * np.cos(x1) ** 2
+    reg = R.Regularization("h1s", 1e-2)
+    prob = R.Problem(mR, mT, nt, reg, distance=distance, mask=w)
+    v = 0.3 * vs
+    J0 = prob.objective(v)
+    gw = R.dot(prob.gradient(v), vs)
+    h = 1e-4
+    fd = (prob.objective(v + h * vs) - J0) / h
+    assert abs(fd - gw) < 1e-2 * abs(gw)
+    ones = R.Problem(mR, mT, nt, reg, distance=distance, mask=np.ones((n, n, n)))
+    plain = R.Problem(mR, mT, nt, reg, distance=distance)
+    assert abs(ones.objective(v) - plain.objective(v)) <= 1e-12 * abs(plain.objective(v))
