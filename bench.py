@@ -540,6 +540,7 @@ def run_serve(a, rank, world, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    tuned = None if a.no_autotune else tune(cb, list(EDGES), a.slots)
     reqs = serve_requests(a, rank)
     for r in reqs:  # inputs are built before the timed run (setup, not served work)
         mR, mT, _ = synthetic.ellipsoid_problem(r["n"], r["nt"], 5, r["idx"], dev)
@@ -592,6 +593,7 @@ def run_serve(a, rank, world, local):
                        "max": float(ls[-1])},
         "timing": "wall clock from the first arrival to the last result (host-to-host, includes queueing)",
         "mean_gn_iterations": float(np.mean([s["gn_iterations"] for s in stats])),
+        "fft_variants": tuned or "defaults (--no-autotune)",
     }
     print(json.dumps(line), flush=True)
 
