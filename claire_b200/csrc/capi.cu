@@ -357,6 +357,10 @@ int run_scalecont(Solver& s, const std::vector<int>& sel) {
 // finest level when it is under 0.01, the Krylov reference norm of the first
 // solve kept.  The finest level is the context's own solver.
 int run_gridcont(Solver& s, const std::vector<int>& sel) {
+  if (s.d.n1 != s.d.n2 || s.d.n2 != s.d.n3) {
+    s.err = "grid continuation needs a cubic grid";
+    return CB_ERR_UNSUPPORTED;
+  }
   if (s.img16) {
     s.err = "grid continuation needs FP32 images";
     return CB_ERR_UNSUPPORTED;
@@ -615,7 +619,7 @@ static bool dims_ok(const int nx[3]) {
   return nx && nx[0] > 0 && nx[1] > 0 && nx[2] > 0;
 }
 static bool fft_ok(const int nx[3]) {
-  return nx[0] == nx[1] && nx[1] == nx[2] && fft_size_supported(nx[0]);
+  return fft_size_supported(nx[0]) && fft_size_supported(nx[1]) && fft_size_supported(nx[2]);
 }
 
 int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt, int flag, void* stream) {

@@ -866,13 +866,16 @@ static int pencil_impl(float2* spec, long long sp, long long fstr, int nprob, co
   return (int)cudaGetLastError();
 }
 
-static bool cubic_supported(const Dims& d) {
-  return d.n1 == d.n2 && d.n2 == d.n3 && fft_size_supported(d.n1);
+// Every axis has its own transform (rows: x3, columns: x2, pencils: x1), so
+// grids need not be cubic; each axis length must have a plan.
+static bool axes_supported(const Dims& d) {
+  return fft_size_supported(d.n1) && fft_size_supported(d.n2) && fft_size_supported(d.n3);
 }
+static bool cubic_supported(const Dims& d) { return d.n1 == d.n2 && d.n2 == d.n3 && axes_supported(d); }
 
 int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, long long sp, int nf,
                  int nprob, const Dims& d, const int* active, cudaStream_t s) {
-  if (!cubic_supported(d) || !aligned16(in) || ((ip | ifs) & 3)) return (int)cudaErrorInvalidValue;
+  if (!axes_supported(d) || !aligned16(in) || ((ip | ifs) & 3)) return (int)cudaErrorInvalidValue;
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
@@ -886,7 +889,7 @@ int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, lon
 
 int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
                   const SpecParams* dparams, int nin, int nout, const int* active, cudaStream_t s) {
-  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (!axes_supported(d)) return (int)cudaErrorInvalidValue;
   int e = 0;
   CB_DISPATCH_NV(d.n1, e = (pencil_impl<NN, VV>(spec, sp, d.nc(), nprob, d, op, dparams, nin, nout, active, s)));
   return e;
@@ -939,7 +942,7 @@ int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long lon
                  int nprob, const Dims& d, int epi, const float* alpha, double* partials, int nparts,
                  const int* active, cudaStream_t s, const float* other) {
   if ((epi == EPI_STORE_DOT || epi == EPI_ADD_DOT) && !other) return (int)cudaErrorInvalidValue;
-  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (!axes_supported(d)) return (int)cudaErrorInvalidValue;
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
@@ -1000,7 +1003,7 @@ int deriv_partials(const Dims& d, int axis, int nf, bool any_variant) {
 int launch_deriv(const float* in, long long ip, long long ifs, float* out, long long op_,
                  long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
                  double* partials, int nparts, const int* active, cudaStream_t s) {
-  if (!cubic_supported(d)) return (int)cudaErrorInvalidValue;
+  if (!axes_supported(d)) return (int)cudaErrorInvalidValue;
   if (axis == 2 && (!aligned16(in) || ((ip | ifs) & 3))) return (int)cudaErrorInvalidValue;
   const int n = (axis == 0) ? d.n1 : (axis == 1 ? d.n2 : d.n3);
   int e = 0;

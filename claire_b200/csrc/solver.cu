@@ -187,8 +187,8 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     err = "invalid batch size or nt";
     return CB_ERR_ARG;
   }
-  if (!(d.n1 == d.n2 && d.n2 == d.n3 && fft_size_supported(d.n1))) {
-    err = "grid size has no FFT plan (supported: cubic 16,32,48,64,96,128,192,256)";
+  if (!(fft_size_supported(d.n1) && fft_size_supported(d.n2) && fft_size_supported(d.n3))) {
+    err = "grid size has no FFT plan (each axis one of 16,32,48,64,96,128,192,256)";
     return CB_ERR_UNSUPPORTED;
   }
   n = d.n();
@@ -207,10 +207,12 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     return CB_ERR_CUDA;
   }
   stream = own_stream;
-  if (o.autotune && !fft_tuned(d.n1) && fft_autotune_once(d.n1, B, stream)) {
-    err = "FFT autotuning failed";
-    return CB_ERR_CUDA;
-  }
+  if (o.autotune)
+    for (int axis_n : {d.n1, d.n2, d.n3})
+      if (!fft_tuned(axis_n) && fft_autotune_once(axis_n, B, stream)) {
+        err = "FFT autotuning failed";
+        return CB_ERR_CUDA;
+      }
   const size_t S = sizeof(float) * n * B, V = 3 * S;
   img16 = o.bf16_images != 0;
   ncc = o.distance == CB_DIST_NCC;
