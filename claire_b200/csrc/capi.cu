@@ -619,7 +619,7 @@ static bool dims_ok(const int nx[3]) {
   return nx && nx[0] > 0 && nx[1] > 0 && nx[2] > 0;
 }
 static bool fft_ok(const int nx[3]) {
-  return fft_size_supported(nx[0]) && fft_size_supported(nx[1]) && fft_size_supported(nx[2]);
+  return fft_col_size_supported(nx[0]) && fft_col_size_supported(nx[1]) && fft_size_supported(nx[2]);
 }
 
 int claire_b200_trajectory(const float* v, float* disp, const int nx[3], int nt, int flag, void* stream) {
@@ -662,7 +662,7 @@ int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigne
 }
 
 int claire_b200_autotune(int n, int nbatch, void* stream, int* variant, float* ms) {
-  if (!fft_size_supported(n) || nbatch < 1) return CB_ERR_ARG;
+  if (!fft_col_size_supported(n) || nbatch < 1) return CB_ERR_ARG;
   float t[4] = {-1.f, -1.f, -1.f, -1.f};
   int best = 0;
   const int e = fft_autotune(n, nbatch, (cudaStream_t)stream, &best, t);
@@ -673,10 +673,10 @@ int claire_b200_autotune(int n, int nbatch, void* stream, int* variant, float* m
   return CB_OK;
 }
 
-int claire_b200_fft_variant(int n) { return fft_size_supported(n) ? fft_variant(n) : -1; }
+int claire_b200_fft_variant(int n) { return fft_col_size_supported(n) ? fft_variant(n) : -1; }
 
 int claire_b200_set_fft_variant(int n, int variant) {
-  if (!fft_size_supported(n)) return CB_ERR_ARG;
+  if (!fft_col_size_supported(n)) return CB_ERR_ARG;
   return set_fft_variant(n, variant) ? CB_ERR_ARG : CB_OK;
 }
 

@@ -55,12 +55,18 @@ static const float2* twiddles(int n) {
   return d;
 }
 
+// Lengths with a plan on every axis, and the extra lengths the column and
+// pencil passes (axes x1, x2) also take: 150 = 10 x 15 (the x2 length of the
+// reference's example brains, 128 x 150 x 128).  Row passes need N % 16 == 0
+// (16-byte row loads, whole float4 per thread).
 bool fft_size_supported(int n) {
   switch (n) {
     case 16: case 32: case 48: case 64: case 96: case 128: case 192: case 256: return true;
     default: return false;
   }
 }
+
+bool fft_col_size_supported(int n) { return fft_size_supported(n) || n == 150; }
 
 // Packed lines per CTA for row kernels, and columns per CTA for column kernels.
 // With 256 threads and at least 32 lines a warp's lanes are 32 consecutive
@@ -139,17 +145,28 @@ CB_DEVICE bool epi_reduces(int epi) { return epi == EPI_SUMSQ || epi == EPI_STOR
 // Column tile: N elements (es apart) of the thread's column into split
 // re/im shared arrays.  The thread owns column c = tid % C and rows
 // e = tid / C + k * (kThreads / C).  colp == nullptr loads zeros.
+// Lengths that RSTEP does not divide (150) take K = ceil(N / RSTEP) steps and
+// skip the elements e >= N; for the others the test is compile-time true.
+template <int N, int RSTEP>
+CB_DEVICE bool in_line(int e) {
+  return (N % RSTEP == 0) || e < N;
+}
+
 template <int N, int C, int PITCH>
 CB_DEVICE void load_col_tile(float* re, float* im, const float2* __restrict__ colp, long long es) {
   constexpr int RSTEP = kThreads / C;
-  constexpr int K = N / RSTEP;
+  constexpr int K = (N + RSTEP - 1) / RSTEP;
   const int c = threadIdx.x % C, e0 = threadIdx.x / C;
   float2 v[K];
 #pragma unroll
-  for (int k = 0; k < K; ++k) v[k] = colp ? __ldg(colp + (long long)(e0 + k * RSTEP) * es) : make_float2(0.f, 0.f);
+  for (int k = 0; k < K; ++k) {
+    const int e = e0 + k * RSTEP;
+    v[k] = (colp && in_line<N, RSTEP>(e)) ? __ldg(colp + (long long)e * es) : make_float2(0.f, 0.f);
+  }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
+    if (!in_line<N, RSTEP>(e)) continue;
     re[e * PITCH + c] = v[k].x;
     im[e * PITCH + c] = v[k].y;
   }
@@ -158,13 +175,14 @@ CB_DEVICE void load_col_tile(float* re, float* im, const float2* __restrict__ co
 template <int N, int C, int PITCH>
 CB_DEVICE void store_col_tile(const float* re, const float* im, float2* __restrict__ colp, long long es) {
   constexpr int RSTEP = kThreads / C;
-  constexpr int K = N / RSTEP;
+  constexpr int K = (N + RSTEP - 1) / RSTEP;
   const int c = threadIdx.x % C, e0 = threadIdx.x / C;
   if (!colp) return;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
-    colp[(long long)(e0 + k * RSTEP) * es] = make_float2(re[e * PITCH + c], im[e * PITCH + c]);
+    if (!in_line<N, RSTEP>(e)) continue;
+    colp[(long long)e * es] = make_float2(re[e * PITCH + c], im[e * PITCH + c]);
   }
 }
 
@@ -485,7 +503,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
                                                        const float2* __restrict__ twg,
                                                        const int* __restrict__ active) {
   constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
-  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
+  constexpr int RSTEP = kThreads / C, K = (N + RSTEP - 1) / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -510,6 +528,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
+    if (!in_line<N, RSTEP>(e)) continue;
     const int a = e * PITCH + c;
     const float2 y = apply_op1(op, q, d, e, ck, blockIdx.y, make_float2(re[a], im[a]), s);
     re[a] = y.x;
@@ -527,7 +546,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
                                                        const float2* __restrict__ twg,
                                                        const int* __restrict__ active) {
   constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
-  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
+  constexpr int RSTEP = kThreads / C, K = (N + RSTEP - 1) / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -557,6 +576,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
+    if (!in_line<N, RSTEP>(e)) continue;
     const int a = e * PITCH + c;
     float2 x[3];
 #pragma unroll
@@ -635,7 +655,7 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   constexpr int L = ColCfg<N, V>::C;       // packed complex lines per CTA
   constexpr int C = 2 * L;              // real columns per CTA
   constexpr int PITCH = ColCfg<N, V>::PITCH;
-  constexpr int RSTEP = kThreads / C, K = N / RSTEP;
+  constexpr int RSTEP = kThreads / C, K = (N + RSTEP - 1) / RSTEP;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -654,9 +674,15 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   {
     float v[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = ok ? __ldg(src + cbase + (long long)(e0 + k * RSTEP) * es) : 0.f;
+    for (int k = 0; k < K; ++k) {
+      const int e = e0 + k * RSTEP;
+      v[k] = (ok && in_line<N, RSTEP>(e)) ? __ldg(src + cbase + (long long)e * es) : 0.f;
+    }
 #pragma unroll
-    for (int k = 0; k < K; ++k) lane[(e0 + k * RSTEP) * PITCH] = v[k];
+    for (int k = 0; k < K; ++k) {
+      const int e = e0 + k * RSTEP;
+      if (in_line<N, RSTEP>(e)) lane[e * PITCH] = v[k];
+    }
   }
   __syncthreads();
   fft_lines<N, false, L, PITCH, V>(re, im, sre, sim, tw);
@@ -667,10 +693,14 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   if (ok) {
     float old[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) old[k] = (epi == EPI_ADD) ? dst[cbase + (long long)(e0 + k * RSTEP) * es] : 0.f;
+    for (int k = 0; k < K; ++k) {
+      const int e = e0 + k * RSTEP;
+      old[k] = (epi == EPI_ADD && in_line<N, RSTEP>(e)) ? dst[cbase + (long long)e * es] : 0.f;
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int e = e0 + k * RSTEP;
+      if (!in_line<N, RSTEP>(e)) continue;
       const float val = lane[e * PITCH];
       const long long gi = cbase + (long long)e * es;
       if (epi == EPI_STORE) dst[gi] = val;
@@ -725,7 +755,7 @@ static bool aligned16(const void* p) { return (reinterpret_cast<unsigned long lo
 // change while no transform of that size is in flight (contexts tune when
 // they are created, before any of their work).
 // ---------------------------------------------------------------------------
-static std::atomic<int> g_fft_var[8];
+static std::atomic<int> g_fft_var[9];
 
 static int size_slot(int n) {
   switch (n) {
@@ -737,6 +767,7 @@ static int size_slot(int n) {
     case 128: return 5;
     case 192: return 6;
     case 256: return 7;
+    case 150: return 8;
     default: return -1;
   }
 }
@@ -747,6 +778,11 @@ int fft_variant_candidates(int n, int* out) {
   if (n == 16 || n == 256) {  // one factorization: line counts only
     out[0] = 0;
     out[1] = 2;
+    return 2;
+  }
+  if (n == 150) {  // column passes only, one line count: radix orders only
+    out[0] = 0;
+    out[1] = 1;
     return 2;
   }
   for (int v = 0; v < 4; ++v) out[v] = v;
@@ -786,6 +822,12 @@ int set_fft_variant(int n, int v) {
     switch (fft_variant(N_)) { CB_V(0, CALL) CB_V(2, CALL)                                 \
       default: return (int)cudaErrorInvalidValue; }                                        \
   } break;
+#define CB_VSW01(N_, CALL)                                                                 \
+  {                                                                                        \
+    constexpr int NN = N_;                                                                 \
+    switch (fft_variant(N_)) { CB_V(0, CALL) CB_V(1, CALL)                                 \
+      default: return (int)cudaErrorInvalidValue; }                                        \
+  } break;
 // CB_DISPATCH_N with the size's current variant as the constexpr VV
 #define CB_DISPATCH_NV(n, CALL)      \
   switch (n) {                       \
@@ -795,6 +837,20 @@ int set_fft_variant(int n, int v) {
     case 64: CB_VSW4(64, CALL)       \
     case 96: CB_VSW4(96, CALL)       \
     case 128: CB_VSW4(128, CALL)     \
+    case 192: CB_VSW4(192, CALL)     \
+    case 256: CB_VSW2(256, CALL)     \
+    default: return (int)cudaErrorInvalidValue; \
+  }
+// the same for column / pencil passes, which also take 150 points
+#define CB_DISPATCH_NV_COL(n, CALL)  \
+  switch (n) {                       \
+    case 16: CB_VSW2(16, CALL)       \
+    case 32: CB_VSW4(32, CALL)       \
+    case 48: CB_VSW4(48, CALL)       \
+    case 64: CB_VSW4(64, CALL)       \
+    case 96: CB_VSW4(96, CALL)       \
+    case 128: CB_VSW4(128, CALL)     \
+    case 150: CB_VSW01(150, CALL)    \
     case 192: CB_VSW4(192, CALL)     \
     case 256: CB_VSW2(256, CALL)     \
     default: return (int)cudaErrorInvalidValue; \
@@ -869,7 +925,7 @@ static int pencil_impl(float2* spec, long long sp, long long fstr, int nprob, co
 // Every axis has its own transform (rows: x3, columns: x2, pencils: x1), so
 // grids need not be cubic; each axis length must have a plan.
 static bool axes_supported(const Dims& d) {
-  return fft_size_supported(d.n1) && fft_size_supported(d.n2) && fft_size_supported(d.n3);
+  return fft_col_size_supported(d.n1) && fft_col_size_supported(d.n2) && fft_size_supported(d.n3);
 }
 static bool cubic_supported(const Dims& d) { return d.n1 == d.n2 && d.n2 == d.n3 && axes_supported(d); }
 
@@ -882,7 +938,7 @@ int launch_r2c3d(const float* in, long long ip, long long ifs, float2* spec, lon
   CB_DISPATCH_NV(d.n3, e = (r2c_rows_impl<NN, VV>(in, ip, ifs, spec, sp, nc, d.n1 * d.n2, nf, nprob, active, s)));
   if (e) return e;
   // x2 columns: column g = (i1, k3) starts at i1*n2*n3h + k3, stride n3h
-  CB_DISPATCH_NV(d.n2, e = (cols_impl<NN, false, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
+  CB_DISPATCH_NV_COL(d.n2, e = (cols_impl<NN, false, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
                                                 nf, nprob, active, s)));
   return e;
 }
@@ -891,7 +947,7 @@ int launch_pencil(float2* spec, long long sp, int nprob, const Dims& d, int op,
                   const SpecParams* dparams, int nin, int nout, const int* active, cudaStream_t s) {
   if (!axes_supported(d)) return (int)cudaErrorInvalidValue;
   int e = 0;
-  CB_DISPATCH_NV(d.n1, e = (pencil_impl<NN, VV>(spec, sp, d.nc(), nprob, d, op, dparams, nin, nout, active, s)));
+  CB_DISPATCH_NV_COL(d.n1, e = (pencil_impl<NN, VV>(spec, sp, d.nc(), nprob, d, op, dparams, nin, nout, active, s)));
   return e;
 }
 
@@ -925,6 +981,7 @@ static int col_lines(int n, bool min_over_variants = false) {
     case 128: base = ColLines<128>::base; alt = ColLines<128>::alt; break;
     case 192: base = ColLines<192>::base; alt = ColLines<192>::alt; break;
     case 256: base = ColLines<256>::base; alt = ColLines<256>::alt; break;
+    case 150: base = ColLines<150>::base; alt = ColLines<150>::alt; break;
     default: return 0;
   }
   if (min_over_variants) return base < alt ? base : alt;
@@ -946,7 +1003,7 @@ int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long lon
   const long long nc = d.nc();
   const int n3h = d.n3 / 2 + 1;
   int e = 0;
-  CB_DISPATCH_NV(d.n2, e = (cols_impl<NN, true, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
+  CB_DISPATCH_NV_COL(d.n2, e = (cols_impl<NN, true, VV>(spec, sp, nc, d.n1 * n3h, n3h, (long long)d.n2 * n3h, n3h,
                                                nf, nprob, active, s)));
   if (e) return e;
   CB_DISPATCH_NV(d.n3, e = (c2r_rows_impl<NN, VV>(spec, sp, nc, out, op_, ofs, d.n1 * d.n2, nf, nprob, epi, alpha,
@@ -955,35 +1012,40 @@ int launch_c2r3d(float2* spec, long long sp, float* out, long long op_, long lon
 }
 
 template <int N, int V>
-static int deriv_impl(const float* in, long long ip, long long ifs, float* out, long long op_,
-                      long long ofs, int nf, int nprob, const Dims& d, int axis, int epi,
-                      double* partials, int nparts, const int* active, cudaStream_t s) {
+static int deriv_rows_impl(const float* in, long long ip, long long ifs, float* out, long long op_, long long ofs,
+                           int nf, int nprob, const Dims& d, int epi, double* partials, int nparts,
+                           const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  if (axis == 2) {
-    size_t sm = row_smem<N, V>(false);
-    int e = set_smem(k_deriv_rows<N, V>, sm);
-    if (e) return e;
-    const int nrows = d.n1 * d.n2;
-    dim3 grid((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), nf, nprob);
-    k_deriv_rows<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, nrows, tw, epi, partials, nparts,
-                                                active);
-  } else {
-    size_t sm = col_smem<N, V>(2);
-    int e = set_smem(k_deriv_cols<N, V>, sm);
-    if (e) return e;
-    int ncols, cpg;
-    long long gs, es;
-    if (axis == 1) {  // lines along x2: column (i1, i3)
-      ncols = d.n1 * d.n3; cpg = d.n3; gs = (long long)d.n2 * d.n3; es = d.n3;
-    } else {          // lines along x1: column (i2, i3)
-      ncols = d.n2 * d.n3; cpg = ncols; gs = 0; es = (long long)d.n2 * d.n3;
-    }
-    constexpr int C = 2 * ColCfg<N, V>::C;
-    dim3 grid((ncols + C - 1) / C, nf, nprob);
-    k_deriv_cols<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, ncols, cpg, gs, es, tw, epi,
-                                                partials, nparts, active);
+  size_t sm = row_smem<N, V>(false);
+  int e = set_smem(k_deriv_rows<N, V>, sm);
+  if (e) return e;
+  const int nrows = d.n1 * d.n2;
+  dim3 grid((nrows + 2 * RowCfg<N, V>::P - 1) / (2 * RowCfg<N, V>::P), nf, nprob);
+  k_deriv_rows<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, nrows, tw, epi, partials, nparts, active);
+  return (int)cudaGetLastError();
+}
+
+template <int N, int V>
+static int deriv_cols_impl(const float* in, long long ip, long long ifs, float* out, long long op_, long long ofs,
+                           int nf, int nprob, const Dims& d, int axis, int epi, double* partials, int nparts,
+                           const int* active, cudaStream_t s) {
+  const float2* tw = twiddles(N);
+  if (!tw) return (int)cudaErrorMemoryAllocation;
+  size_t sm = col_smem<N, V>(2);
+  int e = set_smem(k_deriv_cols<N, V>, sm);
+  if (e) return e;
+  int ncols, cpg;
+  long long gs, es;
+  if (axis == 1) {  // lines along x2: column (i1, i3)
+    ncols = d.n1 * d.n3; cpg = d.n3; gs = (long long)d.n2 * d.n3; es = d.n3;
+  } else {          // lines along x1: column (i2, i3)
+    ncols = d.n2 * d.n3; cpg = ncols; gs = 0; es = (long long)d.n2 * d.n3;
   }
+  constexpr int C = 2 * ColCfg<N, V>::C;
+  dim3 grid((ncols + C - 1) / C, nf, nprob);
+  k_deriv_cols<N, V><<<grid, kThreads, sm, s>>>(in, ip, ifs, out, op_, ofs, ncols, cpg, gs, es, tw, epi, partials,
+                                                nparts, active);
   return (int)cudaGetLastError();
 }
 
@@ -1007,8 +1069,13 @@ int launch_deriv(const float* in, long long ip, long long ifs, float* out, long 
   if (axis == 2 && (!aligned16(in) || ((ip | ifs) & 3))) return (int)cudaErrorInvalidValue;
   const int n = (axis == 0) ? d.n1 : (axis == 1 ? d.n2 : d.n3);
   int e = 0;
-  CB_DISPATCH_NV(n, e = (deriv_impl<NN, VV>(in, ip, ifs, out, op_, ofs, nf, nprob, d, axis, epi, partials, nparts,
-                                      active, s)));
+  if (axis == 2) {
+    CB_DISPATCH_NV(n, e = (deriv_rows_impl<NN, VV>(in, ip, ifs, out, op_, ofs, nf, nprob, d, epi, partials, nparts,
+                                                   active, s)));
+  } else {
+    CB_DISPATCH_NV_COL(n, e = (deriv_cols_impl<NN, VV>(in, ip, ifs, out, op_, ofs, nf, nprob, d, axis, epi,
+                                                       partials, nparts, active, s)));
+  }
   return e;
 }
 
@@ -1060,7 +1127,7 @@ __global__ void k_tune_fill(float* x, long long len) {
     x[i] = __sinf(0.001f * (float)(i % 100003));
 }
 
-static std::atomic<bool> g_fft_tuned[8];
+static std::atomic<bool> g_fft_tuned[9];
 static std::mutex g_tune_mutex;
 
 bool fft_tuned(int n) {
@@ -1079,7 +1146,7 @@ int fft_autotune(int n, int nprob, cudaStream_t s, int* best, float* ms) {
   int cand[4];
   const int ncand = fft_variant_candidates(n, cand);
   if (!ncand || nprob < 1) return (int)cudaErrorInvalidValue;
-  const Dims d{n, n, n};
+  const Dims d{n, n, fft_size_supported(n) ? n : 64};  // 150: column / pencil passes only
   const long long nn = d.n(), nc = d.nc();
   float *in = nullptr, *out = nullptr;
   float2* spec = nullptr;

@@ -5,7 +5,7 @@
 // re[e*PITCH + p], im[e*PITCH + p] (line index fastest, PITCH odd so that
 // consecutive lines hit distinct banks).  Line count and pitch are
 // compile-time so every loop has a known trip count.  Every plan has exactly two radix
-// stages (N = R0*R1, R0, R1 in {4, 8, 12, 16}), each an in-register DFT
+// stages (N = R0*R1, R0, R1 in {4, 8, 10, 12, 15, 16}), each an in-register DFT
 // followed by one shared-memory exchange, so the result lands back in the
 // source buffer after one ping-pong through the scratch buffer.
 //
@@ -35,6 +35,71 @@ __device__ __constant__ float2 kTw12[12] = {
     {-1.000000000f, -0.000000000f}, {-0.866025404f, 0.500000000f}, {-0.500000000f, 0.866025404f},
     {-0.000000000f, 1.000000000f}, {0.500000000f, 0.866025404f}, {0.866025404f, 0.500000000f}};
 
+// exp(-2*pi*i*m/60), m = 0..59: the small twiddles of radices 5, 10, 15
+// (grids with a factor 5, such as 150 points).
+__device__ __constant__ float2 kTw60[60] = {
+    {1.000000000f, -0.000000000f},
+    {0.994521895f, -0.104528463f},
+    {0.978147601f, -0.207911691f},
+    {0.951056516f, -0.309016994f},
+    {0.913545458f, -0.406736643f},
+    {0.866025404f, -0.500000000f},
+    {0.809016994f, -0.587785252f},
+    {0.743144825f, -0.669130606f},
+    {0.669130606f, -0.743144825f},
+    {0.587785252f, -0.809016994f},
+    {0.500000000f, -0.866025404f},
+    {0.406736643f, -0.913545458f},
+    {0.309016994f, -0.951056516f},
+    {0.207911691f, -0.978147601f},
+    {0.104528463f, -0.994521895f},
+    {0.000000000f, -1.000000000f},
+    {-0.104528463f, -0.994521895f},
+    {-0.207911691f, -0.978147601f},
+    {-0.309016994f, -0.951056516f},
+    {-0.406736643f, -0.913545458f},
+    {-0.500000000f, -0.866025404f},
+    {-0.587785252f, -0.809016994f},
+    {-0.669130606f, -0.743144825f},
+    {-0.743144825f, -0.669130606f},
+    {-0.809016994f, -0.587785252f},
+    {-0.866025404f, -0.500000000f},
+    {-0.913545458f, -0.406736643f},
+    {-0.951056516f, -0.309016994f},
+    {-0.978147601f, -0.207911691f},
+    {-0.994521895f, -0.104528463f},
+    {-1.000000000f, -0.000000000f},
+    {-0.994521895f, 0.104528463f},
+    {-0.978147601f, 0.207911691f},
+    {-0.951056516f, 0.309016994f},
+    {-0.913545458f, 0.406736643f},
+    {-0.866025404f, 0.500000000f},
+    {-0.809016994f, 0.587785252f},
+    {-0.743144825f, 0.669130606f},
+    {-0.669130606f, 0.743144825f},
+    {-0.587785252f, 0.809016994f},
+    {-0.500000000f, 0.866025404f},
+    {-0.406736643f, 0.913545458f},
+    {-0.309016994f, 0.951056516f},
+    {-0.207911691f, 0.978147601f},
+    {-0.104528463f, 0.994521895f},
+    {-0.000000000f, 1.000000000f},
+    {0.104528463f, 0.994521895f},
+    {0.207911691f, 0.978147601f},
+    {0.309016994f, 0.951056516f},
+    {0.406736643f, 0.913545458f},
+    {0.500000000f, 0.866025404f},
+    {0.587785252f, 0.809016994f},
+    {0.669130606f, 0.743144825f},
+    {0.743144825f, 0.669130606f},
+    {0.809016994f, 0.587785252f},
+    {0.866025404f, 0.500000000f},
+    {0.913545458f, 0.406736643f},
+    {0.951056516f, 0.309016994f},
+    {0.978147601f, 0.207911691f},
+    {0.994521895f, 0.104528463f}
+};
+
 CB_DEVICE float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -42,12 +107,13 @@ CB_DEVICE float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + 
 CB_DEVICE float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 CB_DEVICE float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
-// W_R^m (forward) or its conjugate (inverse), R divides 16 or 12.
+// W_R^m (forward) or its conjugate (inverse), R divides 16, 12 or 60.
 template <int R, bool INV>
 CB_DEVICE float2 wsmall(int m) {
   float2 w;
   if (16 % R == 0) w = kTw16[(m * (16 / R)) % 16];
-  else w = kTw12[(m * (12 / R)) % 12];
+  else if (12 % R == 0) w = kTw12[(m * (12 / R)) % 12];
+  else w = kTw60[(m * (60 / R)) % 60];
   if (INV) w.y = -w.y;
   return w;
 }
@@ -57,6 +123,8 @@ template <> struct Factor<6> { static constexpr int A = 2, B = 3; };
 template <> struct Factor<8> { static constexpr int A = 2, B = 4; };
 template <> struct Factor<12> { static constexpr int A = 3, B = 4; };
 template <> struct Factor<16> { static constexpr int A = 4, B = 4; };
+template <> struct Factor<10> { static constexpr int A = 2, B = 5; };
+template <> struct Factor<15> { static constexpr int A = 3, B = 5; };
 
 template <int R, bool INV> struct Dft;
 
@@ -79,6 +147,30 @@ template <bool INV> struct Dft<3, INV> {
     v[0] = cadd(v[0], t);
     v[1] = cadd(a, r);
     v[2] = csub(a, r);
+  }
+};
+
+// Radix 5: with t1 = x1 + x4, t2 = x2 + x3, t3 = x1 - x4, t4 = x2 - x3,
+//   X1,4 = x0 + c1 t1 + c2 t2 -/+ i (s1 t3 + s2 t4)
+//   X2,3 = x0 + c2 t1 + c1 t2 -/+ i (s2 t3 - s1 t4)
+// c1 = cos(2 pi/5), c2 = cos(4 pi/5), s1 = sin(2 pi/5), s2 = sin(4 pi/5);
+// the inverse flips the sign of i.
+template <bool INV> struct Dft<5, INV> {
+  static CB_DEVICE void run(float2 (&v)[5]) {
+    const float c1 = 0.309016994f, c2 = -0.809016994f;
+    const float s1 = INV ? -0.951056516f : 0.951056516f, s2 = INV ? -0.587785252f : 0.587785252f;
+    const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    const float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    const float2 a1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+    const float2 a2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+    const float2 b1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+    const float2 b2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+    v[0] = cadd(v[0], cadd(t1, t2));
+    // -i b = (b.y, -b.x)
+    v[1] = make_float2(a1.x + b1.y, a1.y - b1.x);
+    v[4] = make_float2(a1.x - b1.y, a1.y + b1.x);
+    v[2] = make_float2(a2.x + b2.y, a2.y - b2.x);
+    v[3] = make_float2(a2.x - b2.y, a2.y + b2.x);
   }
 };
 
@@ -135,6 +227,7 @@ template <> struct Plan0<96> { static constexpr int R0 = 12, R1 = 8; };
 template <> struct Plan0<128> { static constexpr int R0 = 16, R1 = 8; };
 template <> struct Plan0<192> { static constexpr int R0 = 12, R1 = 16; };
 template <> struct Plan0<256> { static constexpr int R0 = 16, R1 = 16; };
+template <> struct Plan0<150> { static constexpr int R0 = 10, R1 = 15; };
 template <int N> struct Plan1;
 template <> struct Plan1<16> { static constexpr int R0 = 4, R1 = 4; };
 template <> struct Plan1<32> { static constexpr int R0 = 8, R1 = 4; };
@@ -144,6 +237,7 @@ template <> struct Plan1<96> { static constexpr int R0 = 8, R1 = 12; };
 template <> struct Plan1<128> { static constexpr int R0 = 8, R1 = 16; };
 template <> struct Plan1<192> { static constexpr int R0 = 16, R1 = 12; };
 template <> struct Plan1<256> { static constexpr int R0 = 16, R1 = 16; };
+template <> struct Plan1<150> { static constexpr int R0 = 15, R1 = 10; };
 template <int N, int V = 0> struct Plan {
   static constexpr int R0 = (V & 1) ? Plan1<N>::R0 : Plan0<N>::R0;
   static constexpr int R1 = (V & 1) ? Plan1<N>::R1 : Plan0<N>::R1;

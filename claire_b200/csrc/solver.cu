@@ -187,8 +187,8 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     err = "invalid batch size or nt";
     return CB_ERR_ARG;
   }
-  if (!(fft_size_supported(d.n1) && fft_size_supported(d.n2) && fft_size_supported(d.n3))) {
-    err = "grid size has no FFT plan (each axis one of 16,32,48,64,96,128,192,256)";
+  if (!(fft_col_size_supported(d.n1) && fft_col_size_supported(d.n2) && fft_size_supported(d.n3))) {
+    err = "grid size has no FFT plan (each axis one of 16,32,48,64,96,128,192,256; x1 and x2 also 150)";
     return CB_ERR_UNSUPPORTED;
   }
   n = d.n();

@@ -81,7 +81,8 @@ int fft_autotune(int n, int nprob, cudaStream_t s, int* best, float* ms);
 bool fft_tuned(int n);
 int fft_autotune_once(int n, int nprob, cudaStream_t s);
 
-bool fft_size_supported(int n);
+bool fft_size_supported(int n);      // every axis (rows need N % 16 == 0)
+bool fft_col_size_supported(int n);  // axes x1 and x2 (column / pencil passes): also 150
 
 // Spectral grid change (restriction / prolongation) of nf cubic fields, ns^3
 // (ip apart) -> nt^3 (op apart); work: grid_change_work(ns, nt, nf) floats.

@@ -29,18 +29,30 @@ def to_dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
 
 
-@pytest.mark.parametrize("shape", [(32, 48, 16), (64, 32, 128), (16, 96, 32)])
+@pytest.mark.parametrize("shape", [(32, 48, 16), (64, 32, 128), (16, 96, 32), (32, 150, 16), (150, 32, 64)])
 def test_spectral_ops_non_cubic(cb, shape):
+    # 150 points (x1 or x2 only): radix 10 x 15 plans, both radix orders
     rng = np.random.default_rng(sum(shape))
     f = rng.standard_normal(shape).astype(np.float32)
-    assert rel(cb.fft_grad(to_dev(f)).cpu().numpy(), R.grad(f.astype(np.float64))) < TOL
     v = rng.standard_normal((3,) + shape).astype(np.float32)
-    assert rel(cb.fft_div(to_dev(v)).cpu().numpy(), R.div(v.astype(np.float64))) < TOL
-    for norm in ("h1s", "h2"):
-        reg = R.Regularization(norm, 1e-2, 1e-4)
-        op = cb.Regularization(norm, 1e-2, 1e-4)
-        assert rel(op.EvaluateGradient(to_dev(v)).cpu().numpy(), reg.gradient(v.astype(np.float64))) < TOL
-        assert rel(op.ApplyInverse(to_dev(v)).cpu().numpy(), reg.apply_inverse(v.astype(np.float64))) < TOL
+    variants = cb.fft_variant_candidates(150) if 150 in shape else [None]
+    try:
+        for var in variants:
+            if var is not None:
+                cb.set_fft_variant(150, var)
+            assert rel(cb.fft_grad(to_dev(f)).cpu().numpy(), R.grad(f.astype(np.float64))) < TOL, var
+            assert rel(cb.fft_div(to_dev(v)).cpu().numpy(), R.div(v.astype(np.float64))) < TOL, var
+            for norm in ("h1s", "h2"):
+                reg = R.Regularization(norm, 1e-2, 1e-4)
+                op = cb.Regularization(norm, 1e-2, 1e-4)
+                assert rel(op.EvaluateGradient(to_dev(v)).cpu().numpy(), reg.gradient(v.astype(np.float64))) < TOL
+                assert rel(op.ApplyInverse(to_dev(v)).cpu().numpy(), reg.apply_inverse(v.astype(np.float64))) < TOL
+            b = to_dev(v)
+            cb.leray(b, "stokes", (1e-2, 1e-4, 1e-4))
+            ref = R.leray_projection(v.astype(np.float64), "stokes", 1e-2, 1e-4)
+            assert rel(b.cpu().numpy(), ref) < TOL, var
+    finally:
+        cb.set_fft_variant(150, 0)
 
 
 @pytest.mark.parametrize("shape", [(32, 48, 16), (48, 32, 64)])
@@ -57,8 +69,9 @@ def test_transport_non_cubic(cb, shape):
     assert rel(out, R.interp3(f.astype(np.float64), q)) < TOL
 
 
-def test_registration_non_cubic(cb):
-    shape, nt = (32, 48, 32), 4
+@pytest.mark.parametrize("shape", [(32, 48, 32), (32, 150, 32)])
+def test_registration_non_cubic(cb, shape):
+    nt = 4
     mT = R.rescale(R.template_sin2(shape))
     v = R.velocity_trig(shape, 0.5, reference_case=False)
     mR = R.rescale(R.forward_transport(mT, v, nt))
