@@ -58,7 +58,8 @@ class Opts(ctypes.Structure):
         ("krylovfseq", ctypes.c_int), ("precond", ctypes.c_int), ("iporder", ctypes.c_int),
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int), ("betacont", ctypes.c_double),
         ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int), ("distance", ctypes.c_int),
-        ("scalecont", ctypes.c_int), ("gridcont", ctypes.c_int),
+        ("scalecont", ctypes.c_int), ("gridcont", ctypes.c_int), ("train", ctypes.c_int),
+        ("jbound", ctypes.c_double), ("betainit", ctypes.c_double),
     ]
 
 
@@ -74,7 +75,7 @@ class Stats(ctypes.Structure):
         ("pde_solves", ctypes.c_int), ("converged_reason", ctypes.c_int), ("J", ctypes.c_double),
         ("J0", ctypes.c_double), ("D", ctypes.c_double), ("D0", ctypes.c_double), ("R", ctypes.c_double),
         ("gnorm", ctypes.c_double), ("gnorm0", ctypes.c_double), ("rel_mismatch", ctypes.c_double),
-        ("seconds", ctypes.c_double),
+        ("seconds", ctypes.c_double), ("beta", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -68,6 +68,9 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->distance = CB_DIST_SL2;  // src/RegOpt.cpp:1079
   o->scalecont = 0;
   o->gridcont = 0;
+  o->train = CB_TRAIN_OFF;
+  o->jbound = 2.5e-1;  // src/RegOpt.cpp:1254
+  o->betainit = 1.0;   // src/RegOpt.cpp:1228
   return CB_OK;
 }
 
@@ -150,6 +153,19 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (!std::strcmp(val, "sl2")) o->distance = CB_DIST_SL2;
       else if (!std::strcmp(val, "ncc")) o->distance = CB_DIST_NCC;
       else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-train")) {
+      // src/RegOpt.cpp:730-755; a search runs at least one GN iteration per solve
+      if (next(&val)) return CB_ERR_ARG;
+      if (o->betacont > 0.0) return CB_ERR_ARG;  // no training and continuation together
+      if (!std::strcmp(val, "binary")) o->train = CB_TRAIN_BINARY;
+      else if (!std::strcmp(val, "reduce")) o->train = CB_TRAIN_REDUCE;
+      else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-jbound")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->jbound = std::atof(val);  // src/RegOpt.cpp:551-553
+    } else if (!std::strcmp(a, "-betainit")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->betainit = std::atof(val);  // src/RegOpt.cpp:767-769
     } else if (!std::strcmp(a, "-scalecont")) {
       o->scalecont = 1;  // src/RegOpt.cpp:769-770
     } else if (!std::strcmp(a, "-gridcont")) {
@@ -437,7 +453,9 @@ int run_gridcont(Solver& s, const std::vector<int>& sel) {
 }
 
 int run_dispatch(Solver& s, const std::vector<int>& sel) {
-  if (s.opts.betacont > 0.0) return s.run(sel);  // RunSolverRegParaCont first (src/CLAIREInterface.cpp:729-753)
+  // RunSolverRegParaCont first (src/CLAIREInterface.cpp:729-753)
+  if (s.opts.train != CB_TRAIN_OFF) return s.run_train(sel, s.opts.train);
+  if (s.opts.betacont > 0.0) return s.run(sel);
   if (s.opts.scalecont) return run_scalecont(s, sel);
   if (s.opts.gridcont) return run_gridcont(s, sel);
   return s.run(sel);
@@ -508,6 +526,7 @@ int claire_b200_get_stats(const claire_b200_ctx* c, int b, claire_b200_stats* st
   st->gnorm0 = p.gnorm0;
   st->rel_mismatch = p.rel_mismatch;
   st->seconds = p.seconds;
+  st->beta = p.beta0;
   return CB_OK;
 }
 

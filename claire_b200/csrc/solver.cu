@@ -1347,25 +1347,7 @@ int Solver::run_betacont(const std::vector<int>& sel, double beta_star, double p
       if (sel[b]) ps[b].beta0 = beta;
     return upload_params();
   };
-  auto level = [&](double gttol) -> int {
-    for (int b = 0; b < B; ++b)
-      if (sel[b]) {
-        ps[b].iter = 0;
-        ps[b].done = false;
-        ps[b].step = 1.0;
-        state_of[b] = 0;  // the objective changed with beta
-      }
-    CB_TRY(objective_at(v, sel));
-    CB_TRY(gradient_at_current(sel));
-    std::vector<int> fin;
-    while (true) {
-      bool running = false;
-      for (int b = 0; b < B; ++b) running |= sel[b] && ps[b].running && !ps[b].done;
-      if (!running) break;
-      CB_TRY(step(fin, gttol, 1));
-    }
-    return 0;
-  };
+  auto level = [&](double gttol) -> int { return solve_level(sel, gttol); };
   double beta = 1.0;
   CB_TRY(set_beta(beta));
   CB_TRY(begin(sel));
@@ -1376,6 +1358,127 @@ int Solver::run_betacont(const std::vector<int>& sel, double beta_star, double p
   }
   CB_TRY(set_beta(beta_star));
   CB_TRY(level(opts.opttol));
+  return finish(sel);
+}
+
+int Solver::solve_level(const std::vector<int>& sel, double gttol) {
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ps[b].iter = 0;
+      ps[b].done = false;
+      ps[b].running = true;
+      ps[b].reason = 0;
+      ps[b].step = 1.0;
+      state_of[b] = 0;  // the objective changed with beta
+    }
+  CB_TRY(objective_at(v, sel));
+  CB_TRY(gradient_at_current(sel));
+  std::vector<int> fin;
+  while (true) {
+    bool running = false;
+    for (int b = 0; b < B; ++b) running |= sel[b] && ps[b].running && !ps[b].done;
+    if (!running) break;
+    CB_TRY(step(fin, gttol, 1));
+  }
+  return 0;
+}
+
+// Regularisation-parameter searches of CLAIREInterface (src/CLAIREInterface.cpp):
+// RunSolverRegParaContBinarySearch (:955-1186) and ReductSearch (:1192-1285).
+// ||g0|| comes from one initialisation at beta = -betainit and v = 0; every
+// solve starts from the last solution whose det(grad y) stayed inside the
+// bound (CheckBounds, src/CLAIREBase.cpp:1386-1445: min J <= jbound or
+// 1 / max J <= jbound is a breach); a solve counts as converged unless it
+// ended on a line-search failure or NaN (Optimizer::GetSolutionStatus,
+// src/Optimizer.cpp:557-580).  Constants of src/RegOpt.hpp:337-343: beta is
+// scaled by 1/10 per step, at most 10 steps, down to 1e-4 (H1 types) or
+// 1e-7 (H2 types); the bisection stops when |dbeta| < 1e-2 beta*.  The
+// reported solution is the last valid one, with beta* in the stats.
+int Solver::run_train(const std::vector<int>& sel, int strategy) {
+  constexpr double kScale = 1e-1, kDScale = 1e-2;
+  constexpr int kMaxSteps = 10, kMaxSolves = 64;  // kMaxSolves: guard against endless re-lifting
+  float* best = nullptr;
+  if (cudaMalloc((void**)&best, sizeof(float) * 3 * n) != cudaSuccess) return CB_ERR_ALLOC;
+  struct Free {
+    float* p;
+    ~Free() { cudaFree(p); }
+  } free_best{best};
+  for (int pb = 0; pb < B; ++pb) {
+    if (!sel[pb]) continue;
+    std::vector<int> one(B, 0);
+    one[pb] = 1;
+    const int norm = ps[pb].norm;
+    const double betamin =
+        (norm == NORM_H1 || norm == NORM_H1SN) ? 1e-4 : ((norm == NORM_H2 || norm == NORM_H2SN) ? 1e-7 : 1e-9);
+    float* vb = v + pb * 3 * n;
+    auto set_beta = [&](double beta) -> int {
+      ps[pb].beta0 = beta;
+      return upload_params();
+    };
+    auto save_best = [&]() -> int {
+      return cudaMemcpyAsync(best, vb, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess
+                 ? 0 : CB_ERR_CUDA;
+    };
+    auto load_best = [&]() -> int {
+      state_of[pb] = 0;
+      return cudaMemcpyAsync(vb, best, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, stream) == cudaSuccess
+                 ? 0 : CB_ERR_CUDA;
+    };
+    // one solve at beta from the best solution: converged, bound reached
+    int solves = 0;
+    auto solve = [&](double beta, bool& converged, bool& breach) -> int {
+      ++solves;
+      CB_TRY(set_beta(beta));
+      CB_TRY(load_best());
+      CB_TRY(solve_level(one, opts.opttol));
+      converged = ps[pb].reason != 5 && ps[pb].reason != -1;
+      std::vector<double> st;
+      CB_TRY(det_def_grad(one, false, st));
+      breach = st[3 * pb] <= opts.jbound || 1.0 / st[3 * pb + 2] <= opts.jbound;
+      return 0;
+    };
+    double beta = opts.betainit, betastar = beta;
+    CB_TRY(set_beta(beta));
+    CB_TRY(begin(one));  // InitializeOptimization at beta0, v = initial guess
+    CB_TRY(save_best());
+    bool converged = true, breach = false;
+    for (int level = 0; level < kMaxSteps && solves < kMaxSolves; ++level) {
+      CB_TRY(solve(beta, converged, breach));
+      if (strategy == CB_TRAIN_BINARY && !converged && level > 0) break;
+      if (breach) {
+        if (strategy == CB_TRAIN_REDUCE || level > 0) break;
+        beta /= kScale;  // bound reached with the first beta: lift it
+        level = -1;
+      } else {
+        betastar = beta;
+        CB_TRY(save_best());
+        beta *= kScale;
+      }
+      if (beta < betamin) break;
+    }
+    if (strategy == CB_TRAIN_BINARY) {
+      double betahat = kScale * betastar;
+      double dbeta = (betastar - betahat) / 2.0;
+      beta = betastar - dbeta;
+      const double dbetamin = kDScale * betastar;
+      bool stop = false;
+      while (!stop && solves < kMaxSolves) {
+        CB_TRY(solve(beta, converged, breach));
+        if (converged && !breach) {
+          betastar = beta;
+          CB_TRY(save_best());
+        } else {
+          betahat = beta;
+        }
+        dbeta = (betastar - betahat) / 2.0;
+        beta = betastar - dbeta;
+        if (std::fabs(dbeta) < dbetamin) stop = true;
+      }
+    }
+    // Finalize(m_Solution): the last valid solution at beta*
+    CB_TRY(set_beta(betastar));
+    CB_TRY(load_best());
+  }
   return finish(sel);
 }
 

@@ -47,6 +47,11 @@ class Solver {
   int begin(const std::vector<int>& sel);                // join the GN loop (J0, ||g0||)
   int step(std::vector<int>& finished, double gttol = -1.0, int miniter = 0);  // one GN iteration
   int run_betacont(const std::vector<int>& sel, double beta_star, double presolve_gttol);
+  // -train binary|reduce: beta search against the det(grad y) bound, one problem at a time
+  int run_train(const std::vector<int>& sel, int strategy);
+  // one solve at the current weights from the current velocity, stopping tests
+  // from iteration 1 on, reference norms of the last begin() (a continuation level)
+  int solve_level(const std::vector<int>& sel, double gttol);
   int finish(const std::vector<int>& sel);               // final mismatch; leave the loop
   int objective_at(const float* vel, const std::vector<int>& sel);  // fills ps[p].J/D/R
   int gradient_at_current(const std::vector<int>& sel);              // g, ||g|| for v

@@ -33,6 +33,8 @@ enum {
   CB_NORM_L2 = 0, CB_NORM_H1 = 1, CB_NORM_H1SN = 2, CB_NORM_H2 = 3,
   CB_NORM_H2SN = 4, CB_NORM_H3 = 5, CB_NORM_H3SN = 6
 };
+/* Regularisation-parameter searches (-train): binary search and reduction. */
+enum { CB_TRAIN_OFF = 0, CB_TRAIN_BINARY = 1, CB_TRAIN_REDUCE = 2 };
 /* Registration models: CLAIRE (no projection), Stokes, relaxed Stokes. */
 enum { CB_MODEL_COMPRESSIBLE = 0, CB_MODEL_STOKES = 1, CB_MODEL_RELAXEDSTOKES = 2 };
 /* Distance measures (-distance): squared L2 (DistanceMeasureSL2) or
@@ -70,6 +72,9 @@ typedef struct claire_b200_opts {
   int distance;         /* -distance sl2|ncc (CB_DIST_SL2); NCC needs FP32 images */
   int scalecont;        /* -scalecont: continuation over image smoothing widths */
   int gridcont;         /* -gridcont: continuation over grid sizes */
+  int train;            /* -train binary|reduce: search beta against the det(grad y) bound (0: off) */
+  double jbound;        /* -jbound: bound on min det(grad y) and 1/max det(grad y) (0.25) */
+  double betainit;      /* -betainit: first beta of -train and -betacont searches (1.0) */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {
@@ -81,6 +86,7 @@ typedef struct claire_b200_stats {
   double gnorm, gnorm0;     /* ||g|| and ||g0|| (FP64) */
   double rel_mismatch;      /* ||mR - m1|| / ||mR - mT|| */
   double seconds;           /* wall time of claire_b200_run */
+  double beta;              /* regularisation weight of the solution (the estimate of -train) */
 } claire_b200_stats;
 
 typedef struct claire_b200_ctx claire_b200_ctx;

@@ -950,6 +950,81 @@ def scale_continuation(mR, mT, nt: int, reg: Regularization, opts: GNOptions = G
     return res
 
 
+def train_search(mR, mT, nt: int, reg: Regularization, opts: GNOptions = GNOptions(), strategy="binary",
+                 jbound=0.25, betainit=1.0, **problem_kw):
+    """Regularisation-parameter search (CLAIREInterface::
+    RunSolverRegParaContBinarySearch, src/CLAIREInterface.cpp:955-1186, and
+    RunSolverRegParaContReductSearch, :1192-1285): ||g0|| at beta = betainit
+    and v = 0; every solve warm-starts from the last solution whose
+    det(grad y) stays inside the bound (CheckBounds, src/CLAIREBase.cpp:
+    1386-1445), with tests from iteration 1; beta scaled by 1/10 per step (at
+    most 10 steps, not below 1e-4 for H1 types, 1e-7 for H2 types); the
+    binary search then bisects [beta*/10, beta*] until |dbeta| < 1e-2 beta*.
+    A solve that ended on a line-search failure or NaN counts as not
+    converged (Optimizer::GetSolutionStatus, src/Optimizer.cpp:557-580).
+    Returns beta*, its solution, and the list of (beta, converged, breach)."""
+    import dataclasses
+    scale, dscale, maxsteps, maxsolves = 1e-1, 1e-2, 10, 64
+    betamin = 1e-4 if reg.norm in ("h1", "h1s") else (1e-7 if reg.norm in ("h2", "h2s") else 1e-9)
+    prob = Problem(mR, mT, nt, dataclasses.replace(reg, beta0=betainit), **problem_kw)
+    z = np.zeros((3,) + prob.shape, dtype=prob.dtype)
+    prob.objective(z)
+    gz = prob.gradient(z)
+    g0 = math.sqrt(dot(gz, gz))
+    g0 = g0 if g0 > 0 else 1.0
+    state = {"best": z, "kg0": None}
+    log = []
+
+    def solve(beta):
+        prob.reg = dataclasses.replace(reg, beta0=beta)
+        res = gauss_newton(prob, opts, v0=state["best"], g0=g0, krylov_g0=state["kg0"], miniter=1)
+        state["kg0"] = res["krylov_g0"]
+        converged = res["reason"] not in ("lsfail", "nan")
+        _, (mn, _, mx) = det_def_grad(res["v"], nt)
+        breach = mn <= jbound or 1.0 / mx <= jbound
+        log.append((beta, converged, breach))
+        return res, converged, breach
+
+    beta = betastar = betainit
+    level = 0
+    while level < maxsteps and len(log) < maxsolves:
+        res, converged, breach = solve(beta)
+        if strategy == "binary" and not converged and level > 0:
+            break
+        if breach:
+            if strategy == "reduce" or level > 0:
+                break
+            beta /= scale
+            level = -1
+        else:
+            betastar = beta
+            state["best"] = res["v"]
+            beta *= scale
+        if beta < betamin:
+            break
+        level += 1
+    if strategy == "binary":
+        betahat = scale * betastar
+        dbeta = (betastar - betahat) / 2.0
+        beta = betastar - dbeta
+        dbetamin = dscale * betastar
+        while len(log) < maxsolves:
+            res, converged, breach = solve(beta)
+            if converged and not breach:
+                betastar = beta
+                state["best"] = res["v"]
+            else:
+                betahat = beta
+            dbeta = (betastar - betahat) / 2.0
+            beta = betastar - dbeta
+            if abs(dbeta) < dbetamin:
+                break
+    prob.reg = dataclasses.replace(reg, beta0=betastar)
+    prob.set_velocity(state["best"])
+    m1 = prob.solve_state()[nt]
+    return dict(beta=betastar, v=state["best"], log=log, m1=m1, prob=prob)
+
+
 def relative_mismatch(mR, m1, mT) -> float:
     """||mR - m1|| / ||mR - mT|| (src/CLAIRE.cpp:4232-4262)."""
     a = np.linalg.norm((mR - m1).astype(np.float64).ravel())

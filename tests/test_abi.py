@@ -60,6 +60,11 @@ def test_parse_args():
     assert cb.RegOpt(["-nx", "64", "-bf16images"]).opts.bf16_images == 1
     assert o.autotune == 0 and cb.RegOpt(["-nx", "64", "-autotune"]).opts.autotune == 1
     assert o.distance == 0 and cb.RegOpt(["-nx", "64", "-distance", "ncc"]).opts.distance == 1
+    assert o.train == 0 and o.jbound == 0.25 and o.betainit == 1.0
+    t = cb.RegOpt(["-nx", "64", "-train", "binary", "-jbound", "0.3", "-betainit", "0.5"]).opts
+    assert t.train == 1 and t.jbound == 0.3 and t.betainit == 0.5
+    with pytest.raises(cb.ClaireError):
+        cb.RegOpt(["-nx", "64", "-betacont", "1e-3", "-train", "reduce"])
     opt2 = cb.RegOpt(["-nx", "96", "-regnorm", "h1s-stokes"])
     assert tuple(opt2.opts.nx) == (96, 96, 96) and opt2.opts.model == cb.MODELS["stokes"]
 
