@@ -59,7 +59,7 @@ class Opts(ctypes.Structure):
         ("verbosity", ctypes.c_int), ("bf16_images", ctypes.c_int), ("betacont", ctypes.c_double),
         ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int), ("distance", ctypes.c_int),
         ("scalecont", ctypes.c_int), ("gridcont", ctypes.c_int), ("train", ctypes.c_int),
-        ("jbound", ctypes.c_double), ("betainit", ctypes.c_double),
+        ("jbound", ctypes.c_double), ("betainit", ctypes.c_double), ("monitordefgrad", ctypes.c_int),
     ]
 
 
@@ -75,7 +75,8 @@ class Stats(ctypes.Structure):
         ("pde_solves", ctypes.c_int), ("converged_reason", ctypes.c_int), ("J", ctypes.c_double),
         ("J0", ctypes.c_double), ("D", ctypes.c_double), ("D0", ctypes.c_double), ("R", ctypes.c_double),
         ("gnorm", ctypes.c_double), ("gnorm0", ctypes.c_double), ("rel_mismatch", ctypes.c_double),
-        ("seconds", ctypes.c_double), ("beta", ctypes.c_double),
+        ("seconds", ctypes.c_double), ("beta", ctypes.c_double), ("solution_status", ctypes.c_int),
+        ("det_min", ctypes.c_double), ("det_mean", ctypes.c_double), ("det_max", ctypes.c_double),
     ]
 
     def as_dict(self):

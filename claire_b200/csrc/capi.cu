@@ -71,6 +71,7 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->train = CB_TRAIN_OFF;
   o->jbound = 2.5e-1;  // src/RegOpt.cpp:1254
   o->betainit = 1.0;   // src/RegOpt.cpp:1228
+  o->monitordefgrad = 0;
   return CB_OK;
 }
 
@@ -160,6 +161,8 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       if (!std::strcmp(val, "binary")) o->train = CB_TRAIN_BINARY;
       else if (!std::strcmp(val, "reduce")) o->train = CB_TRAIN_REDUCE;
       else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-monitordefgrad")) {
+      o->monitordefgrad = 1;  // src/RegOpt.cpp:779-780
     } else if (!std::strcmp(a, "-jbound")) {
       if (next(&val)) return CB_ERR_ARG;
       o->jbound = std::atof(val);  // src/RegOpt.cpp:551-553
@@ -458,6 +461,7 @@ int run_dispatch(Solver& s, const std::vector<int>& sel) {
   if (s.opts.betacont > 0.0) return s.run(sel);
   if (s.opts.scalecont) return run_scalecont(s, sel);
   if (s.opts.gridcont) return run_gridcont(s, sel);
+  if (s.opts.monitordefgrad) return s.run_monitored(sel);
   return s.run(sel);
 }
 
@@ -527,6 +531,10 @@ int claire_b200_get_stats(const claire_b200_ctx* c, int b, claire_b200_stats* st
   st->rel_mismatch = p.rel_mismatch;
   st->seconds = p.seconds;
   st->beta = p.beta0;
+  st->solution_status = p.solution_status;
+  st->det_min = p.det[0];
+  st->det_mean = p.det[1];
+  st->det_max = p.det[2];
   return CB_OK;
 }
 

@@ -1397,6 +1397,7 @@ int Solver::solve_level(const std::vector<int>& sel, double gttol) {
 int Solver::run_train(const std::vector<int>& sel, int strategy) {
   constexpr double kScale = 1e-1, kDScale = 1e-2;
   constexpr int kMaxSteps = 10, kMaxSolves = 64;  // kMaxSolves: guard against endless re-lifting
+  std::vector<double> det_keep((size_t)3 * B, 0.0);
   float* best = nullptr;
   if (cudaMalloc((void**)&best, sizeof(float) * 3 * n) != cudaSuccess) return CB_ERR_ALLOC;
   struct Free {
@@ -1426,6 +1427,7 @@ int Solver::run_train(const std::vector<int>& sel, int strategy) {
     };
     // one solve at beta from the best solution: converged, bound reached
     int solves = 0;
+    double best_det[3] = {0.0, 0.0, 0.0};  // det(grad y) of the last valid solution
     auto solve = [&](double beta, bool& converged, bool& breach) -> int {
       ++solves;
       CB_TRY(set_beta(beta));
@@ -1435,6 +1437,8 @@ int Solver::run_train(const std::vector<int>& sel, int strategy) {
       std::vector<double> st;
       CB_TRY(det_def_grad(one, false, st));
       breach = st[3 * pb] <= opts.jbound || 1.0 / st[3 * pb + 2] <= opts.jbound;
+      if (!breach)
+        for (int k = 0; k < 3; ++k) best_det[k] = st[3 * pb + k];
       return 0;
     };
     double beta = opts.betainit, betastar = beta;
@@ -1478,8 +1482,71 @@ int Solver::run_train(const std::vector<int>& sel, int strategy) {
     // Finalize(m_Solution): the last valid solution at beta*
     CB_TRY(set_beta(betastar));
     CB_TRY(load_best());
+    for (int k = 0; k < 3; ++k) det_keep[(size_t)3 * pb + k] = best_det[k];
   }
-  return finish(sel);
+  CB_TRY(finish(sel));
+  for (int b = 0; b < B; ++b)
+    if (sel[b])
+      for (int k = 0; k < 3; ++k) ps[b].det[k] = det_keep[(size_t)3 * b + k];
+  return 0;
+}
+
+// RunSolver with -monitordefgrad (src/CLAIREInterface.cpp:790-862): after a
+// solve from the initial guess, CheckBounds; while breached (at most 10
+// times) beta moves halfway toward beta* = 10 beta (RegNorm.beta[3] is never
+// set, :806-810) and the problem is solved again from the initial guess.
+// solution_status 0: the first solution kept the bound, 1: a raised beta
+// did, 2: none did (beta is then reported as beta*).
+int Solver::run_monitored(const std::vector<int>& sel) {
+  float* guess = nullptr;
+  if (cudaMalloc((void**)&guess, sizeof(float) * 3 * n) != cudaSuccess) return CB_ERR_ALLOC;
+  struct Free {
+    float* p;
+    ~Free() { cudaFree(p); }
+  } free_guess{guess};
+  std::vector<double> det_keep((size_t)3 * B, 0.0);
+  std::vector<int> status(B, 0);
+  for (int pb = 0; pb < B; ++pb) {
+    if (!sel[pb]) continue;
+    std::vector<int> one(B, 0);
+    one[pb] = 1;
+    float* vb = v + pb * 3 * n;
+    if (cudaMemcpyAsync(guess, vb, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+    double beta = ps[pb].beta0;
+    const double betastar = beta / 1e-1;
+    CB_TRY(begin(one));  // InitializeOptimization once, at the first beta
+    bool breach = true;
+    int level = 0;
+    std::vector<double> st;
+    while (breach && level < 10) {
+      if (cudaMemcpyAsync(vb, guess, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+        return CB_ERR_CUDA;
+      state_of[pb] = 0;
+      CB_TRY(solve_level(one, opts.opttol));
+      CB_TRY(det_def_grad(one, false, st));
+      breach = st[3 * pb] <= opts.jbound || 1.0 / st[3 * pb + 2] <= opts.jbound;
+      if (breach) {
+        beta += (betastar - beta) / 2.0;
+        ps[pb].beta0 = beta;
+        CB_TRY(upload_params());
+        ++level;
+      }
+    }
+    status[pb] = level == 0 ? 0 : (breach ? 2 : 1);
+    if (status[pb] == 2) {
+      ps[pb].beta0 = betastar;
+      CB_TRY(upload_params());
+    }
+    for (int k = 0; k < 3; ++k) det_keep[(size_t)3 * pb + k] = st[3 * pb + k];
+  }
+  CB_TRY(finish(sel));
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ps[b].solution_status = status[b];
+      for (int k = 0; k < 3; ++k) ps[b].det[k] = det_keep[(size_t)3 * b + k];
+    }
+  return 0;
 }
 
 int Solver::run(const std::vector<int>& sel) {

@@ -33,6 +33,8 @@ struct ProbState {
   std::chrono::steady_clock::time_point t0{};
   int obj_evals = 0, grad_evals = 0, hess_matvecs = 0, pc_matvecs = 0, pde_solves = 0;
   double seconds = 0.0, rel_mismatch = -1.0;
+  int solution_status = 0;
+  double det[3] = {0.0, 0.0, 0.0};  // min, mean, max of det(grad y) when checked
 };
 
 class Solver {
@@ -49,6 +51,8 @@ class Solver {
   int run_betacont(const std::vector<int>& sel, double beta_star, double presolve_gttol);
   // -train binary|reduce: beta search against the det(grad y) bound, one problem at a time
   int run_train(const std::vector<int>& sel, int strategy);
+  // -monitordefgrad: RunSolver's bound check and beta raising
+  int run_monitored(const std::vector<int>& sel);
   // one solve at the current weights from the current velocity, stopping tests
   // from iteration 1 on, reference norms of the last begin() (a continuation level)
   int solve_level(const std::vector<int>& sel, double gttol);

@@ -75,6 +75,8 @@ typedef struct claire_b200_opts {
   int train;            /* -train binary|reduce: search beta against the det(grad y) bound (0: off) */
   double jbound;        /* -jbound: bound on min det(grad y) and 1/max det(grad y) (0.25) */
   double betainit;      /* -betainit: first beta of -train and -betacont searches (1.0) */
+  int monitordefgrad;   /* -monitordefgrad: check det(grad y) against -jbound after the solve and
+                           raise beta toward 10 beta while it is breached (RunSolver) */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {
@@ -87,6 +89,8 @@ typedef struct claire_b200_stats {
   double rel_mismatch;      /* ||mR - m1|| / ||mR - mT|| */
   double seconds;           /* wall time of claire_b200_run */
   double beta;              /* regularisation weight of the solution (the estimate of -train) */
+  int solution_status;      /* -monitordefgrad: 0 bound kept, 1 kept after raising beta, 2 still breached */
+  double det_min, det_mean, det_max; /* det(grad y) of the solution (-monitordefgrad / -train) */
 } claire_b200_stats;
 
 typedef struct claire_b200_ctx claire_b200_ctx;

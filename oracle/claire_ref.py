@@ -1025,6 +1025,40 @@ def train_search(mR, mT, nt: int, reg: Regularization, opts: GNOptions = GNOptio
     return dict(beta=betastar, v=state["best"], log=log, m1=m1, prob=prob)
 
 
+def monitored_run(mR, mT, nt: int, reg: Regularization, opts: GNOptions = GNOptions(), jbound=0.25,
+                  **problem_kw):
+    """CLAIREInterface::RunSolver with -monitordefgrad (src/CLAIREInterface.cpp:
+    790-862): ||g0|| once at the first beta; solve from the initial guess
+    (zero); while det(grad y) breaches the bound (at most 10 times) beta moves
+    halfway toward beta* = 10 beta and the solve restarts from the guess.
+    Status 0: first solution kept the bound, 1: a raised beta did, 2: none
+    did (beta reported as beta*)."""
+    import dataclasses
+    beta = reg.beta0
+    betastar = beta / 1e-1
+    prob = Problem(mR, mT, nt, reg, **problem_kw)
+    z = np.zeros((3,) + prob.shape, dtype=prob.dtype)
+    prob.objective(z)
+    gz = prob.gradient(z)
+    g0 = math.sqrt(dot(gz, gz))
+    g0 = g0 if g0 > 0 else 1.0
+    level, breach, kg0 = 0, True, None
+    while breach and level < 10:
+        res = gauss_newton(prob, opts, v0=z, g0=g0, krylov_g0=kg0, miniter=1)
+        kg0 = res["krylov_g0"]
+        _, (mn, mean, mx) = det_def_grad(res["v"], nt)
+        breach = mn <= jbound or 1.0 / mx <= jbound
+        if breach:
+            beta += (betastar - beta) / 2.0
+            prob.reg = dataclasses.replace(prob.reg, beta0=beta)
+            level += 1
+    status = 0 if level == 0 else (2 if breach else 1)
+    res["beta"] = betastar if status == 2 else beta
+    res["status"] = status
+    res["det"] = (mn, mean, mx)
+    return res
+
+
 def relative_mismatch(mR, m1, mT) -> float:
     """||mR - m1|| / ||mR - mT|| (src/CLAIRE.cpp:4232-4262)."""
     a = np.linalg.norm((mR - m1).astype(np.float64).ravel())

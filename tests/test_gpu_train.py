@@ -51,3 +51,25 @@ def test_train_search_matches_oracle(cb, strategy):
         assert np.linalg.norm((v - res["v"]).ravel()) <= 1e-3 * nv, facts
     else:
         assert abs(st["beta"] - res["beta"]) <= 0.1 * res["beta"], facts
+
+
+def test_monitordefgrad_raises_beta_like_oracle(cb):
+    # -monitordefgrad: beta = 1e-2 breaches min det > 0.5 on this problem; beta
+    # is raised halfway toward 10 beta and the solve repeated from zero
+    mR, mT, n, nt = problem()
+    jb = 0.5
+    res = R.monitored_run(mR, mT, nt, R.Regularization("h1s", 1e-2), R.GNOptions(maxit=5, gttol=5e-2), jbound=jb)
+    opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", "h1s", "-beta", "1e-2", "-maxit", "5",
+                     "-opttol", "5e-2", "-monitordefgrad", "-jbound", str(jb)])
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        ci.Run()
+        st = ci.stats()
+        v = np.asarray(ci.GetSolution())
+    facts = dict(st={k: st[k] for k in ("beta", "solution_status", "det_min", "det_max")},
+                 oracle=(res["beta"], res["status"], res["det"]))
+    assert st["solution_status"] == res["status"] == 1, facts
+    assert st["beta"] == pytest.approx(res["beta"], rel=1e-12), facts
+    assert abs(st["det_min"] - res["det"][0]) <= 1e-3 * res["det"][0], facts
+    nv = np.linalg.norm(res["v"].ravel())
+    assert np.linalg.norm((v - res["v"]).ravel()) <= 1e-3 * nv, facts
