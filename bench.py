@@ -458,7 +458,8 @@ def cpu_op_times(n, workers=None):
 
 
 def cpu_seconds_per_registration(stats, nt, t_gather, t_fft):
-    """Compose the reference's per-call operation counts (SURVEY call stacks):
+    """Compose the reference's per-call operation counts (the call stacks of
+    its objective, gradient, Hessian matvec and preconditioner):
     objective: 3 (trajectory) + nt gathers, 6 FFTs (H2 functional);
     gradient: 3 + 1 + nt gathers, 4(nt+1) + 4 + 6 FFTs;
     Hessian matvec: 5nt + 4 gathers, 12nt + 14 FFTs; preconditioner: 6 FFTs."""

@@ -84,7 +84,7 @@ class Solver {
   std::vector<ProbState> ps;
   std::string err;
 
-  // device state (see DESIGN.md for the layout)
+  // device state: one allocation per array, problem p at base + p * stride
   float *mR = nullptr, *mT = nullptr, *v = nullptr, *vtrial = nullptr, *m = nullptr;
   float *disp_st = nullptr, *disp_adj = nullptr, *gm = nullptr, *gx = nullptr;
   int4 *tab_st = nullptr, *tab_adj = nullptr;  // box tables of the two characteristics

@@ -1,0 +1,74 @@
+"""Registrations at 64^3 on the device against the oracle's FP64 runs
+committed in tests/golden/ (made by tests/golden/make_golden.py):
+
+* c1_64: the reference's own synthetic configuration (sin^2 template, trig
+  velocity, H1 seminorm beta = 1e-2, nt = 4, gradient tolerance 1e-2, at
+  most 10 GN iterations): iteration counts within one, monitor values and
+  velocity within 1e-4;
+* c3_64: an ellipsoid / random-velocity problem with H1 (beta1 = 1e-4 makes
+  the inverse symbol 1e6 at k = 0, so PCG counts follow FP32 roundoff): GN
+  count within one, objective, mismatch and velocity within 1e-3.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import claire_ref as R
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def cb(cuda):
+    import claire_b200
+    return claire_b200
+
+
+def projections(v, k=8, seed=2026):
+    rng = np.random.default_rng(seed)
+    return [float(np.sum(np.asarray(v, np.float64) * rng.standard_normal(v.shape))) for _ in range(k)]
+
+
+def c1_images(p):
+    mR, mT, _ = R.synthetic_c1(p["n"], np.float64, p["nt"])
+    return mR, mT
+
+
+def c3_images(p):
+    n, nt = p["n"], p["nt"]
+    rng = np.random.Generator(np.random.PCG64(R.problem_seed(2, 0)))
+    shape = (n, n, n)
+    mT = R.template_ellipsoids(shape, rng)
+    v = R.velocity_random(shape, rng)
+    return R.forward_transport(mT, v, nt), mT
+
+
+@pytest.mark.parametrize("name,images,tol,exact_pcg", [("c1_64.json", c1_images, 1e-4, True),
+                                                       ("c3_64.json", c3_images, 1e-3, False)])
+def test_registration_matches_golden(cb, name, images, tol, exact_pcg):
+    g = json.load(open(os.path.join(HERE, "golden", name)))
+    p = g["problem"]
+    mR, mT = images(p)
+    opt = cb.RegOpt(["-nx", str(p["n"]), "-nt", str(p["nt"]), "-regnorm", p["regnorm"], "-beta", str(p["beta"]),
+                     "-maxit", str(p["maxit"]), "-opttol", str(p["opttol"])])
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR.astype(np.float32), mT.astype(np.float32))
+        ci.Run()
+        st = ci.stats()
+        v = np.asarray(ci.GetSolution())
+    facts = dict(gn=(st["gn_iterations"], g["gn_iterations"]), pcg=(st["pcg_iterations"], g["pcg_iterations"]),
+                 mis=(st["rel_mismatch"], g["rel_mismatch"]), J=(st["J"], g["J"]))
+    assert abs(st["gn_iterations"] - g["gn_iterations"]) <= 1, facts
+    if exact_pcg:
+        assert abs(st["pcg_iterations"] - sum(g["pcg_iterations"])) <= len(g["pcg_iterations"]), facts
+    assert abs(st["rel_mismatch"] - g["rel_mismatch"]) <= tol * g["rel_mismatch"], facts
+    assert abs(st["J"] - g["J"]) <= tol * abs(g["J"]), facts
+    assert abs(np.linalg.norm(v.ravel()) - g["velocity_norm"]) <= tol * g["velocity_norm"], facts
+    got = projections(v)
+    scale = g["velocity_norm"] * np.sqrt(v.size)  # size of a projection onto a random field
+    for a, b in zip(got, g["velocity_projections"]):
+        assert abs(a - b) <= tol * scale, (a, b, facts)

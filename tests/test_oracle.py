@@ -1,6 +1,6 @@
 """Pin the oracle to the reference's own known-answer checks (CPU only).
 
-The reference ships no golden vectors; what it does check (SURVEY §8c):
+The reference ships no golden vectors; what it does check:
 tricubic Lagrange reproduction of cubics / node values, spectral operators
 exact on trig polynomials, the forward/backward transport round trip of
 apps/benchmark.cpp:297-380, the Taylor gradient test and the Hessian
@@ -321,3 +321,20 @@ def test_masked_distance_taylor_gradient_and_unit_mask(distance):
     ones = R.Problem(mR, mT, nt, reg, distance=distance, mask=np.ones((n, n, n)))
     plain = R.Problem(mR, mT, nt, reg, distance=distance)
     assert abs(ones.objective(v) - plain.objective(v)) <= 1e-12 * abs(plain.objective(v))
+
+
+def test_golden_c1_64_is_the_current_oracle():
+    # the committed 64^3 fixture was made by this oracle: its problem
+    # description and its initial gradient norm agree with a fresh evaluation
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c1_64.json")))
+    p = g["problem"]
+    assert (p["n"], p["nt"], p["regnorm"], p["beta"]) == (64, 4, "h1s", 1e-2)
+    mR, mT, _ = R.synthetic_c1(p["n"], np.float64, p["nt"])
+    prob = R.Problem(mR.astype(np.float32), mT.astype(np.float32), p["nt"], R.Regularization("h1s", p["beta"]))
+    z = np.zeros((3,) + prob.shape)
+    prob.objective(z)
+    gz = prob.gradient(z)
+    assert abs(np.sqrt(R.dot(gz, gz)) - g["g0"]) <= 1e-12 * g["g0"]
+    assert g["reason"] in ("gttol", "maxit", "steptol") and len(g["pcg_iterations"]) == g["gn_iterations"]
