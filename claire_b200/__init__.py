@@ -60,6 +60,7 @@ class Opts(ctypes.Structure):
         ("presolvetol", ctypes.c_double), ("autotune", ctypes.c_int), ("distance", ctypes.c_int),
         ("scalecont", ctypes.c_int), ("gridcont", ctypes.c_int), ("train", ctypes.c_int),
         ("jbound", ctypes.c_double), ("betainit", ctypes.c_double), ("monitordefgrad", ctypes.c_int),
+        ("pcgridscale", ctypes.c_double), ("pctolscale", ctypes.c_double), ("pcsolvermaxit", ctypes.c_int),
     ]
 
 

@@ -72,6 +72,9 @@ int claire_b200_default_opts(claire_b200_opts* o) {
   o->jbound = 2.5e-1;  // src/RegOpt.cpp:1254
   o->betainit = 1.0;   // src/RegOpt.cpp:1228
   o->monitordefgrad = 0;
+  o->pcgridscale = 2.0;   // src/RegOpt.cpp:1124
+  o->pctolscale = 1e-1;   // src/RegOpt.cpp:1121
+  o->pcsolvermaxit = 10;  // src/RegOpt.cpp:1123
   return CB_OK;
 }
 
@@ -141,9 +144,35 @@ int claire_b200_parse_args(claire_b200_opts* o, int argc, const char* const* arg
       else return CB_ERR_ARG;
     } else if (!std::strcmp(a, "-precond")) {
       if (next(&val)) return CB_ERR_ARG;
-      if (!std::strcmp(val, "none")) o->precond = 0;
-      else if (!std::strcmp(val, "invreg")) o->precond = 1;
-      else return CB_ERR_UNSUPPORTED;  // 2level: not on this path
+      // src/RegOpt.cpp:592-611
+      if (!std::strcmp(val, "none")) o->precond = CB_PC_NONE;
+      else if (!std::strcmp(val, "invreg")) o->precond = CB_PC_INVREG;
+      else if (!std::strcmp(val, "2level")) o->precond = CB_PC_TWOLEVEL;
+      else return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-gridscale")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->pcgridscale = std::atof(val);  // src/RegOpt.cpp:612-614
+      if (!(o->pcgridscale >= 1.0)) return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-pcsolver")) {
+      // src/RegOpt.cpp:615-631: the coarse solve runs KSPCG; the flexible and
+      // Chebyshev solvers are not on this path
+      if (next(&val)) return CB_ERR_ARG;
+      if (std::strcmp(val, "pcg")) {
+        if (!std::strcmp(val, "fpcg") || !std::strcmp(val, "gmres") || !std::strcmp(val, "fgmres") ||
+            !std::strcmp(val, "cheb"))
+          return CB_ERR_UNSUPPORTED;
+        return CB_ERR_ARG;
+      }
+    } else if (!std::strcmp(a, "-pctolscale")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->pctolscale = std::atof(val);  // src/RegOpt.cpp:645-647, checked at :1696-1700
+      if (!(o->pctolscale >= 0.0 && o->pctolscale < 1.0)) return CB_ERR_ARG;
+    } else if (!std::strcmp(a, "-pcsolvermaxit")) {
+      if (next(&val)) return CB_ERR_ARG;
+      o->pcsolvermaxit = std::atoi(val);  // src/RegOpt.cpp:648-650
+    } else if (!std::strcmp(a, "-monitorpcsolver")) {
+      // src/RegOpt.cpp:643-644: prints the coarse solver's residuals (here:
+      // its iteration count per application at -verbosity > 0)
     } else if (!std::strcmp(a, "-iporder")) {
       if (next(&val)) return CB_ERR_ARG;
       o->iporder = std::atoi(val);
@@ -460,7 +489,15 @@ int run_dispatch(Solver& s, const std::vector<int>& sel) {
   if (s.opts.train != CB_TRAIN_OFF) return s.run_train(sel, s.opts.train);
   if (s.opts.betacont > 0.0) return s.run(sel);
   if (s.opts.scalecont) return run_scalecont(s, sel);
-  if (s.opts.gridcont) return run_gridcont(s, sel);
+  if (s.opts.gridcont) {
+    if (s.opts.precond == CB_PC_TWOLEVEL) {
+      // the coarsest continuation levels would need coarse grids below the
+      // smallest transform size
+      s.err = "grid continuation with the two-level preconditioner is not supported";
+      return CB_ERR_UNSUPPORTED;
+    }
+    return run_gridcont(s, sel);
+  }
   if (s.opts.monitordefgrad) return s.run_monitored(sel);
   return s.run(sel);
 }

@@ -349,8 +349,11 @@ int claire_b200_server_submit(claire_b200_server* s, const claire_b200_opts* o, 
                               long long* id) {
   if (!s || !o || !mR || !mT || !id) return CB_ERR_ARG;
   // a pool advances its slots one GN iteration at a time: the continuation
-  // drivers (several solves per request) run through claire_b200_run instead
-  if (o->betacont > 0.0 || o->scalecont || o->gridcont || o->train || o->monitordefgrad) return CB_ERR_UNSUPPORTED;
+  // drivers (several solves per request) and the two-level preconditioner
+  // (a nested coarse solve per Krylov iteration) run through claire_b200_run
+  if (o->betacont > 0.0 || o->scalecont || o->gridcont || o->train || o->monitordefgrad ||
+      o->precond == CB_PC_TWOLEVEL)
+    return CB_ERR_UNSUPPORTED;
   if (o->nx[0] <= 0 || o->nx[1] <= 0 || o->nx[2] <= 0 || o->nt < 1) return CB_ERR_ARG;
   const long long n = (long long)o->nx[0] * o->nx[1] * o->nx[2];
   cb::srv::Request r;

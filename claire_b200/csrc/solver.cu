@@ -129,10 +129,11 @@ static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 // allocation
 // ---------------------------------------------------------------------------
 Solver::~Solver() {
+  coarse.reset();  // it issues work on this solver's stream
   prof_clear();
   if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
   void* ptrs[] = {mR, mT, m, mR16, mT16, m16, wmask, v, vtrial, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
-                  r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams};
+                  r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams, gwork};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (hsc) cudaFreeHost(hsc);
@@ -158,6 +159,19 @@ static int max_parts(const Dims& d) {
   return mp;
 }
 
+// Options of the two-level preconditioner's coarse problems
+// (Preconditioner::SetupCoarseGrid, src/Preconditioner.cpp:370-387): every
+// option of the fine grid but nx = ceil(nx / gridscale); the coarse Krylov
+// solve has no preconditioner (src/Preconditioner.cpp:947-951).
+static claire_b200_opts coarse_opts(const claire_b200_opts& o) {
+  claire_b200_opts oc = o;
+  for (int k = 0; k < 3; ++k) oc.nx[k] = (int)std::ceil((double)o.nx[k] / o.pcgridscale);
+  oc.precond = CB_PC_NONE;
+  oc.betacont = 0.0;
+  oc.scalecont = oc.gridcont = oc.train = oc.monitordefgrad = 0;
+  return oc;
+}
+
 long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   Dims d{o.nx[0], o.nx[1], o.nx[2]};
   const long long n = d.n(), nc = d.nc();
@@ -175,7 +189,14 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   long long bytes = floats * 4 + image_bytes + 3 * nc * 8;
   bytes += 2 * tile_table_int4s(d) * 16;  // box tables of the two characteristics
   bytes += (long long)max_parts(d) * 8;
-  return bytes * B;
+  bytes *= B;
+  if (o.precond == CB_PC_TWOLEVEL) {
+    // the coarse problems and the grid-change workspace
+    const claire_b200_opts oc = coarse_opts(o);
+    bytes += estimate_bytes(oc, B);
+    bytes += 4 * grid_change_work(d.n1, oc.nx[0], std::max(3, nt + 1));
+  }
+  return bytes;
 }
 
 int Solver::init(const claire_b200_opts& o, int Bn) {
@@ -219,6 +240,20 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   if (ncc && img16) {
     err = "the NCC distance needs FP32 images";
     return CB_ERR_UNSUPPORTED;
+  }
+  mv_kind = o.precond == CB_PC_TWOLEVEL ? 1 : 0;
+  if (mv_kind) {
+    // the coarse grid must have an FFT plan, and an even size makes the
+    // rectangular filters of Apply2LevelPrecond the restriction's band
+    nc1 = coarse_opts(o).nx[0];
+    if (img16 || ncc || d.n1 != d.n2 || d.n2 != d.n3) {
+      err = "the two-level preconditioner needs a cubic grid, FP32 images and the SL2 distance";
+      return CB_ERR_UNSUPPORTED;
+    }
+    if (nc1 < 2 || nc1 > d.n1 || (nc1 % 2) || !fft_size_supported(nc1)) {
+      err = "the two-level preconditioner's coarse grid (ceil(nx / gridscale) points) is odd or has no FFT plan";
+      return CB_ERR_UNSUPPORTED;
+    }
   }
   if (img16) {
     const size_t S16 = sizeof(bf16) * n * B;
@@ -446,6 +481,7 @@ int Solver::set_mask(int b, const float* w) {
     CB_TRY(launch_fill(wmask + b * n, 0, 1.f, n, 1, nullptr, stream));
   }
   images_changed(b);
+  coarse.reset();  // rebuilt with a mask by the next two-level setup
   // the recorded PCG iteration may lack the weighting: record it again
   if (pcg_exec) {
     cudaGraphExecDestroy(pcg_exec);
@@ -777,7 +813,8 @@ int Solver::divergence(const float* vel, float* out, const int* act) {
 // `lamh` holds lambda(t=1); on exit every level 0..nt is filled.  With
 // add_reg (no projection), bout receives the body force and is then expected
 // to be completed by an accumulating regularisation pass.
-int Solver::adjoint_sweep(float* bout, const int* act) {
+int Solver::adjoint_sweep(float* bout, const int* act, double hscale) {
+  const double hfac = hscale >= 0.0 ? hscale : (double)hd;
   const long long PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
   for (int j = 0; j < nt; ++j) {
     const int l = nt - j;  // lambda^{l-1} = c * lambda^l(X_adj)
@@ -787,14 +824,14 @@ int Solver::adjoint_sweep(float* bout, const int* act) {
     CB_TRY(prof_mark(CB_PROF_ADJOINT_STEP));
   }
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
-  CB_TRY(launch_body_force(lamh, PL, gm, PGM, bout, 3 * n, nt, ht, proj ? 1.f : hd, B, n, act, stream));
+  CB_TRY(launch_body_force(lamh, PL, gm, PGM, bout, 3 * n, nt, ht, proj ? 1.f : (float)hfac, B, n, act, stream));
   note_launches(nt + 1);
   if (proj) {
     CB_TRY(launch_r2c3d(bout, 3 * n, n, spec, 3 * nc, 3, B, d, act, stream));
     CB_TRY(launch_pencil(spec, 3 * nc, B, d, opts.model == CB_MODEL_STOKES ? OP_LERAY : OP_LERAY_RELAXED, dparams,
                          3, 3, act, stream));
     CB_TRY(launch_c2r3d(spec, 3 * nc, bout, 3 * n, n, 3, B, d, EPI_ADD, nullptr, nullptr, 0, act, stream));
-    CB_TRY(launch_lincomb(bout, 3 * n, bout, 3 * n, nullptr, (double)hd, nullptr, 0, nullptr, 0.0, 3 * n, B, act,
+    CB_TRY(launch_lincomb(bout, 3 * n, bout, 3 * n, nullptr, hfac, nullptr, 0, nullptr, 0.0, 3 * n, B, act,
                           stream));
     note_launches(6);
   }
@@ -846,7 +883,7 @@ int Solver::hessian_prep(const int* act) {
 // GN Hessian matvec (src/CLAIRE.cpp:1311-1379, 3147-3290, 3307-3490, 3849-4012).
 // m~^0 = 0, so m~^1 = s_0; steps j = 1 .. nt-1 gather; the last one writes
 // lambda~(t=1) = -m~(t=1) straight into the adjoint's level nt.
-int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) {
+int Solver::inc_state(const float* vin, const int* act) {
   const long long PGM = (nt + 1) * 3 * n, PGX = nt * 3 * n, PL = (nt + 1) * n, PS = nt * n;
   CB_TRY(launch_interp(vin, 3 * n, n, disp_st, 3 * n, tab_st, TP, vtx, 3 * n, n, 3, B, d, act, stream));
   CB_TRY(launch_incstate_source(gx, PGX, vtx, 3 * n, gm, PGM, vin, 3 * n, sj, PS, nt, ht, B, n, act, stream));
@@ -875,8 +912,31 @@ int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) 
   if (ncc) CB_TRY(ncc_inc_final_condition(lam_end, PL, act));
   // DistanceMeasureSL2::SetFinalConditionIAE with a mask: -w m~(1)
   else if (wmask) CB_TRY(launch_mulw(lam_end, PL, wmask, n, n, B, act, stream));
+  return 0;
+}
+
+int Solver::hessian(const float* vin, float* hout, const int* act, int pq_slot) {
+  CB_TRY(inc_state(vin, act));
   CB_TRY(finish_with_reg(vin, hout, act, pq_slot >= 0 ? vin : nullptr, pq_slot));
   return 0;
+}
+
+// Symmetrically preconditioned GN Hessian, CLAIRE::PrecondHessMatVecSym
+// (src/CLAIRE.cpp:1455-1532): hout = hd vin + P^1/2 b~[P^1/2 vin], with
+// P^1/2 = (beta A)^-1/2 (ApplyInverse, applysqrt) and b~ the incremental body
+// force (hd and the projection included).  mv_kind 2 divides by hd
+// (HessianMatVec with scale = false, src/CLAIRE.cpp:1279-1285): hd drops out
+// of the first term and the body force is formed with factor 1.
+int Solver::hessian_sym(const float* vin, float* hout, const int* act, int pq_slot) {
+  float* t = work3;  // P^1/2 vin
+  CB_TRY(reg_op(vin, t, OP_REG_SQRTINV, EPI_STORE, act));
+  CB_TRY(inc_state(t, act));
+  const bool unscaled = mv_kind == 2;
+  CB_TRY(adjoint_sweep(bf, act, unscaled ? 1.0 : (double)hd));
+  CB_TRY(launch_lincomb(hout, 3 * n, vin, 3 * n, nullptr, unscaled ? 1.0 : (double)hd, nullptr, 0, nullptr, 0.0,
+                        3 * n, B, act, stream));
+  note_launches(1);
+  return reg_op(bf, hout, OP_REG_SQRTINV, EPI_ADD, act, pq_slot >= 0 ? vin : nullptr, pq_slot);
 }
 
 // det(grad y) (inverse: det(grad(inv(y)))) of the selected problems at their
@@ -956,7 +1016,7 @@ int Solver::hessian_matvec(const float* vin, float* hout, const std::vector<int>
   CB_TRY(gradient_at_current(sel));  // state, adjoint trajectory and caches for v
   CB_TRY(upload_mask(sel, dact));
   CB_TRY(hessian_prep(dact));
-  CB_TRY(hessian(vin, hout, dact));
+  CB_TRY(apply_op(vin, hout, dact));
   if (cudaStreamSynchronize(stream) != cudaSuccess) return CB_ERR_CUDA;
   for (int b = 0; b < B; ++b)
     if (sel[b]) ps[b].hess_matvecs++;
@@ -964,6 +1024,22 @@ int Solver::hessian_matvec(const float* vin, float* hout, const std::vector<int>
 }
 
 int Solver::precond(const float* rin, float* zout, const std::vector<int>& sel) {
+  if (opts.precond == CB_PC_TWOLEVEL) {
+    // set up at the current velocity; coarse tolerance pctolscale * the
+    // Krylov relative tolerance (-krylovtol), as outside a GN solve
+    CB_TRY(gradient_at_current(sel));
+    CB_TRY(twolevel_setup(sel));
+    outer_rtol.assign(B, opts.krylovtol[0]);
+    if (rin != r &&
+        cudaMemcpyAsync(r, rin, sizeof(float) * 3 * n * B, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+    CB_TRY(upload_mask(sel, dact));
+    CB_TRY(twolevel_apply(sel, dact, S_RZ));
+    if (zout != z &&
+        cudaMemcpyAsync(zout, z, sizeof(float) * 3 * n * B, cudaMemcpyDeviceToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+    return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+  }
   CB_TRY(upload_mask(sel, dact));
   if (opts.precond) CB_TRY(reg_op(rin, zout, OP_REG_INV, EPI_STORE, dact));
   else CB_TRY(launch_lincomb(zout, 3 * n, rin, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact, stream));
@@ -1031,7 +1107,7 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   // clear when a problem stops), so it is recorded once as a CUDA graph and
   // replayed, and several iterations can run between host checks.
   auto body = [&]() -> int {
-    CB_TRY(hessian(pv, q, act, S_PQ));  // q = H p and p.q
+    CB_TRY(apply_op(pv, q, act, S_PQ));  // q = H p and p.q
     k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
     // x += alpha p, r -= alpha q and the new r.r in one pass
     CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
@@ -1095,6 +1171,206 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
     const bool stopped_at_check = reason == 1 || reason == 2 || reason == 4;
     ps[b].hess_matvecs += its + (reason == 3 ? 1 : 0);
     ps[b].pc_matvecs += 1 + its - (stopped_at_check ? 1 : 0);
+    ps[b].pcg_total += its;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Two-level preconditioner (-precond 2level: TWOLEVEL with PRECONDMATVECSYM,
+// src/RegOpt.cpp:602-606; src/Preconditioner.cpp:323-1176,
+// src/KrylovInterface.cpp:405-521).
+//
+// M r = L P y + (I - L) r with y the coarse solve of R L r, L the rectangular
+// low-pass filter of ApplyRectFreqFilter at pct = nc / n, R / P the spectral
+// restriction / prolongation.  For an even coarse size L keeps exactly the
+// band R carries (|k| <= nc/2 - 1 on every axis), so R L = R and L P = P, and
+// M r = r + P (y - R r): one restriction and one prolongation per application.
+// ---------------------------------------------------------------------------
+int Solver::ensure_wmask() {
+  if (wmask) return 0;
+  CB_TRY(alloc((void**)&wmask, sizeof(float) * n * B));
+  CB_TRY(launch_fill(wmask, n, 1.f, n, B, nullptr, stream));
+  return 0;
+}
+
+// CLAIRE::SetStateVariable / SetAdjointVariable (src/CLAIRE.cpp:599-725): both
+// characteristics from the (restricted) velocity; then the caches the GN
+// Hessian reads: grad m^j, div v, the adjoint step factor, (grad m^j)(X).
+int Solver::prepare_from_state(const int* act) {
+  CB_TRY(characteristic(v, 1.f, act));
+  CB_TRY(characteristic(v, -1.f, act));
+  CB_TRY(image_grad(act));
+  CB_TRY(divergence(v, divv, act));
+  CB_TRY(launch_adjoint_coef(divv, n, disp_adj, 3 * n, tab_adj, TP, cadj, n, ht, B, d, act, stream));
+  note_launches(1);
+  return hessian_prep(act);
+}
+
+int Solver::inner_solve(const std::vector<int>& sel, const std::vector<double>& rtol, int maxit) {
+  if (cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream) !=
+      cudaSuccess)
+    return CB_ERR_CUDA;
+  return pcg(sel, maxit);
+}
+
+// Preconditioner::SetupCoarseGrid + ApplyRestriction (src/Preconditioner.cpp:
+// 353-499, 676-831): coarse problems with every option of the fine ones but
+// the grid; velocity, the nt+1 state levels (restricted, not re-solved) and
+// the mask restricted from the selected problems' current ones; the current
+// regularisation weights handed down.
+int Solver::twolevel_setup(const std::vector<int>& sel) {
+  if (!coarse) {
+    coarse.reset(new (std::nothrow) Solver());
+    if (!coarse) return CB_ERR_ALLOC;
+    if (int e = coarse->init(coarse_opts(opts), B)) {
+      err = "two-level preconditioner, coarse grid: " + coarse->err;
+      coarse.reset();
+      return e;
+    }
+    coarse->mv_kind = 2;
+    coarse->graphs = graphs;
+    if (wmask) CB_TRY(coarse->ensure_wmask());
+  }
+  Solver& c = *coarse;
+  c.stream = stream;
+  const long long need = grid_change_work(d.n1, nc1, std::max(3, nt + 1));
+  if (gwork_floats < need) {
+    if (gwork) {
+      cudaFree(gwork);
+      bytes_ -= (long long)sizeof(float) * gwork_floats;
+      gwork = nullptr;
+      gwork_floats = 0;
+    }
+    CB_TRY(alloc((void**)&gwork, sizeof(float) * need));
+    gwork_floats = need;
+  }
+  const long long cn = c.n, PM = (nt + 1) * n, PMc = (nt + 1) * cn;
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    c.ps[b].norm = ps[b].norm;
+    c.ps[b].beta0 = ps[b].beta0;
+    c.ps[b].beta1 = ps[b].beta1;
+    c.ps[b].beta2 = ps[b].beta2;
+    if (launch_grid_change(v + b * 3 * n, n, d.n1, c.v + b * 3 * cn, cn, nc1, 3, gwork, stream) ||
+        launch_grid_change(m + b * PM, n, d.n1, c.m + b * PMc, cn, nc1, nt + 1, gwork, stream) ||
+        (wmask && launch_grid_change(wmask + b * n, n, d.n1, c.wmask + b * cn, cn, nc1, 1, gwork, stream)))
+      return CB_ERR_CUDA;
+    c.state_of[b] = 0;
+  }
+  note_launches(9);
+  CB_TRY(c.upload_params());
+  CB_TRY(c.upload_mask(sel, c.dact));
+  return c.prepare_from_state(c.dact);
+}
+
+// Preconditioner::Apply2LevelPrecond (src/Preconditioner.cpp:584-673) on r,
+// result in z.  The coarse solve is KSPCG without a preconditioner, zero
+// initial guess, on the symmetric coarse operator divided by hd, with
+// rtol = pctolscale * the outer forcing value in [1e-16, 1/2], atol 1e-16,
+// dtol 1e6 and at most 1000 iterations (InvertPrecondPreKrylovSolve,
+// src/KrylovInterface.cpp:430-521; SetupKrylovMethod, src/Preconditioner.cpp:
+// 842-945).  Each coarse Hessian application counts as a preconditioner
+// matvec (src/Preconditioner.cpp:980).
+int Solver::twolevel_apply(const std::vector<int>& sel, const int* act, int rz_slot) {
+  Solver& c = *coarse;
+  const long long cn = c.n;
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && launch_grid_change(r + b * 3 * n, n, d.n1, c.g + b * 3 * cn, cn, nc1, 3, gwork, stream))
+      return CB_ERR_CUDA;
+  // the coarse PCG starts from r = -g: g = -R r
+  CB_TRY(c.upload_mask(sel, c.dact));
+  CB_TRY(launch_lincomb(c.g, 3 * cn, c.g, 3 * cn, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * cn, B, c.dact,
+                        stream));
+  std::vector<double> rt(B, 0.5);
+  std::vector<int> before(B, 0);
+  for (int b = 0; b < B; ++b) {
+    const double outer = b < (int)outer_rtol.size() ? outer_rtol[b] : opts.krylovtol[0];
+    rt[b] = std::max(1e-16, std::min(0.5, opts.pctolscale * outer));
+    before[b] = c.ps[b].hess_matvecs;
+  }
+  CB_TRY(c.inner_solve(sel, rt, 1000));
+  // y - R r = x + g, prolonged; z = r + P (y - R r)
+  CB_TRY(c.upload_mask(sel, c.dact));
+  CB_TRY(launch_lincomb(c.x, 3 * cn, c.x, 3 * cn, nullptr, 1.0, c.g, 3 * cn, nullptr, 1.0, 3 * cn, B, c.dact,
+                        stream));
+  for (int b = 0; b < B; ++b)
+    if (sel[b] && launch_grid_change(c.x + b * 3 * cn, cn, nc1, z + b * 3 * n, n, d.n1, 3, gwork, stream))
+      return CB_ERR_CUDA;
+  CB_TRY(launch_lincomb(z, 3 * n, z, 3 * n, nullptr, 1.0, r, 3 * n, nullptr, 1.0, 3 * n, B, act, stream));
+  note_launches(9);
+  CB_TRY(dot(r, 3 * n, z, 3 * n, 3 * n, rz_slot, act));
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) {
+      ps[b].pc_matvecs += c.ps[b].hess_matvecs - before[b];
+      if (opts.verbosity > 0)
+        std::fprintf(stderr, "[claire_b200] p%d two-level coarse solve: %d iterations (rtol %.3e)\n", b,
+                     c.ps[b].hess_matvecs - before[b], rt[b]);
+    }
+  return 0;
+}
+
+// KSPCG on the symmetrically preconditioned Hessian with the two-level
+// preconditioner.  The iteration is pcg()'s; the preconditioner runs a nested
+// Krylov solve driven from the host, so these iterations are direct launches
+// with the active set read back before every preconditioner application.
+int Solver::pcg_twolevel(const std::vector<int>& sel, double maxit_d) {
+  const int maxit = (int)maxit_d;
+  int* act = dact2;
+  CB_TRY(upload_mask(sel, act));
+  // PreKrylovSolve (src/KrylovInterface.cpp:79-196, src/CLAIREBase.cpp:936-952):
+  // the right-hand side is the optimiser's gradient vector itself and becomes
+  // P^1/2 g in place (the forcing value was taken from ||g|| before)
+  CB_TRY(reg_op(g, g, OP_REG_SQRTINV, EPI_STORE, act));
+  CB_TRY(launch_lincomb(r, 3 * n, g, 3 * n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+  CB_TRY(launch_lincomb(x, 3 * n, g, 3 * n, nullptr, 0.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+  note_launches(2);
+  CB_TRY(dot(r, 3 * n, r, 3 * n, 3 * n, S_RR, act));
+  k_pcg_init<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, opts.krylovtol[1]);
+  note_launches(1);
+  // DoSetup at the first preconditioner application of every GN iteration
+  // (src/KrylovInterface.cpp:444-447, reset by src/TaoInterface.cpp:546)
+  CB_TRY(twolevel_setup(sel));
+  std::vector<int> hact(B, 0);
+  bool any = false;
+  auto read_active = [&]() -> int {
+    cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+      err = "device error in PCG";
+      return CB_ERR_CUDA;
+    }
+    any = false;
+    for (int b = 0; b < B; ++b) any |= hact[b] != 0;
+    return 0;
+  };
+  CB_TRY(read_active());
+  if (any) {
+    CB_TRY(twolevel_apply(hact, act, S_RZ));
+    CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
+    note_launches(1);
+  }
+  for (int it = 0; it < maxit && any; ++it) {
+    CB_TRY(apply_op(pv, q, act, S_PQ));  // q = A p and p.q
+    k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
+    CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
+    CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(S_RR), B, 1.0, false, stream, act));
+    k_pcg_check<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B, maxit, opts.krylovtol[2]);
+    note_launches(4);
+    CB_TRY(read_active());
+    if (!any) break;
+    CB_TRY(twolevel_apply(hact, act, S_RZNEW));
+    k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
+    CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
+    note_launches(2);
+  }
+  // PostKrylovSolve (src/CLAIREBase.cpp:958-972): x <- P^1/2 x
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(reg_op(x, x, OP_REG_SQRTINV, EPI_STORE, dact));
+  CB_TRY(fetch_scalars());
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    const int its = hint[I_IT * B + b], reason = hint[I_REASON * B + b];
+    ps[b].hess_matvecs += its + (reason == 3 ? 1 : 0);
     ps[b].pcg_total += its;
   }
   return 0;
@@ -1278,9 +1554,11 @@ int Solver::step(std::vector<int>& finished, double gttol, int miniter) {
     }
   }
   cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+  outer_rtol = rtol;
   CB_TRY(upload_mask(act, dact));
   CB_TRY(hessian_prep(dact));
-  CB_TRY(pcg(act, std::max(0, opts.krylovmaxit - 1)));
+  if (opts.precond == CB_PC_TWOLEVEL) CB_TRY(pcg_twolevel(act, std::max(0, opts.krylovmaxit - 1)));
+  else CB_TRY(pcg(act, std::max(0, opts.krylovmaxit - 1)));
   std::vector<int> acc = act;
   CB_TRY(line_search(acc));
   bool anyacc = false;

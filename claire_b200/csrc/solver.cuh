@@ -8,6 +8,7 @@
 #pragma once
 
 #include <chrono>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -129,6 +130,31 @@ class Solver {
     if (b >= 0 && b < (int)ncc_scale_ok.size()) ncc_scale_ok[b] = 0;
   }
 
+  // ---- two-level preconditioner (-precond 2level) --------------------------
+  // Hessian operator of the Krylov solve: 0 the GN Hessian (DEFAULTMATVEC),
+  // 1 its symmetrically preconditioned form hd x + P^1/2 b~[P^1/2 x]
+  // (PRECONDMATVECSYM), 2 that form divided by hd (the coarse operator).
+  int mv_kind = 0;
+  // coarse-grid problems (same batch layout), created by the first setup
+  std::unique_ptr<Solver> coarse;
+  int nc1 = 0;                 // coarse points per axis, ceil(n1 / gridscale)
+  float* gwork = nullptr;      // grid-change workspace
+  long long gwork_floats = 0;
+  std::vector<double> outer_rtol;  // forcing value of the current Krylov solve, per problem
+  // DoSetup / ApplyRestriction: coarse velocity, state levels and mask from
+  // the selected problems' current ones; coarse trajectories and caches
+  int twolevel_setup(const std::vector<int>& sel);
+  // Apply2LevelPrecond: z = M r and r.z into slot rz_slot for the problems in
+  // sel (act: the same set on the device)
+  int twolevel_apply(const std::vector<int>& sel, const int* act, int rz_slot);
+  // coarse side: trajectories, grad m levels and the Hessian caches from the
+  // velocity and state levels already in v and m
+  int prepare_from_state(const int* act);
+  // coarse side: CG on the operator mv_kind with rhs -g, no preconditioner,
+  // per-problem relative tolerances; the solution lands in x
+  int inner_solve(const std::vector<int>& sel, const std::vector<double>& rtol, int maxit);
+  int ensure_wmask();
+
   // PCG iteration recorded as a CUDA graph (built on the second iteration the
   // solver runs; graphs = false switches replay off)
   bool graphs = true, pcg_warm = false;
@@ -179,13 +205,22 @@ class Solver {
                   long long ofs, int nf, const int* act);
   int divergence(const float* vel, float* out, const int* act);
   int div_penalty(const float* vel, const int* act);
-  int adjoint_sweep(float* bout, const int* act);
+  // hscale >= 0 replaces hd as the body force's final factor
+  int adjoint_sweep(float* bout, const int* act, double hscale = -1.0);
   int finish_with_reg(const float* vin, float* out, const int* act, const float* dot_with = nullptr,
                       int dot_slot = -1);
   int gradient(const int* act);
   int hessian_prep(const int* act);
+  // incremental state and adjoint final condition for vin (everything of the
+  // Hessian matvec before the incremental adjoint sweep)
+  int inc_state(const float* vin, const int* act);
   int hessian(const float* vin, float* hout, const int* act, int pq_slot = -1);
+  int hessian_sym(const float* vin, float* hout, const int* act, int pq_slot = -1);
+  int apply_op(const float* vin, float* hout, const int* act, int pq_slot = -1) {
+    return mv_kind ? hessian_sym(vin, hout, act, pq_slot) : hessian(vin, hout, act, pq_slot);
+  }
   int pcg(const std::vector<int>& sel, double maxit);
+  int pcg_twolevel(const std::vector<int>& sel, double maxit);
   int line_search(std::vector<int>& sel);
   int dot(const float* a, long long ap, const float* b, long long bp, long long len, int slot,
           const int* act, double scale = 1.0);

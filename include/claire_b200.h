@@ -42,6 +42,9 @@ enum { CB_MODEL_COMPRESSIBLE = 0, CB_MODEL_STOKES = 1, CB_MODEL_RELAXEDSTOKES = 
 enum { CB_DIST_SL2 = 0, CB_DIST_NCC = 1 };
 /* Krylov forcing sequences (-krylovfseq). */
 enum { CB_FSEQ_NONE = 0, CB_FSEQ_QUADRATIC = 1, CB_FSEQ_SUPERLINEAR = 2 };
+/* Preconditioners (-precond): none, inverse regularisation, two-level
+ * (coarse-grid solve of the symmetrically preconditioned Hessian). */
+enum { CB_PC_NONE = 0, CB_PC_INVREG = 1, CB_PC_TWOLEVEL = 2 };
 /* Regularisation operator kinds for claire_b200_reg_apply. */
 enum { CB_REG_GRADIENT = 0, CB_REG_INVERSE = 1, CB_REG_SQRTINVERSE = 2 };
 
@@ -61,7 +64,7 @@ typedef struct claire_b200_opts {
   int krylovmaxit;      /* -krylovmaxit (50); PCG runs krylovmaxit-1 iterations */
   double krylovtol[3];  /* rtol 1e-12, atol 1e-16, dtol 1e6 */
   int krylovfseq;       /* -krylovfseq (CB_FSEQ_SUPERLINEAR) */
-  int precond;          /* 1: inverse regularisation (INVREG), 0: none */
+  int precond;          /* -precond: CB_PC_INVREG (default), CB_PC_NONE, CB_PC_TWOLEVEL */
   int iporder;          /* -iporder: 3 (tricubic) is the only order on this path */
   int verbosity;        /* -verbosity */
   int bf16_images;      /* store transported images in bf16 (gathers accumulate in fp32) */
@@ -77,6 +80,11 @@ typedef struct claire_b200_opts {
   double betainit;      /* -betainit: first beta of -train and -betacont searches (1.0) */
   int monitordefgrad;   /* -monitordefgrad: check det(grad y) against -jbound after the solve and
                            raise beta toward 10 beta while it is breached (RunSolver) */
+  double pcgridscale;   /* -gridscale: coarse grid of the two-level preconditioner, ceil(nx / 2) */
+  double pctolscale;    /* -pctolscale: coarse solve tolerance = pctolscale * forcing value (0.1) */
+  int pcsolvermaxit;    /* -pcsolvermaxit (10): iterations of a flexible outer solver's coarse
+                           solve; the PCG outer solver used here runs the coarse solve to its
+                           tolerance (at most 1000 iterations) */
 } claire_b200_opts;
 
 typedef struct claire_b200_stats {

@@ -676,6 +676,21 @@ class Problem:
         self.counters["pcmatvec"] += 1
         return self.reg.apply_inverse(np.asarray(x, dtype=self.dtype)).astype(self.dtype)
 
+    def hessian_sym(self, vt, scale: bool = True) -> np.ndarray:
+        """Symmetrically preconditioned GN Hessian, CLAIRE::PrecondHessMatVecSym
+        (src/CLAIRE.cpp:1455-1532): hd vt + P^1/2 b~[P^1/2 vt] with
+        P^1/2 = (beta A)^-1/2 (ApplyInverse with applysqrt) and b~ the
+        incremental body force (hd and the model's projection included).
+        scale=False divides the result by hd (CLAIRE::HessianMatVec with
+        scale = false, src/CLAIRE.cpp:1279-1285), as the two-level
+        preconditioner's coarse operator does (src/Preconditioner.cpp:963-978)."""
+        vt = np.asarray(vt, dtype=self.dtype)
+        t = self.reg.apply_inverse(vt, applysqrt=True).astype(self.dtype)
+        bt = self.inc_body_force(self.inc_state(t))
+        out = (self.hd * vt + self.reg.apply_inverse(bt, applysqrt=True)).astype(self.dtype)
+        self.counters["hessmatvec"] += 1
+        return out if scale else (out / self.hd).astype(self.dtype)
+
 
 # --------------------------------------------------------------------------
 # Krylov + Gauss-Newton loop
@@ -748,6 +763,9 @@ class GNOptions:
     ls_sigma: float = 1e-4
     ls_max_trials: int = 30
     min_step: float = 2.0 ** -10
+    precond: str = "invreg"   # -precond invreg | 2level
+    pcgridscale: float = 2.0  # -gridscale (src/RegOpt.cpp:1124)
+    pctolscale: float = 1e-1  # -pctolscale (src/RegOpt.cpp:1121)
 
 
 def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None, g0=None, krylov_g0=None,
@@ -800,13 +818,28 @@ def gauss_newton(prob: Problem, opts: GNOptions = GNOptions(), v0=None, log=None
         if krylov_g0 is None:
             krylov_g0 = gnorm
         rtol = forcing_tolerance(gnorm, krylov_g0, opts.fseq)
-        d, kit, _ = pcg(prob.hessian_matvec, prob.precond, (-g).astype(prob.dtype), rtol,
-                        maxit=max(0, opts.krylov_maxit - 1))
+        gls = g  # the gradient the descent test and the line search see
+        if opts.precond == "2level":
+            # PreKrylovSolve applies P^1/2 to the right-hand side in place
+            # (src/CLAIREBase.cpp:936-952); that vector is the optimiser's
+            # gradient, so the line search below sees P^1/2 g.  The operator
+            # is PrecondHessMatVecSym, the preconditioner the two-level one
+            # (set up once per iteration, src/TaoInterface.cpp:546), and
+            # PostKrylovSolve maps the solution back (:958-972).
+            gls = prob.reg.apply_inverse(g, applysqrt=True).astype(prob.dtype)
+            coarse = two_level_setup(prob, opts.pcgridscale)
+            inner = max(1e-16, min(0.5, opts.pctolscale * rtol))
+            xh, kit, _ = pcg(prob.hessian_sym, lambda r: two_level_apply(coarse, r, inner),
+                             (-gls).astype(prob.dtype), rtol, maxit=max(0, opts.krylov_maxit - 1))
+            d = prob.reg.apply_inverse(xh, applysqrt=True).astype(prob.dtype)
+        else:
+            d, kit, _ = pcg(prob.hessian_matvec, prob.precond, (-g).astype(prob.dtype), rtol,
+                            maxit=max(0, opts.krylov_maxit - 1))
         pcg_iters.append(kit)
-        gd = dot(g, d)
+        gd = dot(gls, d)
         if not (gd < 0.0):
-            d = (-g).astype(prob.dtype)
-            gd = -gnorm * gnorm
+            d = (-gls).astype(prob.dtype)
+            gd = -dot(gls, gls)
         alpha = 1.0
         accepted = False
         for _ in range(opts.ls_max_trials):
@@ -885,6 +918,65 @@ def grid_transfer(f: np.ndarray, nt: int) -> np.ndarray:
     out = np.zeros((nt, nt, nt), dtype=complex)
     out[np.ix_(dst, dst, dst)] = fh[np.ix_(src, src, src)] / float(ns) ** 3
     return np.real(np.fft.ifftn(out)) * float(nt) ** 3
+
+
+def rect_freq_filter(f: np.ndarray, pct: float, lowpass: bool = True) -> np.ndarray:
+    """Preprocessing::ApplyRectFreqFilter (src/Preprocessing.cpp:1812-1913):
+    keep (lowpass) or drop (highpass) the coefficients whose index w on every
+    axis of the r2c spectrum satisfies w < pct (N/2 - 1) or w > N - pct N/2."""
+    f = np.asarray(f, np.float64)
+    if pct == 1.0:
+        return f.copy() if lowpass else np.zeros_like(f)
+    shape = f.shape
+    fh = np.fft.rfftn(f)
+    inside = np.ones(fh.shape, dtype=bool)
+    for ax, n in enumerate(shape):
+        w = np.arange(fh.shape[ax])
+        keep = (w < pct * (n / 2.0 - 1.0)) | (w > n - pct * (n / 2.0))
+        sh = [1, 1, 1]
+        sh[ax] = -1
+        inside &= keep.reshape(sh)
+    fh = np.where(inside if lowpass else ~inside, fh, 0.0)
+    return np.fft.irfftn(fh, s=shape, axes=(0, 1, 2))
+
+
+def two_level_setup(prob: Problem, gridscale: float = 2.0) -> Problem:
+    """Preconditioner::SetupCoarseGrid + ApplyRestriction
+    (src/Preconditioner.cpp:353-499, 676-831): a problem on ceil(N/gridscale)
+    points per axis whose velocity, state levels (all nt+1, not re-solved),
+    images and mask are the restrictions of the fine problem's at its current
+    velocity; its trajectories follow from the restricted velocity
+    (CLAIRE::SetStateVariable / SetAdjointVariable)."""
+    m = prob.solve_state()
+    nf = prob.shape[0]
+    nc = int(math.ceil(nf / gridscale))
+    cp = Problem(grid_transfer(prob.mR, nc), grid_transfer(prob.mT, nc), prob.nt, prob.reg,
+                 projection=prob.projection, mask=None if prob.mask is None else grid_transfer(prob.mask, nc))
+    cp.beta_w = prob.beta_w
+    cp.set_velocity(np.stack([grid_transfer(prob.v[k], nc) for k in range(3)]))
+    cp.m = np.stack([grid_transfer(m[j], nc) for j in range(prob.nt + 1)])
+    cp.fine_n = nf
+    return cp
+
+
+def two_level_apply(coarse: Problem, r: np.ndarray, rtol: float, maxit: int = 1000):
+    """Preconditioner::Apply2LevelPrecond (src/Preconditioner.cpp:584-673):
+    low-pass filter, restrict, solve with the coarse operator (KSPCG, no
+    preconditioner, zero guess, rtol = pctolscale * the outer forcing value,
+    atol 1e-16, at most 1000 iterations: src/KrylovInterface.cpp:430-521,
+    src/Preconditioner.cpp:842-945), prolong, low-pass filter, and add the
+    high-pass part of the input."""
+    nf = coarse.fine_n
+    nc = coarse.shape[0]
+    pct = nc / nf
+    low = np.stack([rect_freq_filter(r[k], pct) for k in range(3)])
+    rc = np.stack([grid_transfer(low[k], nc) for k in range(3)])
+    y, its, _ = pcg(lambda x: coarse.hessian_sym(x, scale=False), lambda x: x, rc, rtol, atol=1e-16,
+                    maxit=maxit)
+    coarse.inner_iters = getattr(coarse, "inner_iters", 0) + its
+    yp = np.stack([grid_transfer(y[k], nf) for k in range(3)])
+    out = np.stack([rect_freq_filter(yp[k], pct) + rect_freq_filter(r[k], pct, lowpass=False) for k in range(3)])
+    return out.astype(r.dtype)
 
 
 def grid_levels(n: int):

@@ -92,3 +92,26 @@ def test_parse_betacont():
     o = cb.RegOpt(["-nx", "32", "-betacont", "1e-4"]).opts
     assert o.betacont == 1e-4 and o.presolvetol == 1e-1
     assert cb.RegOpt().opts.betacont == 0.0
+
+
+def test_parse_two_level_preconditioner():
+    # src/RegOpt.cpp:592-650 and the defaults of :1120-1124
+    import claire_b200 as cb
+    d = cb.RegOpt().opts
+    assert d.pcgridscale == 2.0 and d.pctolscale == 0.1 and d.pcsolvermaxit == 10
+    o = cb.RegOpt(["-nx", "64", "-precond", "2level", "-gridscale", "4", "-pctolscale", "0.05",
+                   "-pcsolvermaxit", "5", "-pcsolver", "pcg", "-monitorpcsolver"]).opts
+    assert o.precond == 2 and o.pcgridscale == 4.0 and o.pctolscale == 0.05 and o.pcsolvermaxit == 5
+    assert cb.RegOpt(["-precond", "none"]).opts.precond == 0
+    for bad in (["-precond", "amg"], ["-pctolscale", "1.5"], ["-gridscale", "0.5"]):
+        with pytest.raises(cb.ClaireError) as e:
+            cb.RegOpt(bad)
+        assert e.value.code == -1
+    for other in ("gmres", "fgmres", "fpcg", "cheb"):
+        with pytest.raises(cb.ClaireError) as e:
+            cb.RegOpt(["-pcsolver", other])
+        assert e.value.code == -6  # flexible / Chebyshev coarse solvers are not on this path
+    # the coarse problems and the grid-change workspace are part of the footprint
+    a = cb.RegOpt(["-nx", "64", "-nt", "4"]).estimate_bytes(2)
+    b = cb.RegOpt(["-nx", "64", "-nt", "4", "-precond", "2level"]).estimate_bytes(2)
+    assert 1.1 * a < b < 1.5 * a
