@@ -150,11 +150,17 @@ int claire_b200_forward(claire_b200_ctx* ctx, int b, const float* m0, float* m1,
 int claire_b200_get_stats(const claire_b200_ctx* ctx, int b, claire_b200_stats* stats);
 /* Objective J(v), gradient g(v) and GN Hessian matvec H*vt at velocity v for
  * problem b (OptimizationProblem::{EvaluateObjective, EvaluateGradient,
- * HessianMatVec}, include/OptimizationProblem.hpp:51-121).  Host pointers. */
+ * HessianMatVec}, include/OptimizationProblem.hpp:51-121).  Host pointers.
+ * With -precond 2level the matvec is the Krylov operator of that mode,
+ * hd vt + P^1/2 b~[P^1/2 vt] (CLAIRE::PrecondHessMatVecSym,
+ * src/CLAIRE.cpp:1455-1532). */
 int claire_b200_objective(claire_b200_ctx* ctx, int b, const float* v, double* J, double* D, double* R);
 int claire_b200_gradient(claire_b200_ctx* ctx, int b, const float* v, float* g);
 int claire_b200_hessian_matvec(claire_b200_ctx* ctx, int b, const float* v, const float* vt, float* hvt);
-/* Preconditioner::MatVec (INVREG): P x = (beta A)^-1 x (src/Preconditioner.cpp:549-580). */
+/* Preconditioner::MatVec (src/Preconditioner.cpp:507-580): INVREG
+ * P x = (beta A)^-1 x; with -precond 2level Apply2LevelPrecond (:584-673),
+ * set up at the problem's current velocity, coarse tolerance
+ * pctolscale * krylovtol[0]. */
 int claire_b200_precond(claire_b200_ctx* ctx, int b, const float* x, float* px);
 /* det(grad y) of problem b at its current velocity (inverse != 0:
  * det(grad(inv(y)))), DeformationFields::ComputeDetDefGrad with the SL solver

@@ -6,12 +6,16 @@
 * tests/golden/c3_64.json: a 64^3 problem of the ellipsoid / random-velocity
   recipe (seeded problem 0 of the mixed-batch set), nt = 4, H1 beta = 1e-2;
 
-both with GN + PCG (INVREG, superlinear forcing) + Armijo, gradient tolerance
-1e-2, at most 10 GN iterations.  Too slow for a test run (NumPy), so the
-results are committed: iteration counts, monitor values and velocity
+* tests/golden/c1_64_2level.json: the c1 problem solved with the two-level
+  preconditioner (-precond 2level: symmetric preconditioned Hessian, coarse
+  solve on 32^3);
+
+all with GN + PCG (superlinear forcing) + Armijo, gradient tolerance 1e-2, at
+most 10 GN iterations, INVREG unless named.  Too slow for a test run (NumPy),
+so the results are committed: iteration counts, monitor values and velocity
 projections onto seeded random fields.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture.json ...]
 """
 import json
 import os
@@ -45,17 +49,17 @@ def c3_images(n, nt):
     return mR, mT, "oracle ellipsoid template and random velocity, seed problem_seed(2, 0), cast to float32"
 
 
-def make(name, images, n, nt, norm, beta, maxit=10, gttol=1e-2):
+def make(name, images, n, nt, norm, beta, maxit=10, gttol=1e-2, precond="invreg"):
     mR, mT, what = images(n, nt)
     mR = mR.astype(np.float32)
     mT = mT.astype(np.float32)
     prob = R.Problem(mR, mT, nt, R.Regularization(norm, beta))
     t = time.time()
-    res = R.gauss_newton(prob, R.GNOptions(maxit=maxit, gttol=gttol))
+    res = R.gauss_newton(prob, R.GNOptions(maxit=maxit, gttol=gttol, precond=precond))
     v = res["v"]
     out = {
         "problem": {"n": n, "nt": nt, "regnorm": norm, "beta": beta, "maxit": maxit, "opttol": gttol,
-                    "images": what},
+                    "precond": precond, "images": what},
         "gn_iterations": res["iters"],
         "pcg_iterations": res["pcg_iters"],
         "reason": res["reason"],
@@ -72,9 +76,16 @@ def make(name, images, n, nt, norm, beta, maxit=10, gttol=1e-2):
     print(name, json.dumps(out))
 
 
+FIXTURES = {
+    "c1_64.json": lambda: make("c1_64.json", c1_images, 64, 4, "h1s", 1e-2),
+    "c3_64.json": lambda: make("c3_64.json", c3_images, 64, 4, "h1", 1e-2),
+    "c1_64_2level.json": lambda: make("c1_64_2level.json", c1_images, 64, 4, "h1s", 1e-2, precond="2level"),
+}
+
+
 def main():
-    make("c1_64.json", c1_images, 64, 4, "h1s", 1e-2)
-    make("c3_64.json", c3_images, 64, 4, "h1", 1e-2)
+    for name in sys.argv[1:] or list(FIXTURES):
+        FIXTURES[name]()
 
 
 if __name__ == "__main__":

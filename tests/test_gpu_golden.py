@@ -7,7 +7,9 @@ committed in tests/golden/ (made by tests/golden/make_golden.py):
   velocity within 1e-4;
 * c3_64: an ellipsoid / random-velocity problem with H1 (beta1 = 1e-4 makes
   the inverse symbol 1e6 at k = 0, so PCG counts follow FP32 roundoff): GN
-  count within one, objective, mismatch and velocity within 1e-3.
+  count within one, objective, mismatch and velocity within 1e-3;
+* c1_64_2level: c1 with the two-level preconditioner (coarse solve on 32^3):
+  as c1, at 1e-3.
 """
 import json
 import os
@@ -48,13 +50,15 @@ def c3_images(p):
 
 
 @pytest.mark.parametrize("name,images,tol,exact_pcg", [("c1_64.json", c1_images, 1e-4, True),
-                                                       ("c3_64.json", c3_images, 1e-3, False)])
+                                                       ("c3_64.json", c3_images, 1e-3, False),
+                                                       ("c1_64_2level.json", c1_images, 1e-3, True)])
 def test_registration_matches_golden(cb, name, images, tol, exact_pcg):
     g = json.load(open(os.path.join(HERE, "golden", name)))
     p = g["problem"]
     mR, mT = images(p)
     opt = cb.RegOpt(["-nx", str(p["n"]), "-nt", str(p["nt"]), "-regnorm", p["regnorm"], "-beta", str(p["beta"]),
-                     "-maxit", str(p["maxit"]), "-opttol", str(p["opttol"])])
+                     "-maxit", str(p["maxit"]), "-opttol", str(p["opttol"]),
+                     "-precond", p.get("precond", "invreg")])
     with cb.CLAIREInterface(opt) as ci:
         ci.set_images(mR.astype(np.float32), mT.astype(np.float32))
         ci.Run()
