@@ -92,6 +92,41 @@ int launch_cg_update(float* x, float* r, const float* p, const float* q, long lo
   return (int)cudaGetLastError();
 }
 
+// y = a + b and partial sums of y.c (y may be a)
+__global__ void __launch_bounds__(kRedThreads) k_add_dot4(float4* y, const float4* a, const float4* __restrict__ b,
+                                                           const float4* __restrict__ c, long long vp,
+                                                           long long len4, double* __restrict__ partials,
+                                                           int nparts, const int* __restrict__ active) {
+  const int pb = blockIdx.y;
+  if (active && !active[pb]) return;
+  float4* py = y + pb * vp;
+  const float4* pa = a + pb * vp;
+  const float4* pbv = b + pb * vp;
+  const float4* pc = c + pb * vp;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len4;
+       i += (long long)gridDim.x * blockDim.x) {
+    float4 v = pa[i];
+    const float4 w = __ldg(pbv + i), cv = __ldg(pc + i);
+    v.x += w.x; v.y += w.y; v.z += w.z; v.w += w.w;
+    py[i] = v;
+    acc += (double)v.x * (double)cv.x + (double)v.y * (double)cv.y + (double)v.z * (double)cv.z +
+           (double)v.w * (double)cv.w;
+  }
+  block_reduce_store(acc, partials + (long long)pb * nparts, blockIdx.x);
+}
+
+int launch_add_dot(float* y, const float* a, const float* b, const float* c, long long vp, long long len, int nprob,
+                   double* partials, int stride, const int* active, cudaStream_t s) {
+  if ((len & 3) || (vp & 3) || !aligned16(y) || !aligned16(a) || !aligned16(b) || !aligned16(c))
+    return (int)cudaErrorInvalidValue;
+  dim3 grid(dot_partials(len), nprob);
+  k_add_dot4<<<grid, kRedThreads, 0, s>>>(reinterpret_cast<float4*>(y), reinterpret_cast<const float4*>(a),
+                                           reinterpret_cast<const float4*>(b), reinterpret_cast<const float4*>(c),
+                                           vp / 4, len / 4, partials, stride, active);
+  return (int)cudaGetLastError();
+}
+
 __global__ void __launch_bounds__(kRedThreads) k_diff_sumsq(const float* __restrict__ a, long long ap,
                                                              const float* __restrict__ b, long long bp,
                                                              long long len, double* __restrict__ partials,

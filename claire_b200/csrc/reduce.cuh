@@ -54,6 +54,9 @@ int launch_dot(const float* a, long long ap, const float* b, long long bp, long 
 int launch_cg_update(float* x, float* r, const float* p, const float* q, long long vp, long long len,
                      const double* alpha, int nprob, double* partials, int stride, const int* active,
                      cudaStream_t s);
+// y = a + b and partial sums of y.c per problem (vectors vp apart; y may be a)
+int launch_add_dot(float* y, const float* a, const float* b, const float* c, long long vp, long long len, int nprob,
+                   double* partials, int stride, const int* active, cudaStream_t s);
 
 // y[p][i] = value, i < len
 int launch_fill(float* y, long long yp, float value, long long len, int nprob, const int* active, cudaStream_t s);

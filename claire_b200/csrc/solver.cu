@@ -123,6 +123,16 @@ __global__ void k_pcg_beta(double* __restrict__ sc, int* __restrict__ act, int B
   sc[Solver::S_RZ * B + p] = rzn;
 }
 
+// a1 = act and flag, a0 = act and not flag
+__global__ void k_split_mask(const int* __restrict__ act, const int* __restrict__ flag, int* __restrict__ a1,
+                             int* __restrict__ a0, int B) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= B) return;
+  const int a = act[p] != 0, f = flag[p] != 0;
+  a1[p] = a && f;
+  a0[p] = a && !f;
+}
+
 static dim3 pgrid(int B) { return dim3((B + 127) / 128); }
 
 // ---------------------------------------------------------------------------
@@ -133,7 +143,7 @@ Solver::~Solver() {
   prof_clear();
   if (pcg_exec) cudaGraphExecDestroy(pcg_exec);
   void* ptrs[] = {mR, mT, m, mR16, mT16, m16, wmask, v, vtrial, disp_st, disp_adj, tab_st, tab_adj, gm, gx, divv, cadj, lamh, bf, g, x,
-                  r, z, pv, q, vtx, mt, mt2, sj, work3, spec, partials, dsc, dact, dint, dparams, gwork};
+                  r, z, pv, q, vtx, mt, mt2, sj, work3, sreg, spec, partials, dsc, dact, dint, dparams, gwork};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (hsc) cudaFreeHost(hsc);
@@ -185,7 +195,7 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   floats += 2 * n + 2 * n;            // divv, adjoint step factor, incremental state x2
   floats += (nt + 1) * n;             // adjoint levels
   floats += nt * n;                   // incremental state sources
-  floats += 3 * n * 9;                // bf, g, x, r, z, p, q, vtx, work3
+  floats += 3 * n * 10;               // bf, g, x, r, z, p, q, vtx, work3, Reg p
   long long bytes = floats * 4 + image_bytes + 3 * nc * 8;
   bytes += 2 * tile_table_int4s(d) * 16;  // box tables of the two characteristics
   bytes += (long long)max_parts(d) * 8;
@@ -220,6 +230,8 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
     graphs = !(ge && ge[0] == '0');
     const char* fd = std::getenv("CLAIRE_B200_FUSED_DOTS");
     fused_dots = fd && fd[0] == '1';
+    const char* rr = std::getenv("CLAIRE_B200_REG_RECURRENCE");
+    reg_rec_enabled = !(rr && rr[0] == '0');
   }
   ht = (float)(1.0 / nt);
   hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
@@ -289,11 +301,12 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   CB_TRY(alloc((void**)&q, V));
   CB_TRY(alloc((void**)&vtx, V));
   CB_TRY(alloc((void**)&work3, V));
+  CB_TRY(alloc((void**)&sreg, V));
   CB_TRY(alloc((void**)&spec, sizeof(float2) * 3 * nc * B));
   maxparts = max_parts(d);
   CB_TRY(alloc((void**)&partials, sizeof(double) * maxparts * B));
   CB_TRY(alloc((void**)&dsc, sizeof(double) * NSLOT * B));
-  CB_TRY(alloc((void**)&dact, sizeof(int) * 8 * B));
+  CB_TRY(alloc((void**)&dact, sizeof(int) * 11 * B));  // masks; 8..10: PCG recurrence flags and splits
   dact2 = dact + B;
   CB_TRY(alloc((void**)&dint, sizeof(int) * NISLOT * B));
   CB_TRY(alloc((void**)&dparams, sizeof(SpecParams) * B));
@@ -843,6 +856,34 @@ int Solver::adjoint_sweep(float* bout, const int* act, double hscale) {
 // and the regularisation's inverse transform accumulates into it.
 int Solver::finish_with_reg(const float* vin, float* out, const int* act, const float* dot_with, int dot_slot) {
   const bool proj = opts.model != CB_MODEL_COMPRESSIBLE;
+  if (reg_in) {
+    // Reg(vin) supplied by the PCG's recurrence for the problems of rec_act:
+    // out = body force + Reg(vin); the others transform as below
+    float* bfo = proj ? bf : out;
+    CB_TRY(adjoint_sweep(bfo, act));
+    if (norec_act) {
+      if (proj) {
+        CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_STORE, norec_act));
+        CB_TRY(launch_lincomb(out, 3 * n, out, 3 * n, nullptr, 1.0, bf, 3 * n, nullptr, 1.0, 3 * n, B, norec_act,
+                              stream));
+        note_launches(1);
+        if (dot_with) CB_TRY(dot(out, 3 * n, dot_with, 3 * n, 3 * n, dot_slot, norec_act));
+      } else {
+        CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_ADD, norec_act, dot_with, dot_slot));
+      }
+    }
+    if (dot_with) {
+      CB_TRY(launch_add_dot(out, bfo, reg_in, dot_with, 3 * n, 3 * n, B, partials, maxparts, rec_act, stream));
+      CB_TRY(launch_finalize(partials, maxparts, dot_partials(3 * n), slot(dot_slot), B, 1.0, false, stream,
+                             rec_act));
+      note_launches(2);
+    } else {
+      CB_TRY(launch_lincomb(out, 3 * n, bfo, 3 * n, nullptr, 1.0, reg_in, 3 * n, nullptr, 1.0, 3 * n, B, rec_act,
+                            stream));
+      note_launches(1);
+    }
+    return 0;
+  }
   if (!proj) {
     CB_TRY(adjoint_sweep(out, act));
     CB_TRY(reg_op(vin, out, OP_REG_GRAD, EPI_ADD, act, dot_with, dot_slot));
@@ -1076,14 +1117,66 @@ int Solver::final_state(float* m1, int b) {
   return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
 }
 
+// The INVREG preconditioner is the inverse of the regularisation operator, so
+// for the full norms with beta1 > 0 Reg P = c I holds symbol by symbol
+// (H1: hd beta0 (k^2 + beta1) / (beta0 (k^2 + beta1)) = hd; H2, H3, L2: 1;
+// src/RegularizationH1.cpp:229 and :379-382, and likewise for the others).
+// The seminorms drop the k = 0 modes from Reg and keep them in P, so there
+// Reg P is not a multiple of the identity.
+// Decided per problem, so a problem computes the same alone and in a batch.
+void Solver::reg_recurrence(const std::vector<int>& sel, std::vector<double>& c) const {
+  c.assign(B, 0.0);
+  if (!reg_rec_enabled || opts.precond != CB_PC_INVREG || mv_kind != 0) return;
+  for (int b = 0; b < B; ++b) {
+    if (!sel[b]) continue;
+    const ProbState& s = ps[b];
+    if (!(s.beta0 > 0.0)) continue;
+    if (s.norm == NORM_H1 && s.beta1 > 0.0) c[b] = (double)hd;
+    else if ((s.norm == NORM_H2 || s.norm == NORM_H3) && s.beta1 > 0.0) c[b] = 1.0;
+    else if (s.norm == NORM_L2) c[b] = 1.0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // PCG (KSPCG, unpreconditioned residual norm, zero initial guess;
 // src/Optimizer.cpp:296-356)
+//
+// Where Reg P = c I (reg_recurrence) the regularisation part of q = H p is
+// not transformed each iteration: with z = P r and p = z + beta p,
+// Reg p = c r + beta Reg p, started from Reg p0 = Reg P r0 = c r0.  In exact
+// arithmetic this is the same Reg p the spectral pass computes; it saves one
+// 3-field forward and inverse transform per iteration.
 // ---------------------------------------------------------------------------
 int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   const int maxit = (int)maxit_d;
   int* act = dact2;
   CB_TRY(upload_mask(sel, act));
+  std::vector<double> rc;
+  reg_recurrence(sel, rc);
+  std::vector<int> flag(B, 0);
+  bool any_rec = false, any_norec = false;
+  for (int b = 0; b < B; ++b) {
+    flag[b] = rc[b] > 0.0;
+    if (sel[b]) (flag[b] ? any_rec : any_norec) = true;
+  }
+  const bool rec = any_rec;
+  const int mode = (any_rec ? 1 : 0) | (any_norec ? 2 : 0);
+  int* dflag = dact + 8 * B;
+  int* act_rec = dact + 9 * B;
+  int* act_norec = dact + 10 * B;
+  if (rec) {
+    if (cudaMemcpyAsync(slot(S_RC), rc.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
+    CB_TRY(upload_mask(flag, dflag));
+  }
+  if (pcg_exec && pcg_exec_mode != mode) {  // recorded for another mix of forms
+    cudaGraphExecDestroy(pcg_exec);
+    pcg_exec = nullptr;
+  }
+  auto split = [&]() {
+    k_split_mask<<<pgrid(B), 128, 0, stream>>>(act, dflag, act_rec, act_norec, B);
+    note_launches(1);
+  };
   // r = -g, x = 0
   CB_TRY(launch_lincomb(r, 3 * n, g, 3 * n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
   CB_TRY(launch_lincomb(x, 3 * n, g, 3 * n, nullptr, 0.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
@@ -1101,13 +1194,28 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   CB_TRY(apply_pc(S_RZ));
   CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
   note_launches(1);
+  if (rec) {  // Reg p0 = c r0
+    split();
+    CB_TRY(launch_lincomb(sreg, 3 * n, r, 3 * n, slot(S_RC), 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act_rec,
+                          stream));
+    note_launches(1);
+  }
   std::vector<int> hact(B);
   // One PCG iteration.  It reads and writes device data only (vectors, the
   // per-problem scalars and the active mask, which k_pcg_alpha / k_pcg_check
   // clear when a problem stops), so it is recorded once as a CUDA graph and
   // replayed, and several iterations can run between host checks.
   auto body = [&]() -> int {
-    CB_TRY(apply_op(pv, q, act, S_PQ));  // q = H p and p.q
+    if (rec) {
+      split();
+      reg_in = sreg;
+      rec_act = act_rec;
+      norec_act = any_norec ? act_norec : nullptr;
+    }
+    const int he = apply_op(pv, q, act, S_PQ);  // q = H p and p.q
+    reg_in = nullptr;
+    rec_act = norec_act = nullptr;
+    CB_TRY(he);
     k_pcg_alpha<<<pgrid(B), 128, 0, stream>>>(dsc, dint, act, B);
     // x += alpha p, r -= alpha q and the new r.r in one pass
     CB_TRY(launch_cg_update(x, r, pv, q, 3 * n, 3 * n, slot(S_ALPHA), B, partials, maxparts, act, stream));
@@ -1118,6 +1226,12 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
     k_pcg_beta<<<pgrid(B), 128, 0, stream>>>(dsc, act, B);
     CB_TRY(launch_lincomb(pv, 3 * n, z, 3 * n, nullptr, 1.0, pv, 3 * n, slot(S_BETA), 1.0, 3 * n, B, act, stream));
     note_launches(2);
+    if (rec) {  // Reg p = c r + beta Reg p
+      split();
+      CB_TRY(launch_lincomb(sreg, 3 * n, r, 3 * n, slot(S_RC), 1.0, sreg, 3 * n, slot(S_BETA), 1.0, 3 * n, B,
+                            act_rec, stream));
+      note_launches(1);
+    }
     return 0;
   };
   auto run_body = [&]() -> int {
@@ -1135,6 +1249,7 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
       const cudaError_t ee = cudaStreamEndCapture(stream, &gr);
       g_graph_capture = false;
       pcg_exec_launches = launches() - l0;
+      pcg_exec_mode = mode;
       if (!e && ee == cudaSuccess && gr && cudaGraphInstantiate(&pcg_exec, gr, 0) != cudaSuccess) pcg_exec = nullptr;
       if (gr) cudaGraphDestroy(gr);
       if (e || ee != cudaSuccess || !pcg_exec) {

@@ -93,6 +93,13 @@ class Solver {
   float *divv = nullptr, *cadj = nullptr, *lamh = nullptr, *bf = nullptr;
   float *g = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *q = nullptr;
   float *vtx = nullptr, *mt = nullptr, *mt2 = nullptr, *sj = nullptr, *work3 = nullptr;
+  // PCG: the regularisation operator applied to the search direction, Reg p,
+  // carried by a recurrence instead of a spectral pass per iteration
+  float* sreg = nullptr;
+  const float* reg_in = nullptr;  // set: finish_with_reg adds this as Reg(vin) for the
+  const int* rec_act = nullptr;   // problems of rec_act, and transforms for those of
+  const int* norec_act = nullptr; // norec_act (null: none)
+  int pcg_exec_mode = 0;          // recorded PCG iteration: bit 0 some, bit 1 not all problems recurrent
   // bf16-image mode (opts.bf16_images): mR, mT and the state levels live in
   // these arrays instead (same layout); mR / mT / m above stay null.
   bool img16 = false;
@@ -114,7 +121,9 @@ class Solver {
               S_RN0, S_GD, S_RTOL, S_RW,
               // NCC: sums <x,x> of m1 (or mT), <mR,mR>, <x,mR>, |mT - mR|^2, the
               // scale, <m1,m~>, <mR,m~>, and final-condition coefficients
-              S_NA, S_NRR, S_NI, S_NL2, S_NS, S_NIM, S_NRM, S_CA, S_CB, S_CC, NSLOT };
+              S_NA, S_NRR, S_NI, S_NL2, S_NS, S_NIM, S_NRM, S_CA, S_CB, S_CC,
+              // PCG: the constant c of Reg P = c I (regularisation recurrence)
+              S_RC, NSLOT };
   enum ISlot { I_IT = 0, I_REASON, NISLOT };
 
   // Krylov reference norms handed to the next begin() (continuation levels keep
@@ -158,6 +167,8 @@ class Solver {
   // PCG iteration recorded as a CUDA graph (built on the second iteration the
   // solver runs; graphs = false switches replay off)
   bool graphs = true, pcg_warm = false;
+  // Reg p by recurrence in the PCG where Reg P = c I (CLAIRE_B200_REG_RECURRENCE=0: off)
+  bool reg_rec_enabled = true;
   // p.q and r.z summed inside the inverse transforms' epilogues instead of a
   // separate dot pass (CLAIRE_B200_FUSED_DOTS=1)
   bool fused_dots = false;
@@ -221,6 +232,8 @@ class Solver {
   }
   int pcg(const std::vector<int>& sel, double maxit);
   int pcg_twolevel(const std::vector<int>& sel, double maxit);
+  // per problem: whether Reg P = c I holds, and c (0: it does not)
+  void reg_recurrence(const std::vector<int>& sel, std::vector<double>& c) const;
   int line_search(std::vector<int>& sel);
   int dot(const float* a, long long ap, const float* b, long long bp, long long len, int slot,
           const int* act, double scale = 1.0);
