@@ -5,6 +5,7 @@
 //   reg::SemiLagrangian    (include/SemiLagrangian.hpp:43-58)
 //   reg::Regularization    (include/Regularization.hpp:46-50)
 //   reg::DistanceMeasureSL2 (include/DistanceMeasure.hpp:44-50)
+//   reg::Preconditioner    (include/Preconditioner.hpp: MatVec)
 //   reg::VecField          (include/VecField.hpp; flat [x1 | x2 | x3])
 // Images and fields are plain float arrays in place of PETSc Vec (host arrays
 // for CLAIREInterface, device arrays for the operator classes).  Every method
@@ -134,6 +135,22 @@ class CLAIREInterface {
   ErrorCode status_ = 0;
   const float* mR_ = nullptr;
   const float* mT_ = nullptr;
+};
+
+// Preconditioner::MatVec (src/Preconditioner.cpp:507-580) of a registration
+// context's problem b on host arrays of 3 nl floats: INVREG P x = (beta A)^-1 x,
+// or with -precond 2level Apply2LevelPrecond (:584-673), set up at the
+// problem's current velocity.
+class Preconditioner {
+ public:
+  explicit Preconditioner(CLAIREInterface* problem) : problem_(problem) {}
+  ErrorCode MatVec(float* Px, const float* x, int b = 0) {
+    return claire_b200_precond(problem_ ? problem_->handle() : nullptr, b, x, Px);
+  }
+  ErrorCode MatVec(VecField* Px, const VecField* x, int b = 0) { return MatVec(Px->data(), x->data(), b); }
+
+ private:
+  CLAIREInterface* problem_;
 };
 
 // Operator seams on device arrays (one problem, explicit stream).

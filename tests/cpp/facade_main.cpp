@@ -2,7 +2,9 @@
 // for tests/test_facade.py.
 //   facade_main opts <args...>            print the parsed options
 //   facade_main run <dir> <args...>       read <dir>/mR.bin, mT.bin (nl floats),
-//                                         register, write <dir>/v.bin and print stats
+//                                         register, write <dir>/v.bin and the
+//                                         preconditioner applied to v, <dir>/pv.bin,
+//                                         and print stats
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -52,6 +54,13 @@ int main(int argc, char** argv) {
     }
     reg::VecField v(opt);
     if (reg.GetSolution(&v)) return 8;
+    reg::Preconditioner pc(&reg);
+    reg::VecField pv(opt);
+    if (pc.MatVec(&pv, &v)) return 11;
+    FILE* fp = std::fopen((dir + "/pv.bin").c_str(), "wb");
+    if (!fp) return 10;
+    std::fwrite(pv.data(), sizeof(float), 3 * pv.nl(), fp);
+    std::fclose(fp);
     double det[3];
     if (reg.ComputeDetDefGrad(nullptr, det)) return 9;
     claire_b200_stats st;

@@ -40,7 +40,8 @@ def test_facade_parses_like_regopt(facade):
 
 
 @pytest.mark.gpu
-def test_facade_registration_equals_python_binding(facade, tmp_path, cuda):
+@pytest.mark.parametrize("precond", ["invreg", "2level"])
+def test_facade_registration_equals_python_binding(facade, tmp_path, cuda, precond):
     import claire_b200 as cb
     n, nt = 32, 4
     mR, mT, _ = R.synthetic_c1(n, np.float64, nt)
@@ -48,16 +49,20 @@ def test_facade_registration_equals_python_binding(facade, tmp_path, cuda):
     mT = mT.astype(np.float32)
     mR.tofile(tmp_path / "mR.bin")
     mT.tofile(tmp_path / "mT.bin")
-    args = ["-nx", str(n), "-nt", str(nt), "-regnorm", "h1s", "-beta", "1e-2", "-maxit", "10", "-opttol", "1e-2"]
+    args = ["-nx", str(n), "-nt", str(nt), "-regnorm", "h1s", "-beta", "1e-2", "-maxit", "10", "-opttol", "1e-2",
+            "-precond", precond]
     r = subprocess.run([facade, "run", str(tmp_path)] + args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     out = json.loads(r.stdout)
     v_cpp = np.fromfile(tmp_path / "v.bin", dtype=np.float32).reshape(3, n, n, n)
+    pv_cpp = np.fromfile(tmp_path / "pv.bin", dtype=np.float32).reshape(3, n, n, n)
     with cb.CLAIREInterface(cb.RegOpt(args)) as ci:
         ci.set_images(mR, mT)
         ci.Run()
         v_py = np.asarray(ci.GetSolution())
         st = ci.stats()
+        pv_py = ci.ApplyInvRegularizationOperator(v_py)
     assert np.array_equal(v_cpp, v_py)
+    assert np.array_equal(pv_cpp, pv_py)  # reg::Preconditioner::MatVec
     assert out["gn"] == st["gn_iterations"] and out["pcg"] == st["pcg_iterations"]
     assert 0.0 < out["det_min"] <= 1.0 <= out["det_max"]
