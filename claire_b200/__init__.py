@@ -66,7 +66,7 @@ class Opts(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("slots_per_pool", ctypes.c_int),
-                ("idle_ms", ctypes.c_int), ("device", ctypes.c_int)]
+                ("idle_ms", ctypes.c_int), ("device", ctypes.c_int), ("batch_window_us", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -672,13 +672,15 @@ class Server:
     and HBM free up, and retired when their stopping test fires.  Images are
     host arrays (NumPy float32 or CPU tensors); results are host arrays."""
 
-    def __init__(self, slots_per_pool: int = 4, hbm_budget_bytes: int = 0, idle_ms: int = 2000, device: int = 0):
+    def __init__(self, slots_per_pool: int = 4, hbm_budget_bytes: int = 0, idle_ms: int = 2000, device: int = 0,
+                 batch_window_us: int = 0):
         o = ServerOpts()
         lib.claire_b200_server_default_opts(ctypes.byref(o))
         o.slots_per_pool = int(slots_per_pool)
         o.hbm_budget_bytes = int(hbm_budget_bytes)
         o.idle_ms = int(idle_ms)
         o.device = int(device)
+        o.batch_window_us = int(batch_window_us)
         h = ctypes.c_void_p()
         _check(lib.claire_b200_server_create(ctypes.byref(o), ctypes.byref(h)), "Server")
         self._srv = h

@@ -226,6 +226,19 @@ static void worker_main(claire_b200_server* s, Pool* p) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (s->stop) break;
+      bool running = false;
+      for (int b = 0; b < S; ++b) running |= p->slot_req[b] != 0;
+      if (!running && s->opts.batch_window_us > 0) {
+        // an idle pool with work: requests submitted together (a client's
+        // batch) get a short window to arrive, so their GN loops start in the
+        // same step instead of one GN iteration apart
+        const long long pend = pending_for(s, p->key);
+        if (pend > 0 && pend < S) {
+          s->cv.wait_until(lk, Clock::now() + std::chrono::microseconds(s->opts.batch_window_us),
+                           [&] { return s->stop || pending_for(s, p->key) >= S; });
+          if (s->stop) break;
+        }
+      }
       admits = admit_locked(s, p);
       bool busy = !admits.empty();
       for (int b = 0; b < S; ++b) busy |= p->slot_req[b] != 0;
@@ -323,6 +336,7 @@ void claire_b200_server_default_opts(claire_b200_server_opts* o) {
   o->slots_per_pool = 4;
   o->idle_ms = 2000;
   o->device = 0;
+  o->batch_window_us = 0;
 }
 
 int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_server** out) {

@@ -280,6 +280,8 @@ typedef struct claire_b200_server_opts {
   int slots_per_pool;         /* problems per pool (batch width) */
   int idle_ms;                /* a pool without work for this long releases its memory */
   int device;                 /* CUDA device of the server */
+  int batch_window_us;        /* an idle pool that receives a request waits up to this long for more
+                                 requests of its key before starting (0: start at once, the default) */
 } claire_b200_server_opts;
 #define CB_REQ_QUEUED 0
 #define CB_REQ_RUNNING 1
