@@ -1509,11 +1509,16 @@ int Solver::line_search(std::vector<int>& sel) {
     if (!(gd[b] < 0.0)) {
       fallback[b] = 1;
       anyfb = true;
-      gd[b] = -ps[b].gnorm * ps[b].gnorm;
     }
   }
   if (anyfb) {
+    // direction -g, slope -|g|^2 of the gradient vector the solve left in g
+    // (P^1/2 g with the two-level preconditioner's PreKrylovSolve)
     CB_TRY(upload_mask(fallback, dact + 3 * B));
+    CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, dact + 3 * B));
+    CB_TRY(fetch_scalars());
+    for (int b = 0; b < B; ++b)
+      if (fallback[b]) gd[b] = -hsc[S_GG * B + b];
     CB_TRY(launch_lincomb(x, 3 * n, g, 3 * n, nullptr, -1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, dact + 3 * B, stream));
     note_launches(1);
   }
