@@ -133,6 +133,8 @@ _signatures = {
     "claire_b200_grid_change": (_I, [_P, _I, _P, _I, _I, _P]),
     "claire_b200_read_nifti": (_I, [ctypes.c_char_p, _IA, _P, ctypes.c_longlong]),
     "claire_b200_write_nifti": (_I, [ctypes.c_char_p, _IA, _P]),
+    "claire_b200_read_bin": (_I, [ctypes.c_char_p, _IA, _P]),
+    "claire_b200_write_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
     "claire_b200_fft_div": (_I, [_P, _P, _IA, _P]),
@@ -191,8 +193,9 @@ def fft_variant_candidates(n: int):
 
 
 def read_nifti(path: str):
-    """ReadWriteReg::ReadNII: the volume of a single-file NIfTI-1 image as a
-    float32 array of shape (nx[0], nx[1], nx[2]) = (nz, ny, nx) of the file."""
+    """ReadWriteReg::ReadNII: the volume of a NIfTI-1 image (single file, or
+    the .hdr / .img pair) as a float32 array of shape (nx[0], nx[1], nx[2]) =
+    (nz, ny, nx) of the file."""
     import numpy as np
     nx = (ctypes.c_int * 3)()
     _check(lib.claire_b200_read_nifti(os.fsencode(path), nx, None, 0), "read_nifti")
@@ -203,13 +206,51 @@ def read_nifti(path: str):
 
 
 def write_nifti(path: str, arr) -> None:
-    """ReadWriteReg::WriteNII: float32 single-file NIfTI-1 (.nii, or .nii.gz compressed)."""
+    """ReadWriteReg::WriteNII: float32 NIfTI-1 (.nii, .nii.gz compressed, or
+    the .hdr / .img pair)."""
     import numpy as np
     a = np.ascontiguousarray(arr, dtype=np.float32)
     if a.ndim != 3:
         raise ValueError("expected a 3D volume")
     _check(lib.claire_b200_write_nifti(os.fsencode(path), _nx(a.shape), a.ctypes.data_as(ctypes.c_void_p)),
            "write_nifti")
+
+
+def read_bin(path: str, shape):
+    """ReadWriteReg::ReadBIN: a PETSc binary vector of prod(shape) values (the
+    grid comes from the caller, as from the options in the reference)."""
+    import numpy as np
+    out = np.empty(tuple(shape), dtype=np.float32)
+    _check(lib.claire_b200_read_bin(os.fsencode(path), _nx(out.shape), out.ctypes.data_as(ctypes.c_void_p)),
+           "read_bin")
+    return out
+
+
+def write_bin(path: str, arr) -> None:
+    """ReadWriteReg::WriteBIN: a PETSc binary vector (big-endian doubles)."""
+    import numpy as np
+    a = np.ascontiguousarray(arr, dtype=np.float32)
+    if a.ndim != 3:
+        raise ValueError("expected a 3D volume")
+    _check(lib.claire_b200_write_bin(os.fsencode(path), _nx(a.shape), a.ctypes.data_as(ctypes.c_void_p)),
+           "write_bin")
+
+
+def read_image(path: str, shape=None):
+    """ReadWriteReg::Read (src/ReadWriteReg.cpp:440-475): by extension, NIfTI-1
+    (.nii, .nii.gz, .hdr / .img) or a PETSc binary vector (.bin, needs shape)."""
+    if ".bin" in os.path.basename(path):
+        if shape is None:
+            raise ValueError("a .bin vector holds no grid: pass shape")
+        return read_bin(path, shape)
+    return read_nifti(path)
+
+
+def write_image(path: str, arr) -> None:
+    """ReadWriteReg::Write (src/ReadWriteReg.cpp:700-745): by extension."""
+    if ".bin" in os.path.basename(path):
+        return write_bin(path, arr)
+    return write_nifti(path, arr)
 
 
 def preprocess(m, rescale: bool = True, sigma=(1.0, 1.0, 1.0)):

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -133,8 +134,18 @@ extern "C" {
 
 int claire_b200_read_nifti(const char* path, int nx[3], float* data, long long capacity) {
   if (!path || !nx) return CB_ERR_ARG;
+  // two-file NIfTI-1 (.hdr + .img, either name given, optionally .gz)
+  std::string hdr_path(path), img_path;
+  for (const char* gz : {"", ".gz"}) {
+    const std::string hs = std::string(".hdr") + gz, is = std::string(".img") + gz;
+    if (ends_with(hdr_path, hs.c_str())) img_path = hdr_path.substr(0, hdr_path.size() - hs.size()) + is;
+    else if (ends_with(hdr_path, is.c_str())) {
+      img_path = hdr_path;
+      hdr_path = hdr_path.substr(0, hdr_path.size() - is.size()) + hs;
+    }
+  }
   Gz gz;
-  gz.f = gzopen(path, "rb");
+  gz.f = gzopen(hdr_path.c_str(), "rb");
   if (!gz.f) return CB_ERR_ARG;
   unsigned char h[kHdr];
   if (!read_exact(gz.f, h, kHdr)) return CB_ERR_ARG;
@@ -145,7 +156,9 @@ int claire_b200_read_nifti(const char* path, int nx[3], float* data, long long c
     hs = get<int>(h, 0, true);
     if (hs != kHdr) return CB_ERR_ARG;  // not a NIfTI-1 header
   }
-  if (std::memcmp(h + 344, "n+1", 4) != 0) return CB_ERR_UNSUPPORTED;  // single-file NIfTI-1 only
+  const bool pair = std::memcmp(h + 344, "ni1", 4) == 0;
+  if (!pair && std::memcmp(h + 344, "n+1", 4) != 0) return CB_ERR_ARG;  // not NIfTI-1
+  if (pair && img_path.empty()) return CB_ERR_ARG;  // a pair header needs a .hdr / .img name
   const int ndim = get<short>(h, 40, swap);
   long long dim[8];
   for (int i = 0; i < 8; ++i) dim[i] = get<short>(h, 40 + 2 * i, swap);
@@ -162,11 +175,22 @@ int claire_b200_read_nifti(const char* path, int nx[3], float* data, long long c
   if (!data) return CB_OK;
   if (capacity < n) return CB_ERR_TOO_LARGE;
   const long long off = (long long)get<float>(h, 108, swap);
-  if (off < kHdr) return CB_ERR_ARG;
-  std::vector<unsigned char> skip((size_t)(off - kHdr));
-  if (!skip.empty() && !read_exact(gz.f, skip.data(), (long long)skip.size())) return CB_ERR_ARG;
+  // single file: voxels at vox_offset (>= 348) of the same file; pair: at
+  // vox_offset (usually 0) of the .img file
+  Gz img;
+  gzFile src = gz.f;
+  long long skip_bytes = off - kHdr;
+  if (pair) {
+    img.f = gzopen(img_path.c_str(), "rb");
+    if (!img.f) return CB_ERR_ARG;
+    src = img.f;
+    skip_bytes = off;
+  }
+  if (skip_bytes < 0) return CB_ERR_ARG;
+  std::vector<unsigned char> skip((size_t)skip_bytes);
+  if (!skip.empty() && !read_exact(src, skip.data(), (long long)skip.size())) return CB_ERR_ARG;
   std::vector<unsigned char> raw((size_t)(n * tb));
-  if (!read_exact(gz.f, raw.data(), n * tb)) return CB_ERR_ARG;
+  if (!read_exact(src, raw.data(), n * tb)) return CB_ERR_ARG;
   switch (datatype) {
     case 2: convert<uint8_t>(raw.data(), data, n, swap); break;
     case 256: convert<int8_t>(raw.data(), data, n, swap); break;
@@ -199,15 +223,33 @@ int claire_b200_write_nifti(const char* path, const int nx[3], const float* data
                            (float)(2.0 * 3.14159265358979323846 / nx[1]),
                            (float)(2.0 * 3.14159265358979323846 / nx[2]), 1.f, 1.f, 1.f, 1.f};
   for (int i = 0; i < 8; ++i) put<float>(h, 76 + 4 * i, pixdim[i]);
-  put<float>(h, 108, 352.f);  // vox_offset
-  put<float>(h, 112, 1.f);    // scl_slope
-  std::memcpy(h + 344, "n+1", 4);
-  const long long n = (long long)nx[0] * nx[1] * nx[2];
   const std::string p(path);
   const bool gzip = ends_with(p, ".gz");
-  gzFile f = gzopen(path, gzip ? "wb6" : "wbT");  // "T": plain (uncompressed) output
+  // .hdr / .img (optionally .gz): the NIfTI-1 pair (NIFTI_FTYPE_NIFTI1_2,
+  // src/ReadWriteReg.cpp:1305-1306), header with magic "ni1" and the voxels
+  // at offset 0 of the .img file
+  std::string base;
+  for (const char* suf : {".hdr", ".img", ".hdr.gz", ".img.gz"})
+    if (ends_with(p, suf)) base = p.substr(0, p.size() - std::strlen(suf));
+  const bool pair = !base.empty();
+  put<float>(h, 108, pair ? 0.f : 352.f);  // vox_offset
+  put<float>(h, 112, 1.f);                 // scl_slope
+  std::memcpy(h + 344, pair ? "ni1" : "n+1", 4);
+  const long long n = (long long)nx[0] * nx[1] * nx[2];
+  const char* mode = gzip ? "wb6" : "wbT";  // "T": plain (uncompressed) output
+  gzFile f = nullptr;
+  bool ok = true;
+  if (pair) {
+    gzFile fh = gzopen((base + (gzip ? ".hdr.gz" : ".hdr")).c_str(), mode);
+    if (!fh) return CB_ERR_ARG;
+    ok = gzwrite(fh, h, sizeof(h)) == (int)sizeof(h);
+    ok = (gzclose(fh) == Z_OK) && ok;
+    f = gzopen((base + (gzip ? ".img.gz" : ".img")).c_str(), mode);
+  } else {
+    f = gzopen(path, mode);
+    if (f) ok = gzwrite(f, h, sizeof(h)) == (int)sizeof(h);
+  }
   if (!f) return CB_ERR_ARG;
-  bool ok = gzwrite(f, h, sizeof(h)) == (int)sizeof(h);
   const unsigned char* src = reinterpret_cast<const unsigned char*>(data);
   long long left = n * 4;
   while (ok && left > 0) {
@@ -218,6 +260,57 @@ int claire_b200_write_nifti(const char* path, const int nx[3], const float* data
   }
   ok = (gzclose(f) == Z_OK) && ok;
   return ok ? CB_OK : CB_ERR_ARG;
+}
+
+// ReadBIN / WriteBIN (src/ReadWriteReg.cpp:1476-1535): a PETSc binary vector
+// (VecLoad / VecView): big-endian int32 class id 1211214, int32 length, then
+// the values big-endian, 8 bytes each in the reference's default double build
+// (4 in a single-precision build; the reader takes either, by file size).
+// The grid is not stored: it comes from the options, nx here.
+int claire_b200_read_bin(const char* path, const int nx[3], float* data) {
+  if (!path || !nx || !data || nx[0] < 1 || nx[1] < 1 || nx[2] < 1) return CB_ERR_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return CB_ERR_ARG;
+  unsigned char hd[8];
+  const bool hok = std::fread(hd, 1, 8, f) == 8;
+  std::fseek(f, 0, SEEK_END);
+  const long long size = std::ftell(f);
+  std::fseek(f, 8, SEEK_SET);
+  const long long n = (long long)nx[0] * nx[1] * nx[2];
+  int rc = CB_OK;
+  if (!hok || get<int>(hd, 0, true) != 1211214 || get<int>(hd, 4, true) != n) rc = CB_ERR_ARG;
+  const long long per = (rc == CB_OK && n > 0) ? (size - 8) / n : 0;
+  if (rc == CB_OK && ((size - 8) % n || (per != 8 && per != 4))) rc = CB_ERR_ARG;
+  if (rc == CB_OK) {
+    std::vector<unsigned char> raw((size_t)(n * per));
+    if (std::fread(raw.data(), 1, raw.size(), f) != raw.size()) rc = CB_ERR_ARG;
+    else if (per == 8) convert<double>(raw.data(), data, n, true);
+    else convert<float>(raw.data(), data, n, true);
+  }
+  std::fclose(f);
+  return rc;
+}
+
+int claire_b200_write_bin(const char* path, const int nx[3], const float* data) {
+  if (!path || !nx || !data || nx[0] < 1 || nx[1] < 1 || nx[2] < 1) return CB_ERR_ARG;
+  const long long n = (long long)nx[0] * nx[1] * nx[2];
+  if (n > 2147483647LL) return CB_ERR_TOO_LARGE;
+  std::vector<unsigned char> out((size_t)(8 + 8 * n));
+  auto be32 = [&](size_t off, uint32_t v) {
+    for (int i = 0; i < 4; ++i) out[off + i] = (unsigned char)(v >> (24 - 8 * i));
+  };
+  be32(0, 1211214u);
+  be32(4, (uint32_t)n);
+  for (long long i = 0; i < n; ++i) {
+    uint64_t bits;
+    const double v = (double)data[i];
+    std::memcpy(&bits, &v, 8);
+    for (int k = 0; k < 8; ++k) out[8 + 8 * i + k] = (unsigned char)(bits >> (56 - 8 * k));
+  }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return CB_ERR_ARG;
+  const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+  return (std::fclose(f) == 0 && ok) ? CB_OK : CB_ERR_ARG;
 }
 
 int claire_b200_preprocess(float* m, const int nx[3], int rescale, const double sigma[3], void* stream) {

@@ -211,12 +211,22 @@ int claire_b200_set_fft_variant(int n, int variant);
  * (nx[0] = NIfTI nz, nx[2] = NIfTI nx, src/ReadWriteReg.cpp:813-815); data
  * (host, at least nx[0]*nx[1]*nx[2] floats = capacity, or NULL to query the
  * size) receives the raw voxel values as float, in file order (x3 fastest).
- * CB_ERR_UNSUPPORTED for two-file (.hdr/.img) images, several volumes or
- * components, or other data types. */
+ * Two-file images (.hdr + .img, magic "ni1") are read when either name is
+ * given.  CB_ERR_UNSUPPORTED for several volumes or components, or other
+ * data types. */
 int claire_b200_read_nifti(const char* path, int nx[3], float* data, long long capacity);
-/* ReadWriteReg::WriteNII (src/ReadWriteReg.cpp:1130-1475): float32 single-file
- * NIfTI-1, gzip-compressed when the path ends in .gz; pixdim = 2*pi/nx. */
+/* ReadWriteReg::WriteNII (src/ReadWriteReg.cpp:1130-1475): float32 NIfTI-1,
+ * gzip-compressed when the path ends in .gz; pixdim = 2*pi/nx.  A path ending
+ * in .hdr or .img (optionally .gz) writes the two-file pair. */
 int claire_b200_write_nifti(const char* path, const int nx[3], const float* data);
+/* ReadWriteReg::ReadBIN / WriteBIN (src/ReadWriteReg.cpp:1476-1535): PETSc
+ * binary vectors (VecLoad / VecView layout: big-endian int32 class id
+ * 1211214, int32 length, big-endian values).  Written as 8-byte doubles (the
+ * reference's default build); read as doubles or 4-byte floats by file size.
+ * The file holds no grid: nx (CLAIRE order) gives it, and the stored length
+ * must equal nx[0]*nx[1]*nx[2]. */
+int claire_b200_read_bin(const char* path, const int nx[3], float* data);
+int claire_b200_write_bin(const char* path, const int nx[3], const float* data);
 /* Image preparation of the file path on a device field (one problem):
  * rescale != 0 applies Normalize (src/CLAIREUtils.cpp:492-525, called by
  * CLAIREInterface::SetReferenceImage / SetTemplateImage,

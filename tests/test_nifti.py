@@ -123,3 +123,60 @@ def test_reference_example_brains(cb, name):
     out = cb.read_nifti(path)
     assert out.shape == (dims[3], dims[2], dims[1])
     assert np.array_equal(out.ravel(), ref.astype(np.float32))
+
+
+def test_two_file_pair_read_and_write(cb, tmp_path):
+    # NIfTI-1 pair (NIFTI_FTYPE_NIFTI1_2, src/ReadWriteReg.cpp:1305-1306):
+    # header with magic "ni1" in .hdr, voxels at vox_offset (0) of .img
+    rng = np.random.default_rng(7)
+    vol = rng.uniform(-5, 5, size=(4, 5, 6)).astype(np.float32)  # (nz, ny, nx)
+    single = make_nifti(vol, 16)
+    h = bytearray(single[:348])
+    h[344:348] = b"ni1\0"
+    struct.pack_into("<f", h, 108, 0.0)
+    for gz in (False, True):
+        suf = ".gz" if gz else ""
+        hdr, img = tmp_path / f"p.hdr{suf}", tmp_path / f"p.img{suf}"
+        data = vol.tobytes()
+        hdr.write_bytes(gzip.compress(bytes(h)) if gz else bytes(h))
+        img.write_bytes(gzip.compress(data) if gz else data)
+        for name in (hdr, img):
+            assert np.array_equal(cb.read_nifti(str(name)), vol)
+    # writing a pair: .hdr with "ni1" and vox_offset 0, .img with the voxels
+    cb.write_nifti(str(tmp_path / "w.hdr"), vol)
+    raw_h = (tmp_path / "w.hdr").read_bytes()
+    assert raw_h[344:348] == b"ni1\0" and struct.unpack_from("<f", raw_h, 108)[0] == 0.0
+    assert struct.unpack_from("<8h", raw_h, 40)[:4] == (5, 6, 5, 4)
+    assert np.array_equal(np.frombuffer((tmp_path / "w.img").read_bytes(), dtype="<f4").reshape(vol.shape), vol)
+    assert np.array_equal(cb.read_nifti(str(tmp_path / "w.img")), vol)
+    # a pair header without its .img name is refused
+    (tmp_path / "lone.nii").write_bytes(bytes(h))
+    with pytest.raises(cb.ClaireError):
+        cb.read_nifti(str(tmp_path / "lone.nii"))
+
+
+def test_petsc_binary_vectors(cb, tmp_path):
+    # ReadBIN / WriteBIN (src/ReadWriteReg.cpp:1476-1535): VecView / VecLoad
+    # layout, big-endian class id 1211214, length, values
+    rng = np.random.default_rng(8)
+    vol = rng.standard_normal((3, 4, 5)).astype(np.float32)
+    p = tmp_path / "v.bin"
+    cb.write_image(str(p), vol)
+    raw = p.read_bytes()
+    cid, n = struct.unpack_from(">ii", raw, 0)
+    assert cid == 1211214 and n == vol.size and len(raw) == 8 + 8 * n
+    assert np.array_equal(np.frombuffer(raw, dtype=">f8", offset=8).astype(np.float32).reshape(vol.shape), vol)
+    assert np.array_equal(cb.read_image(str(p), vol.shape), vol)
+    # a single-precision build's file: 4-byte values
+    q = tmp_path / "s.bin"
+    q.write_bytes(struct.pack(">ii", 1211214, vol.size) + vol.astype(">f4").tobytes())
+    assert np.array_equal(cb.read_bin(str(q), vol.shape), vol)
+    # the length must match the grid; the class id must be a vector's
+    with pytest.raises(cb.ClaireError):
+        cb.read_bin(str(q), (3, 4, 6))
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(struct.pack(">ii", 1211215, vol.size) + vol.astype(">f4").tobytes())
+    with pytest.raises(cb.ClaireError):
+        cb.read_bin(str(bad), vol.shape)
+    with pytest.raises(ValueError):
+        cb.read_image(str(p))
