@@ -134,6 +134,7 @@ _signatures = {
     "claire_b200_read_nifti": (_I, [ctypes.c_char_p, _IA, _P, ctypes.c_longlong]),
     "claire_b200_write_nifti": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_read_bin": (_I, [ctypes.c_char_p, _IA, _P]),
+    "claire_b200_deformation_map": (_I, [_P, _I, _I, _P]),
     "claire_b200_write_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
@@ -571,6 +572,15 @@ class CLAIREInterface:
         out = np.empty((3,) + tuple(self.shape), dtype=np.float32)
         _check(lib.claire_b200_precond(self._ctx, b, p, out.ctypes.data_as(ctypes.c_void_p)), "Precond", self._ctx)
         return out
+
+    def ComputeDeformationMap(self, inverse: bool = False, b: int = 0):
+        """DeformationFields::ComputeDeformationMap (SL RK2) at the current
+        velocity: positions y (3, n1, n2, n3) in physical coordinates."""
+        import numpy as np
+        y = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_deformation_map(self._ctx, b, int(bool(inverse)), y.ctypes.data_as(ctypes.c_void_p)),
+               "ComputeDeformationMap", self._ctx)
+        return y
 
     def GetAdjoint(self, b: int = 0):
         import numpy as np

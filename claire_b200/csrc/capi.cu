@@ -645,6 +645,29 @@ int claire_b200_det_def_grad(claire_b200_ctx* c, int b, int inverse, float* jac,
   return CB_OK;
 }
 
+int claire_b200_deformation_map(claire_b200_ctx* c, int b, int inverse, float* y) {
+  if (!c || !y || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  int e = s.deformation_map(sel, inverse != 0);
+  if (e) return cuda_status(e);
+  e = copy_out(s, y, s.x + b * 3 * s.n, 3 * s.n, 0);
+  if (e) return e;
+  // positions y = x + u h (ComputeRegularGrid: x_i = i h, h = 2 pi / N per axis)
+  const int n1 = s.d.n1, n2 = s.d.n2, n3 = s.d.n3;
+  const double h[3] = {cb::kTwoPi / n1, cb::kTwoPi / n2, cb::kTwoPi / n3};
+  for (int i1 = 0; i1 < n1; ++i1)
+    for (int i2 = 0; i2 < n2; ++i2)
+      for (int i3 = 0; i3 < n3; ++i3) {
+        const long long i = ((long long)i1 * n2 + i2) * n3 + i3;
+        y[i] = (float)((i1 + (double)y[i]) * h[0]);
+        y[s.n + i] = (float)((i2 + (double)y[s.n + i]) * h[1]);
+        y[2 * s.n + i] = (float)((i3 + (double)y[2 * s.n + i]) * h[2]);
+      }
+  return CB_OK;
+}
+
 int claire_b200_get_adjoint(claire_b200_ctx* c, int b, float* lambda0, float* body_force) {
   if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

@@ -1031,6 +1031,43 @@ int Solver::det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<
   return 0;
 }
 
+// Deformation map of the selected problems at their velocity v,
+// DeformationFields::ComputeDeformationMapSLRK2 (src/DeformationFields.cpp:
+// 1472-1585; ComputeDeformationMap, :1189-1268): particles start on the grid
+// (y = x) and move backward along v with RK2, v evaluated at the current
+// positions by the tricubic gather: yt = y - ht v(y), y <- y - ht/2 (v(y) +
+// v(yt)) per time step (ht < 0 for the inverse map).  The positions are kept
+// as displacements u = y - x in grid units (x: u, r: yt - x, z: v at the
+// query points); the gathers take any displacement (periodic wrap).
+int Solver::deformation_map(const std::vector<int>& sel, bool inverse) {
+  CB_TRY(upload_mask(sel, dact));
+  const double h = inverse ? -(double)ht : (double)ht;
+  const double c[3] = {d.n1 / kTwoPi, d.n2 / kTwoPi, d.n3 / kTwoPi};  // grid units per unit length
+  float *u = x, *ut = r, *vy = z;
+  CB_TRY(launch_fill(u, 3 * n, 0.f, 3 * n, B, dact, stream));
+  note_launches(1);
+  for (int j = 0; j < nt; ++j) {
+    CB_TRY(launch_tile_table(u, 3 * n, tab_st, TP, B, d, dact, stream));
+    CB_TRY(launch_interp(v, 3 * n, n, u, 3 * n, tab_st, TP, vy, 3 * n, n, 3, B, d, dact, stream));
+    for (int k = 0; k < 3; ++k) {
+      CB_TRY(launch_lincomb(ut + k * n, 3 * n, u + k * n, 3 * n, nullptr, 1.0, vy + k * n, 3 * n, nullptr,
+                            -h * c[k], n, B, dact, stream));
+      CB_TRY(launch_lincomb(u + k * n, 3 * n, u + k * n, 3 * n, nullptr, 1.0, vy + k * n, 3 * n, nullptr,
+                            -0.5 * h * c[k], n, B, dact, stream));
+    }
+    CB_TRY(launch_tile_table(ut, 3 * n, tab_st, TP, B, d, dact, stream));
+    CB_TRY(launch_interp(v, 3 * n, n, ut, 3 * n, tab_st, TP, vy, 3 * n, n, 3, B, d, dact, stream));
+    for (int k = 0; k < 3; ++k)
+      CB_TRY(launch_lincomb(u + k * n, 3 * n, u + k * n, 3 * n, nullptr, 1.0, vy + k * n, 3 * n, nullptr,
+                            -0.5 * h * c[k], n, B, dact, stream));
+    note_launches(13);
+  }
+  // the state characteristic's box table now belongs to u: cached levels are stale
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) state_of[b] = 0;
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
 // ---------------------------------------------------------------------------
 // public single-shot operations
 // ---------------------------------------------------------------------------

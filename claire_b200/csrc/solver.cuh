@@ -64,6 +64,8 @@ class Solver {
   int precond(const float* rin, float* zout, const std::vector<int>& sel);
   int forward(const float* m0, float* m1, const std::vector<int>& sel);
   int det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<double>& stats);
+  // deformation map y - x in grid units (3 fields per problem, in x)
+  int deformation_map(const std::vector<int>& sel, bool inverse);
   int final_state(float* m1, int b);
   // images of problem b from device arrays (n floats each), converted to the
   // storage type; not synchronised

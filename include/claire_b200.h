@@ -168,6 +168,11 @@ int claire_b200_precond(claire_b200_ctx* ctx, int b, const float* x, float* px);
  * include/CLAIREInterface.hpp:42-90).  jac (host, n floats) may be NULL;
  * stats = {min, mean, max} (the reference's monitor values, :367-375). */
 int claire_b200_det_def_grad(claire_b200_ctx* ctx, int b, int inverse, float* jac, double stats[3]);
+/* Deformation map y of problem b at its current velocity (inverse != 0: the
+ * inverse map), DeformationFields::ComputeDeformationMap with the SL RK2
+ * scheme (src/DeformationFields.cpp:1189-1268, 1472-1585): y (host, 3 nl
+ * floats [y1 | y2 | y3]) holds physical coordinates in [0, 2 pi), unwrapped. */
+int claire_b200_deformation_map(claire_b200_ctx* ctx, int b, int inverse, float* y);
 /* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
  * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);

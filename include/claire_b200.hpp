@@ -119,6 +119,10 @@ class CLAIREInterface {
       for (int k = 0; k < 3; ++k) stats[k] = s[k];
     return e;
   }
+  // ComputeDeformationMap: y (3 nl floats, physical coordinates), or the inverse map
+  ErrorCode ComputeDeformationMap(float* y, bool inverse = false, int b = 0) {
+    return check(claire_b200_deformation_map(ctx_, b, inverse ? 1 : 0, y));
+  }
   ErrorCode GetStats(claire_b200_stats* st, int b = 0) const { return claire_b200_get_stats(ctx_, b, st); }
   claire_b200_ctx* handle() { return ctx_; }
 

@@ -1241,6 +1241,29 @@ def det_def_grad(v, nt, inverse=False):
     return jac, (float(jac.min()), float(jac.mean()), float(jac.max()))
 
 
+def deformation_map(v, nt, inverse=False):
+    """DeformationFields::ComputeDeformationMapSLRK2 (src/DeformationFields.cpp:
+    1472-1585): y = x on the grid (ComputeRegularGrid), then per time step
+    yt = y - ht v(y), y <- y - ht/2 (v(y) + v(yt)), v evaluated at the points by
+    tricubic interpolation; ht < 0 for the inverse map.  Returns y (3, ...) in
+    physical coordinates."""
+    v = np.asarray(v, np.float64)
+    shape = v.shape[1:]
+    ht = (-1.0 if inverse else 1.0) / nt
+    c = np.array([n / (2.0 * math.pi) for n in shape]).reshape(3, 1, 1, 1)  # grid units per length
+    grid = index_grid(shape)
+    u = np.zeros((3,) + shape)
+    for _ in range(nt):
+        q = grid + u
+        vy = np.stack([interp3(v[k], q) for k in range(3)])
+        ut = u - ht * c * vy
+        u = u - 0.5 * ht * c * vy
+        q = grid + ut
+        vyt = np.stack([interp3(v[k], q) for k in range(3)])
+        u = u - 0.5 * ht * c * vyt
+    return (grid + u) / c
+
+
 def gaussian_smooth(f: np.ndarray, sigma_cells=1.0) -> np.ndarray:
     """Spectral Gaussian smoothing (src/Preprocessing.cpp:1956-2056): multiply by
     exp(-1/2 sum_i k_i^2 (sigma_i h_i)^2), Nyquist index kept as +N/2."""

@@ -166,6 +166,27 @@ def test_det_def_grad_matches_oracle(cb, inverse):
     assert abs(gmn - mn) < 1e-5 and abs(gmx - mx) < 1e-5 and abs(gme - me) < 1e-6
 
 
+@pytest.mark.parametrize("inverse", [False, True])
+def test_deformation_map_matches_oracle(cb, inverse):
+    # DeformationFields::ComputeDeformationMapSLRK2 (src/DeformationFields.cpp:1472-1585)
+    n, nt = 32, 8
+    rng = np.random.Generator(np.random.PCG64(12))
+    v = R.velocity_random((n, n, n), rng, rms=0.3)
+    y = R.deformation_map(v, nt, inverse=inverse)
+    grid = R.index_grid((n, n, n)) * (2 * np.pi / n)
+    mR, mT, _ = c1_problem(n, 4)
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.SetInitialGuess(v.astype(np.float32))
+        yg = ci.ComputeDeformationMap(inverse=inverse)
+        # the map does not disturb what follows: the objective at v is unchanged
+        J1, _, _ = ci.EvaluateObjective(v.astype(np.float32))
+    assert rel(yg - grid, y - grid) < 1e-5  # the displacement part, y - x
+    assert np.max(np.abs(yg - grid)) > 0.05
+    prob = R.Problem(mR, mT, 4 * 2, R.Regularization("h1s", 1e-2))
+    assert abs(J1 - prob.objective(v)) <= 1e-5 * abs(J1)
+
+
 def test_det_def_grad_volume_preserving(cb):
     n, nt = 32, 4
     mR, mT, vstar = c1_problem(n, nt)   # divergence-free trig velocity
