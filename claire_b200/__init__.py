@@ -135,6 +135,7 @@ _signatures = {
     "claire_b200_write_nifti": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_read_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_deformation_map": (_I, [_P, _I, _I, _P]),
+    "claire_b200_displacement_field": (_I, [_P, _I, _P]),
     "claire_b200_write_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
@@ -581,6 +582,15 @@ class CLAIREInterface:
         _check(lib.claire_b200_deformation_map(self._ctx, b, int(bool(inverse)), y.ctypes.data_as(ctypes.c_void_p)),
                "ComputeDeformationMap", self._ctx)
         return y
+
+    def ComputeDisplacementField(self, b: int = 0):
+        """DeformationFields::ComputeDisplacementFieldSL at the current velocity:
+        u (3, n1, n2, n3), physical units."""
+        import numpy as np
+        u = np.empty((3,) + tuple(self.shape), dtype=np.float32)
+        _check(lib.claire_b200_displacement_field(self._ctx, b, u.ctypes.data_as(ctypes.c_void_p)),
+               "ComputeDisplacementField", self._ctx)
+        return u
 
     def GetAdjoint(self, b: int = 0):
         import numpy as np

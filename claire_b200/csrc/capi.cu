@@ -668,6 +668,16 @@ int claire_b200_deformation_map(claire_b200_ctx* c, int b, int inverse, float* y
   return CB_OK;
 }
 
+int claire_b200_displacement_field(claire_b200_ctx* c, int b, float* u) {
+  if (!c || !u || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  std::vector<int> sel(s.B, 0);
+  sel[b] = 1;
+  int e = s.displacement_field(sel);
+  if (e) return cuda_status(e);
+  return copy_out(s, u, s.x + b * 3 * s.n, 3 * s.n, 0);
+}
+
 int claire_b200_get_adjoint(claire_b200_ctx* c, int b, float* lambda0, float* body_force) {
   if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

@@ -1068,6 +1068,27 @@ int Solver::deformation_map(const std::vector<int>& sel, bool inverse) {
   return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
 }
 
+// Displacement field by the SL scheme, DeformationFields::
+// ComputeDisplacementFieldSL (src/DeformationFields.cpp:1816-1909): with the
+// state characteristic X of v, u^0 = 0 and u^{j+1} = u^j(X) + ht/2 (v(X) + v).
+int Solver::displacement_field(const std::vector<int>& sel) {
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(characteristic(v, 1.f, dact));
+  float *u = x, *ux = r, *vx = z;
+  CB_TRY(launch_interp(v, 3 * n, n, disp_st, 3 * n, tab_st, TP, vx, 3 * n, n, 3, B, d, dact, stream));
+  CB_TRY(launch_fill(u, 3 * n, 0.f, 3 * n, B, dact, stream));
+  note_launches(2);
+  for (int j = 0; j < nt; ++j) {
+    CB_TRY(launch_interp(u, 3 * n, n, disp_st, 3 * n, tab_st, TP, ux, 3 * n, n, 3, B, d, dact, stream));
+    CB_TRY(launch_lincomb(u, 3 * n, ux, 3 * n, nullptr, 1.0, vx, 3 * n, nullptr, 0.5 * ht, 3 * n, B, dact, stream));
+    CB_TRY(launch_lincomb(u, 3 * n, u, 3 * n, nullptr, 1.0, v, 3 * n, nullptr, 0.5 * ht, 3 * n, B, dact, stream));
+    note_launches(3);
+  }
+  for (int b = 0; b < B; ++b)
+    if (sel[b]) state_of[b] = 0;  // the state characteristic is v's, but the levels are not solved
+  return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
+}
+
 // ---------------------------------------------------------------------------
 // public single-shot operations
 // ---------------------------------------------------------------------------

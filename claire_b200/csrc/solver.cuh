@@ -66,6 +66,8 @@ class Solver {
   int det_def_grad(const std::vector<int>& sel, bool inverse, std::vector<double>& stats);
   // deformation map y - x in grid units (3 fields per problem, in x)
   int deformation_map(const std::vector<int>& sel, bool inverse);
+  // displacement field u (3 fields per problem, physical units, in x)
+  int displacement_field(const std::vector<int>& sel);
   int final_state(float* m1, int b);
   // images of problem b from device arrays (n floats each), converted to the
   // storage type; not synchronised

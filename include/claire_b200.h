@@ -173,6 +173,10 @@ int claire_b200_det_def_grad(claire_b200_ctx* ctx, int b, int inverse, float* ja
  * scheme (src/DeformationFields.cpp:1189-1268, 1472-1585): y (host, 3 nl
  * floats [y1 | y2 | y3]) holds physical coordinates in [0, 2 pi), unwrapped. */
 int claire_b200_deformation_map(claire_b200_ctx* ctx, int b, int inverse, float* y);
+/* Displacement field u of problem b at its current velocity by the SL scheme,
+ * DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:
+ * 1816-1909): u (host, 3 nl floats), physical units. */
+int claire_b200_displacement_field(claire_b200_ctx* ctx, int b, float* u);
 /* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
  * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);

@@ -1264,6 +1264,20 @@ def deformation_map(v, nt, inverse=False):
     return (grid + u) / c
 
 
+def displacement_field(v, nt):
+    """DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:
+    1816-1909): with the state characteristic X, u^0 = 0 and
+    u^{j+1} = u^j(X) + ht/2 (v(X) + v)."""
+    v = np.asarray(v, np.float64)
+    ht = 1.0 / nt
+    tr = Trajectory(v, nt, "state")
+    vx = tr.interp_vec(v)
+    u = np.zeros_like(v)
+    for _ in range(nt):
+        u = tr.interp_vec(u) + 0.5 * ht * (vx + v)
+    return u
+
+
 def gaussian_smooth(f: np.ndarray, sigma_cells=1.0) -> np.ndarray:
     """Spectral Gaussian smoothing (src/Preprocessing.cpp:1956-2056): multiply by
     exp(-1/2 sum_i k_i^2 (sigma_i h_i)^2), Nyquist index kept as +N/2."""

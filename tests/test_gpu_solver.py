@@ -187,6 +187,25 @@ def test_deformation_map_matches_oracle(cb, inverse):
     assert abs(J1 - prob.objective(v)) <= 1e-5 * abs(J1)
 
 
+def test_displacement_field_matches_oracle(cb):
+    # DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:1816-1909)
+    n, nt = 32, 8
+    rng = np.random.Generator(np.random.PCG64(13))
+    v = R.velocity_random((n, n, n), rng, rms=0.3)
+    u = R.displacement_field(v, nt)
+    mR, mT, _ = c1_problem(n, 4)
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.SetInitialGuess(v.astype(np.float32))
+        ug = ci.ComputeDisplacementField()
+        y = ci.ComputeDeformationMap()
+    assert rel(ug, u) < 1e-5
+    # the Eulerian SL displacement and the Lagrangian map y agree to the
+    # discretisation: u(x) ~ x - y(x)
+    grid = R.index_grid((n, n, n)) * (2 * np.pi / n)
+    assert rel(ug, grid - y) < 5e-2
+
+
 def test_det_def_grad_volume_preserving(cb):
     n, nt = 32, 4
     mR, mT, vstar = c1_problem(n, nt)   # divergence-free trig velocity
