@@ -136,6 +136,7 @@ _signatures = {
     "claire_b200_read_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_deformation_map": (_I, [_P, _I, _I, _P]),
     "claire_b200_displacement_field": (_I, [_P, _I, _P]),
+    "claire_b200_def_grad": (_I, [_P, _I, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "claire_b200_write_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
@@ -582,6 +583,17 @@ class CLAIREInterface:
         _check(lib.claire_b200_deformation_map(self._ctx, b, int(bool(inverse)), y.ctypes.data_as(ctypes.c_void_p)),
                "ComputeDeformationMap", self._ctx)
         return y
+
+    def ComputeDefGrad(self, b: int = 0):
+        """DeformationFields::ComputeDefGrad (SL) at the current velocity:
+        (F (9, n1, n2, n3) with F_ab at 3a + b, det F, (min, mean, max))."""
+        import numpy as np
+        F = np.empty((9,) + tuple(self.shape), dtype=np.float32)
+        det = np.empty(tuple(self.shape), dtype=np.float32)
+        st = (ctypes.c_double * 3)()
+        _check(lib.claire_b200_def_grad(self._ctx, b, F.ctypes.data_as(ctypes.c_void_p),
+                                        det.ctypes.data_as(ctypes.c_void_p), st), "ComputeDefGrad", self._ctx)
+        return F, det, (st[0], st[1], st[2])
 
     def ComputeDisplacementField(self, b: int = 0):
         """DeformationFields::ComputeDisplacementFieldSL at the current velocity:

@@ -668,6 +668,39 @@ int claire_b200_deformation_map(claire_b200_ctx* c, int b, int inverse, float* y
   return CB_OK;
 }
 
+int claire_b200_def_grad(claire_b200_ctx* c, int b, float* F, float* det, double stats[3]) {
+  if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  const long long n = s.n;
+  std::vector<float> own;
+  float* F9 = F;
+  if (!F9) {
+    own.resize((size_t)(9 * n));
+    F9 = own.data();
+  }
+  int e = s.def_grad(b, F9);
+  if (e) return cuda_status(e);
+  // det F and its min / mean / max (ComputeDefGrad, src/DeformationFields.cpp:902-935)
+  double mn = 1e300, mx = -1e300, sum = 0.0;
+  for (long long i = 0; i < n; ++i) {
+    const float* f = F9;
+    const float j11 = f[i], j12 = f[n + i], j13 = f[2 * n + i], j21 = f[3 * n + i], j22 = f[4 * n + i],
+                j23 = f[5 * n + i], j31 = f[6 * n + i], j32 = f[7 * n + i], j33 = f[8 * n + i];
+    const float phi = j11 * j22 * j33 + j12 * j23 * j31 + j13 * j21 * j32 - j13 * j22 * j31 - j12 * j21 * j33 -
+                      j11 * j23 * j32;
+    if (det) det[i] = phi;
+    mn = std::min(mn, (double)phi);
+    mx = std::max(mx, (double)phi);
+    sum += phi;
+  }
+  if (stats) {
+    stats[0] = mn;
+    stats[1] = sum / (double)n;
+    stats[2] = mx;
+  }
+  return CB_OK;
+}
+
 int claire_b200_displacement_field(claire_b200_ctx* c, int b, float* u) {
   if (!c || !u || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

@@ -278,6 +278,48 @@ __global__ void k_body_force(const float* __restrict__ lam, long long lp, const 
         make_float4(scale * acc[k].x, scale * acc[k].y, scale * acc[k].z, scale * acc[k].w);
 }
 
+// Second RK2 stage of the deformation-gradient transport
+// (DeformationFields::ComputeDefGradSL, src/DeformationFields.cpp:1060-1085),
+// as written there: with tensors stored component-major (T_ab at T + (3a+b)n),
+// rhs_ab = sum_k gvX_ka jX_kb and
+// j_ab = jX_ab + ht/2 (rhs_ab + gvX_ab + ht sum_k gv_ka rhs_kb).
+__global__ void k_defgrad_step(const float* __restrict__ jx, const float* __restrict__ gvx,
+                               const float* __restrict__ gv, float* __restrict__ j, long long pstride, float ht,
+                               long long n, const int* __restrict__ active) {
+  const int p = blockIdx.y;
+  if (active && !active[p]) return;
+  const long long off = p * pstride;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float JX[9], GX[9], G[9], rhs[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      JX[c] = jx[off + c * n + i];
+      GX[c] = gvx[off + c * n + i];
+      G[c] = gv[off + c * n + i];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        rhs[3 * a + b] = GX[a] * JX[b] + GX[3 + a] * JX[3 + b] + GX[6 + a] * JX[6 + b];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const float s = G[a] * rhs[b] + G[3 + a] * rhs[3 + b] + G[6 + a] * rhs[6 + b];
+        j[off + (3 * a + b) * n + i] = JX[3 * a + b] + 0.5f * ht * (rhs[3 * a + b] + (GX[3 * a + b] + ht * s));
+      }
+  }
+}
+
+int launch_defgrad_step(const float* jx, const float* gvx, const float* gv, float* j, long long pstride, float ht,
+                        int nprob, long long n, const int* active, cudaStream_t s) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_defgrad_step<<<dim3((unsigned)blocks, nprob), 256, 0, s>>>(jx, gvx, gv, j, pstride, ht, n, active);
+  return (int)cudaGetLastError();
+}
+
 __global__ void k_incstate_source(const float* __restrict__ gx, long long gxp, const float* __restrict__ vtx,
                                   long long vtxp, const float* __restrict__ gm, long long gmp,
                                   const float* __restrict__ vt, long long vtp, float* __restrict__ s, long long sp,

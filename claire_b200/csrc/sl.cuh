@@ -144,6 +144,11 @@ int launch_incstate_source(const float* gx, long long gxp, const float* vtx, lon
                            long long gmp, const float* vt, long long vtp, float* src, long long sp, int nt,
                            float ht, int nprob, long long n, const int* active, cudaStream_t s);
 
+// Second RK2 stage of the deformation-gradient transport (9-component
+// tensors jX, gv(X), gv, output j; problem p at base + p * pstride).
+int launch_defgrad_step(const float* jx, const float* gvx, const float* gv, float* j, long long pstride, float ht,
+                        int nprob, long long n, const int* active, cudaStream_t s);
+
 int launch_lincomb(float* y, long long yp, const float* a, long long ap, const double* ca, double sa,
                    const float* b, long long bp, const double* cb, double sb, long long len,
                    int nprob, const int* active, cudaStream_t s);

@@ -1089,6 +1089,41 @@ int Solver::displacement_field(const std::vector<int>& sel) {
   return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : CB_ERR_CUDA;
 }
 
+// Deformation gradient by the SL scheme, DeformationFields::ComputeDefGrad /
+// ComputeDefGradSL (src/DeformationFields.cpp:821-955, 956-1117): F^0 = I,
+// gv = grad v (spectral), gv(X) on the state characteristic, and per time step
+// F <- the second RK2 stage of k_defgrad_step applied to F(X).  Work arrays of
+// 36 n floats are allocated for the call.
+int Solver::def_grad(int b, float* F9) {
+  std::vector<int> sel(B, 0);
+  sel[b] = 1;
+  CB_TRY(upload_mask(sel, dact));
+  CB_TRY(characteristic(v, 1.f, dact));
+  float* w = nullptr;
+  if (cudaMalloc(&w, sizeof(float) * 36 * n * B) != cudaSuccess) {
+    cudaGetLastError();
+    err = "deformation gradient: allocation failed";
+    return CB_ERR_ALLOC;
+  }
+  float *F = w, *FX = w + 9 * n * B, *gv = w + 18 * n * B, *gvx = w + 27 * n * B;
+  const long long P9 = 9 * n;
+  int e = grad_fields(v, 3 * n, n, gv, P9, 3 * n, 3, dact);  // gv[3k + a] = d_a v_k
+  if (!e) e = launch_interp(gv, P9, n, disp_st, 3 * n, tab_st, TP, gvx, P9, n, 9, B, d, dact, stream);
+  for (int c = 0; c < 9 && !e; ++c)
+    e = launch_fill(F + c * n, P9, (c % 4 == 0) ? 1.f : 0.f, n, B, dact, stream);
+  for (int j = 0; j < nt && !e; ++j) {
+    e = launch_interp(F, P9, n, disp_st, 3 * n, tab_st, TP, FX, P9, n, 9, B, d, dact, stream);
+    if (!e) e = launch_defgrad_step(FX, gvx, gv, F, P9, ht, B, n, dact, stream);
+  }
+  note_launches(2 + 9 + 2 * nt);
+  if (!e && (cudaMemcpyAsync(F9, F + b * P9, sizeof(float) * P9, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+             cudaStreamSynchronize(stream) != cudaSuccess))
+    e = CB_ERR_CUDA;
+  cudaFree(w);
+  state_of[b] = 0;  // the state characteristic's tables were rebuilt for v
+  return e ? (e < 0 ? e : CB_ERR_CUDA) : 0;
+}
+
 // ---------------------------------------------------------------------------
 // public single-shot operations
 // ---------------------------------------------------------------------------

@@ -68,6 +68,9 @@ class Solver {
   int deformation_map(const std::vector<int>& sel, bool inverse);
   // displacement field u (3 fields per problem, physical units, in x)
   int displacement_field(const std::vector<int>& sel);
+  // deformation gradient F of problem b (9 fields, component-major) into the
+  // host array F9 (9 n floats)
+  int def_grad(int b, float* F9);
   int final_state(float* m1, int b);
   // images of problem b from device arrays (n floats each), converted to the
   // storage type; not synchronised

@@ -177,6 +177,12 @@ int claire_b200_deformation_map(claire_b200_ctx* ctx, int b, int inverse, float*
  * DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:
  * 1816-1909): u (host, 3 nl floats), physical units. */
 int claire_b200_displacement_field(claire_b200_ctx* ctx, int b, float* u);
+/* Deformation gradient F of problem b at its current velocity by the SL
+ * scheme, DeformationFields::ComputeDefGrad / ComputeDefGradSL
+ * (src/DeformationFields.cpp:821-1117): F (host, 9 nl floats, F_ab at
+ * (3a + b) nl, may be NULL), det F (host, nl floats, may be NULL) and its
+ * {min, mean, max} (may be NULL). */
+int claire_b200_def_grad(claire_b200_ctx* ctx, int b, float* F, float* det, double stats[3]);
 /* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
  * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);

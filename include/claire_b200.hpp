@@ -119,6 +119,11 @@ class CLAIREInterface {
       for (int k = 0; k < 3; ++k) stats[k] = s[k];
     return e;
   }
+  // ComputeDefGrad: F (9 nl floats, F_ab at (3a + b) nl), det F (nl floats) and
+  // {min, mean, max}; any of them may be null
+  ErrorCode ComputeDefGrad(float* F = nullptr, float* det = nullptr, double* stats = nullptr, int b = 0) {
+    return check(claire_b200_def_grad(ctx_, b, F, det, stats));
+  }
   // ComputeDeformationMap: y (3 nl floats, physical coordinates), or the inverse map
   ErrorCode ComputeDeformationMap(float* y, bool inverse = false, int b = 0) {
     return check(claire_b200_deformation_map(ctx_, b, inverse ? 1 : 0, y));

@@ -1264,6 +1264,31 @@ def deformation_map(v, nt, inverse=False):
     return (grid + u) / c
 
 
+def def_grad(v, nt):
+    """DeformationFields::ComputeDefGrad / ComputeDefGradSL
+    (src/DeformationFields.cpp:821-1117), tensors component-major (F_ab at
+    index 3a + b): F^0 = I, gv_ka = d_a v_k, and per step with FX = F(X),
+    gvX = gv(X), rhs_ab = sum_k gvX_ka FX_kb,
+    F_ab = FX_ab + ht/2 (rhs_ab + gvX_ab + ht sum_k gv_ka rhs_kb), as written
+    there.  Returns (F, det F)."""
+    v = np.asarray(v, np.float64)
+    ht = 1.0 / nt
+    tr = Trajectory(v, nt, "state")
+    gv = np.concatenate([grad(v[k]) for k in range(3)])
+    gvx = np.stack([tr.interp(gv[c]) for c in range(9)])
+    F = np.zeros((9,) + v.shape[1:])
+    F[0] = F[4] = F[8] = 1.0
+    for _ in range(nt):
+        FX = np.stack([tr.interp(F[c]) for c in range(9)])
+        rhs = np.stack([sum(gvx[3 * k + a] * FX[3 * k + b] for k in range(3)) for a in range(3) for b in range(3)])
+        F = np.stack([FX[3 * a + b] + 0.5 * ht * (rhs[3 * a + b] + gvx[3 * a + b]
+                                                   + ht * sum(gv[3 * k + a] * rhs[3 * k + b] for k in range(3)))
+                      for a in range(3) for b in range(3)])
+    det = (F[0] * F[4] * F[8] + F[1] * F[5] * F[6] + F[2] * F[3] * F[7]
+           - F[2] * F[4] * F[6] - F[1] * F[3] * F[8] - F[0] * F[5] * F[7])
+    return F, det
+
+
 def displacement_field(v, nt):
     """DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:
     1816-1909): with the state characteristic X, u^0 = 0 and
