@@ -137,6 +137,7 @@ _signatures = {
     "claire_b200_deformation_map": (_I, [_P, _I, _I, _P]),
     "claire_b200_displacement_field": (_I, [_P, _I, _P]),
     "claire_b200_def_grad": (_I, [_P, _I, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "claire_b200_det_def_grad_disp": (_I, [_P, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "claire_b200_write_bin": (_I, [ctypes.c_char_p, _IA, _P]),
     "claire_b200_preprocess": (_I, [_P, _IA, _I, _DA, _P]),
     "claire_b200_set_fft_variant": (_I, [_I, _I]),
@@ -594,6 +595,16 @@ class CLAIREInterface:
         _check(lib.claire_b200_def_grad(self._ctx, b, F.ctypes.data_as(ctypes.c_void_p),
                                         det.ctypes.data_as(ctypes.c_void_p), st), "ComputeDefGrad", self._ctx)
         return F, det, (st[0], st[1], st[2])
+
+    def ComputeDetDefGradViaDispField(self, b: int = 0):
+        """det(grad y) through the displacement field (-detdefgradfromdeffield):
+        (det field, (min, mean, max))."""
+        import numpy as np
+        jac = np.empty(tuple(self.shape), dtype=np.float32)
+        st = (ctypes.c_double * 3)()
+        _check(lib.claire_b200_det_def_grad_disp(self._ctx, b, jac.ctypes.data_as(ctypes.c_void_p), st),
+               "ComputeDetDefGradViaDispField", self._ctx)
+        return jac, (st[0], st[1], st[2])
 
     def ComputeDisplacementField(self, b: int = 0):
         """DeformationFields::ComputeDisplacementFieldSL at the current velocity:

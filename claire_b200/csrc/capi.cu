@@ -701,6 +701,35 @@ int claire_b200_def_grad(claire_b200_ctx* c, int b, float* F, float* det, double
   return CB_OK;
 }
 
+int claire_b200_det_def_grad_disp(claire_b200_ctx* c, int b, float* jac, double stats[3]) {
+  if (!c || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
+  Solver& s = c->solver;
+  const long long n = s.n;
+  std::vector<float> g((size_t)(9 * n));
+  int e = s.disp_grad(b, g.data());
+  if (e) return cuda_status(e);
+  // ComputeDetDefGradViaDispField (src/DeformationFields.cpp:788-800), with
+  // its signs as written (the terms with three off-diagonal entries enter with +)
+  double mn = 1e300, mx = -1e300, sum = 0.0;
+  const float* u = g.data();
+  for (long long i = 0; i < n; ++i) {
+    const float g11 = u[i], g12 = u[n + i], g13 = u[2 * n + i], g21 = u[3 * n + i], g22 = u[4 * n + i],
+                g23 = u[5 * n + i], g31 = u[6 * n + i], g32 = u[7 * n + i], g33 = u[8 * n + i];
+    const float phi = (1.f - g11) * (1.f - g22) * (1.f - g33) + g12 * g23 * g31 + g13 * g21 * g32 -
+                      g13 * (1.f - g22) * g31 - g12 * g21 * (1.f - g33) - (1.f - g11) * g23 * g32;
+    if (jac) jac[i] = phi;
+    mn = std::min(mn, (double)phi);
+    mx = std::max(mx, (double)phi);
+    sum += phi;
+  }
+  if (stats) {
+    stats[0] = mn;
+    stats[1] = sum / (double)n;
+    stats[2] = mx;
+  }
+  return CB_OK;
+}
+
 int claire_b200_displacement_field(claire_b200_ctx* c, int b, float* u) {
   if (!c || !u || b < 0 || b >= c->solver.B) return CB_ERR_ARG;
   Solver& s = c->solver;

@@ -1124,6 +1124,29 @@ int Solver::def_grad(int b, float* F9) {
   return e ? (e < 0 ? e : CB_ERR_CUDA) : 0;
 }
 
+// Gradient of the SL displacement field, the first half of
+// DeformationFields::ComputeDetDefGradViaDispField (src/DeformationFields.cpp:
+// 745-815): u by displacement_field, then the spectral gradient of each
+// component.
+int Solver::disp_grad(int b, float* G9) {
+  std::vector<int> sel(B, 0);
+  sel[b] = 1;
+  CB_TRY(displacement_field(sel));
+  float* w = nullptr;
+  if (cudaMalloc(&w, sizeof(float) * 9 * n * B) != cudaSuccess) {
+    cudaGetLastError();
+    err = "displacement gradient: allocation failed";
+    return CB_ERR_ALLOC;
+  }
+  int e = grad_fields(x, 3 * n, n, w, 9 * n, 3 * n, 3, dact);
+  if (!e && (cudaMemcpyAsync(G9, w + b * 9 * n, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, stream) !=
+                 cudaSuccess ||
+             cudaStreamSynchronize(stream) != cudaSuccess))
+    e = CB_ERR_CUDA;
+  cudaFree(w);
+  return e ? (e < 0 ? e : CB_ERR_CUDA) : 0;
+}
+
 // ---------------------------------------------------------------------------
 // public single-shot operations
 // ---------------------------------------------------------------------------

@@ -71,6 +71,9 @@ class Solver {
   // deformation gradient F of problem b (9 fields, component-major) into the
   // host array F9 (9 n floats)
   int def_grad(int b, float* F9);
+  // spectral gradient of problem b's displacement field (9 fields, gu_ka =
+  // d_a u_k at index 3k + a) into the host array G9 (9 n floats)
+  int disp_grad(int b, float* G9);
   int final_state(float* m1, int b);
   // images of problem b from device arrays (n floats each), converted to the
   // storage type; not synchronised

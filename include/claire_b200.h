@@ -183,6 +183,12 @@ int claire_b200_displacement_field(claire_b200_ctx* ctx, int b, float* u);
  * (3a + b) nl, may be NULL), det F (host, nl floats, may be NULL) and its
  * {min, mean, max} (may be NULL). */
 int claire_b200_def_grad(claire_b200_ctx* ctx, int b, float* F, float* det, double stats[3]);
+/* det(grad y) through the displacement field (-detdefgradfromdeffield,
+ * DeformationFields::ComputeDetDefGradViaDispField,
+ * src/DeformationFields.cpp:745-815): the SL displacement field u, its
+ * spectral gradient, and det(I - grad u) with the reference's signs; jac
+ * (host, nl floats) and {min, mean, max} may be NULL. */
+int claire_b200_det_def_grad_disp(claire_b200_ctx* ctx, int b, float* jac, double stats[3]);
 /* Adjoint state lambda(t=0) and body force b of the last adjoint solve (the
  * last gradient evaluation or Hessian matvec of problem b). */
 int claire_b200_get_adjoint(claire_b200_ctx* ctx, int b, float* lambda0, float* body_force);

@@ -1289,6 +1289,17 @@ def def_grad(v, nt):
     return F, det
 
 
+def det_def_grad_via_disp(v, nt):
+    """DeformationFields::ComputeDetDefGradViaDispField (src/DeformationFields.cpp:
+    745-815): gradient of the SL displacement field and det(I - grad u) with
+    the reference's signs (the products of three off-diagonal entries enter
+    with +)."""
+    u = displacement_field(v, nt)
+    g = np.concatenate([grad(u[k]) for k in range(3)])
+    return ((1 - g[0]) * (1 - g[4]) * (1 - g[8]) + g[1] * g[5] * g[6] + g[2] * g[3] * g[7]
+            - g[2] * (1 - g[4]) * g[6] - g[1] * g[3] * (1 - g[8]) - (1 - g[0]) * g[5] * g[7])
+
+
 def displacement_field(v, nt):
     """DeformationFields::ComputeDisplacementFieldSL (src/DeformationFields.cpp:
     1816-1909): with the state characteristic X, u^0 = 0 and

@@ -230,6 +230,21 @@ def test_def_grad_matches_oracle(cb):
     assert rel(detg, jac) < 0.15
 
 
+def test_det_def_grad_via_displacement_matches_oracle(cb):
+    # -detdefgradfromdeffield: DeformationFields::ComputeDetDefGradViaDispField
+    n, nt = 32, 8
+    rng = np.random.Generator(np.random.PCG64(15))
+    v = R.velocity_random((n, n, n), rng, rms=0.1)
+    ref = R.det_def_grad_via_disp(v, nt)
+    mR, mT, _ = c1_problem(n, 4)
+    with cb.CLAIREInterface(make_opt(cb, n, nt, "h1s", 1e-2)) as ci:
+        ci.set_images(mR, mT)
+        ci.SetInitialGuess(v.astype(np.float32))
+        jac, (mn, me, mx) = ci.ComputeDetDefGradViaDispField()
+    assert rel(jac - 1.0, ref - 1.0) < 1e-4
+    assert abs(mn - ref.min()) < 1e-5 and abs(mx - ref.max()) < 1e-5 and abs(me - ref.mean()) < 1e-5
+
+
 def test_det_def_grad_volume_preserving(cb):
     n, nt = 32, 4
     mR, mT, vstar = c1_problem(n, nt)   # divergence-free trig velocity
