@@ -149,3 +149,33 @@ def test_two_level_refusals(cb):
         with pytest.raises(cb.ClaireError) as e:
             srv.submit(opt2(cb, n, nt, "h1s", 1e-2), mR, mT)
         assert e.value.code == -6
+
+
+def test_two_level_batch_equals_single(cb):
+    # each problem of a batch runs its own coarse solve (per-problem masks and
+    # tolerances): a problem gives the same result alone and in a batch
+    n, nt = 32, 4
+    mR, mT, _, _ = problem(n, nt)
+    rng = np.random.default_rng(21)
+    probs = [(mR, mT)]
+    for _ in range(2):
+        shift = tuple(int(s) for s in rng.integers(1, n, size=3))
+        probs.append((np.roll(mR, shift, axis=(0, 1, 2)).copy(), mT))
+    opt = opt2(cb, n, nt, "h1s", 1e-2, "-maxit", "5", "-opttol", "1e-2")
+    single = []
+    for a, b in probs:
+        with cb.CLAIREInterface(opt) as ci:
+            ci.set_images(a, b)
+            ci.Run()
+            single.append((np.asarray(ci.GetSolution()), ci.stats()))
+    with cb.CLAIREInterface(opt, nbatch=len(probs)) as ci:
+        for k, (a, b) in enumerate(probs):
+            ci.set_images(a, b, k)
+        ci.Run()
+        for k in range(len(probs)):
+            st = ci.stats(k)
+            facts = dict(k=k, gn=(st["gn_iterations"], single[k][1]["gn_iterations"]),
+                         pc=(st["pc_matvecs"], single[k][1]["pc_matvecs"]))
+            assert st["gn_iterations"] == single[k][1]["gn_iterations"], facts
+            assert st["pcg_iterations"] == single[k][1]["pcg_iterations"], facts
+            assert rel(ci.GetSolution(k), single[k][0]) < 1e-6, facts
