@@ -349,6 +349,12 @@ def tune(cb, sizes, nbatch):
     return out
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_gather_scale launch over
+# one 128^3 problem of the workload (42,410,240 bytes; ncu --set full, the
+# command in profiles/k_gather_scale_128.md), per point
+GATHER_SCALE_DRAM_BYTES_PER_POINT = 42410240 / 128 ** 3
+
+
 def roofline(cb, a, ci, load_device, B):
     """Dominant kernel of the registration: the adjoint time step
     k_gather_scale (lambda^{l-1} = c * lambda^l(X), tricubic tile gather).
@@ -357,8 +363,9 @@ def roofline(cb, a, ci, load_device, B):
     timers on; every adjoint-step launch is bracketed by CUDA events on the
     solve's stream.  Algorithmic bytes per launch (B problems of n points):
     field 4n + displacement 12n + factor c 4n + output 4n = 24n per problem.
-    `traffic` is DRAM bytes per launch from an ncu capture of the same kernel
-    in the same workload (profiles/gather_traffic.json), scaled to B problems.
+    `traffic` is DRAM bytes per launch: GATHER_SCALE_DRAM_BYTES_PER_POINT (an
+    ncu capture of the same kernel in the same workload) times the points of
+    the launch.
     """
     import torch
     n = a.n ** 3
@@ -378,14 +385,7 @@ def roofline(cb, a, ci, load_device, B):
     avg_ms = ms / max(cnt, 1)
     bytes_ = 24 * n * B
     achieved = bytes_ / (avg_ms / 1e3) / 1e9
-    traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "gather_traffic.json")))
-        per_problem = prof.get(f"k_gather_scale_{a.n}")
-        if per_problem is not None:
-            traffic = float(per_problem) * B
-    except Exception:
-        pass
+    traffic = GATHER_SCALE_DRAM_BYTES_PER_POINT * n * B
     return {"kernel": "k_gather_scale (adjoint time step: tricubic tile gather x per-point factor)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "algorithmic_bytes": bytes_,
@@ -393,116 +393,159 @@ def roofline(cb, a, ci, load_device, B):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline (oracle port, numpy, host cores)
+# CPU legs: the C++/OpenMP restatement of the reference (oracle/cpu_ref.cpp)
 # ---------------------------------------------------------------------------
-def _worker_ready(delay):
-    """Start-up task of cpu_op_times' workers: import the oracle, then hold the
-    worker long enough that every worker of the pool receives one."""
-    from oracle import claire_ref  # noqa: F401
-    time.sleep(delay)
-    return os.getpid()
-
-
-def _gather_slab(payload):
-    """Worker of cpu_op_times: one tricubic gather of field f at the slab's points."""
-    from oracle import claire_ref as R
-    f, q, shape = payload
-    t = time.perf_counter()
-    R.Stencil(q, shape).apply(f)
-    return time.perf_counter() - t
-
-
-def cpu_workers():
-    """Host threads the CPU baseline uses: every core this process may run on
-    (capped at 64 so that starting the workers stays short)."""
+def cpu_cores():
+    """Host threads the CPU legs use: every core this process may run on."""
     try:
-        k = len(os.sched_getaffinity(0))
+        return len(os.sched_getaffinity(0))
     except AttributeError:
-        k = os.cpu_count() or 1
-    return max(1, min(64, k))
+        return os.cpu_count() or 1
 
 
-def cpu_op_times(n, workers=None):
-    """Seconds for one tricubic gather of a scalar field and one 3D real FFT
-    (r2c or c2r) at n^3 with the oracle port (NumPy FP64) on `workers` host
-    cores: the gather's points split into slabs over a spawned process pool
-    (wall time of the whole gather, including handing each worker the field),
-    the FFT with pocketfft's own threads (scipy.fft, workers=...)."""
-    import multiprocessing
-    from concurrent.futures import ProcessPoolExecutor
-
-    import scipy.fft
-
-    from oracle import claire_ref as R
-    P = workers or cpu_workers()
-    rng = np.random.default_rng(0)
-    shape = (n, n, n)
-    f = rng.standard_normal(shape)
-    disp = rng.uniform(-2, 2, size=(3,) + shape)
-    q = (R.index_grid(shape) + disp).reshape(3, -1)
-    slabs = np.array_split(q, P, axis=1)
-    if P == 1:
-        t_gather = _gather_slab((f, q, shape))
-    else:
-        with ProcessPoolExecutor(P, mp_context=multiprocessing.get_context("spawn")) as ex:
-            list(ex.map(_worker_ready, [0.5] * P))  # every worker started and importing before timing
-            t = time.perf_counter()
-            list(ex.map(_gather_slab, [(f, s, shape) for s in slabs]))
-            t_gather = time.perf_counter() - t
-    scipy.fft.irfftn(scipy.fft.rfftn(f, workers=P), s=shape, workers=P)  # plan / thread warm-up
-    t = time.perf_counter()
-    fh = scipy.fft.rfftn(f, workers=P)
-    scipy.fft.irfftn(fh, s=shape, workers=P)
-    t_fft = (time.perf_counter() - t) / 2
-    return t_gather, t_fft, P
-
-
-def cpu_seconds_per_registration(stats, nt, t_gather, t_fft):
-    """Compose the reference's per-call operation counts (the call stacks of
-    its objective, gradient, Hessian matvec and preconditioner):
-    objective: 3 (trajectory) + nt gathers, 6 FFTs (H2 functional);
-    gradient: 3 + 1 + nt gathers, 4(nt+1) + 4 + 6 FFTs;
-    Hessian matvec: 5nt + 4 gathers, 12nt + 14 FFTs; preconditioner: 6 FFTs."""
-    t_obj = (3 + nt) * t_gather + 6 * t_fft
-    t_grad = (4 + nt) * t_gather + (4 * (nt + 1) + 10) * t_fft
-    t_mv = (5 * nt + 4) * t_gather + (12 * nt + 14) * t_fft
-    t_pc = 6 * t_fft
-    return (stats["obj_evals"] * t_obj + stats["grad_evals"] * t_grad + stats["hess_matvecs"] * t_mv
-            + stats["pc_matvecs"] * t_pc)
-
-
-def default_stats(a):
-    """Operation counts of one registration of the workload (measured on the GPU
-    path; used by the reference arm to size its sample)."""
-    path = os.path.join(ROOT, "profiles", "workload_counts.json")
+def cpu_model():
     try:
-        return json.load(open(path))[f"{a.n}_{a.nt}_{a.norm}_{a.maxit}"]
-    except Exception:
-        return {"obj_evals": 20, "grad_evals": 11, "hess_matvecs": 100, "pc_matvecs": 110}
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_problem(a, problem_index=0):
+    """Inputs of one benchmark problem built on the host (no GPU library):
+    the oracle's ellipsoid template and random velocity of the recipe (same
+    seeds and draws as claire_b200.synthetic), mR = transport of mT by that
+    velocity with the C++ restatement's own semi-Lagrangian solver (FP64)."""
+    from oracle import claire_ref as R
+    from oracle.cpu_ref import CpuRef
+    shape = (a.n,) * 3
+    rng = np.random.Generator(np.random.PCG64(R.problem_seed(1, problem_index)))
+    mT = R.template_ellipsoids(shape, rng)
+    v = R.velocity_random(shape, rng)
+    c = CpuRef(shape, a.nt, a.norm, a.beta, fp64=True, threads=cpu_cores())
+    mR = c.forward(v, mT)
+    c.close()
+    return mR, mT
+
+
+class CpuRegistrations:
+    """Registrations of the workload on the C++ restatement in FP32 (the
+    reference's single-precision build; its loop structure: 5 nt + 4 scalar
+    gathers and 12 nt + 14 3D real transforms per Hessian matvec), on all host
+    cores.  A step is one GN iteration; a registration's first step also runs
+    its initialisation (J0, ||g0|| at v = 0); the next registration starts
+    when the stopping test of the current one fires."""
+
+    def __init__(self, a, mR, mT):
+        from oracle.cpu_ref import CpuRef
+        self.a = a
+        self.cores = cpu_cores()
+        self.c = CpuRef((a.n,) * 3, a.nt, a.norm, a.beta, fp64=False, threads=self.cores)
+        self.c.set_gn(maxit=a.maxit, gttol=a.opttol)
+        self.c.set_images(mR, mT)
+        self.fresh = True
+        self.done = []       # (seconds, stats) of completed registrations
+        self.cur_s = 0.0
+
+    def step(self):
+        t = time.perf_counter()
+        if self.fresh:
+            self.c.reset_counters()
+            self.c.begin()
+            self.fresh = False
+        finished = self.c.step()
+        if finished:
+            self.c.finish()
+        dt = time.perf_counter() - t
+        self.cur_s += dt
+        if finished:
+            self.done.append((self.cur_s, self.c.stats()))
+            self.cur_s = 0.0
+            self.fresh = True
+        return dt
+
+    def summary(self, elapsed, gn_done):
+        """registrations/s: completed registrations over their own seconds; with
+        none completed, GN iterations per second over maxit (flagged)."""
+        if self.done:
+            secs = [d[0] for d in self.done]
+            value = len(secs) / sum(secs)
+            partial = False
+        else:
+            value = gn_done / elapsed / self.a.maxit
+            partial = True
+        st = [d[1] for d in self.done]
+        work = {k: float(np.mean([s[k] for s in st])) for k in
+                ("iters", "pcg_iters", "hess_matvecs", "pc_matvecs", "obj_evals", "grad_evals", "gathers",
+                 "ffts")} if st else None
+        return value, partial, {"registrations_completed": len(self.done),
+                                "seconds_per_registration": [round(d[0], 3) for d in self.done],
+                                "work_per_registration": work,
+                                "rel_mismatch": [round(s["rel_mismatch"], 6) for s in st],
+                                "extrapolated_from_gn_iterations": partial}
+
+    def close(self):
+        self.c.close()
+
+
+def cpu_baseline_sample(a, budget_s=20.0):
+    """cpu_baseline of our line: one registration of the workload on the C++
+    restatement (FP32, all host cores), GN iterations until it finishes or
+    `budget_s` has passed.  An unfinished run is extrapolated as GN iterations
+    per second over maxit: the first GN iterations carry the fewest Krylov
+    iterations (forcing sequence), so that figure overstates the CPU's speed."""
+    mR, mT = cpu_problem(a)
+    reg = CpuRegistrations(a, mR, mT)
+    t0 = time.perf_counter()
+    gn = 0
+    while time.perf_counter() - t0 < budget_s:
+        reg.step()
+        gn += 1
+        if reg.done:
+            break
+    elapsed = time.perf_counter() - t0
+    value, partial, info = reg.summary(elapsed, gn)
+    reg.close()
+    what = ("one complete registration" if not partial else
+            f"the first {gn} GN iterations of one registration ({elapsed:.1f} s), extrapolated to maxit={a.maxit}")
+    return {"value": value, "unit": "registrations/s", "cores": reg.cores, "kind": "port",
+            "sample": f"C++/OpenMP FP32 restatement of the reference (oracle/cpu_ref.cpp, reference loop "
+                      f"structure) on {reg.cores} host threads ({cpu_model()}), {a.n}^3 {a.norm} nt={a.nt}: "
+                      + what, **info}
 
 
 def run_reference(a, rank, world):
+    """Reference arm: the reference's CPU path as restated in C++ (the
+    reference itself needs MPI, PETSc 3.9.1, AccFFT and FFTW, none of which is
+    here), timed on the host cores.  Rank 0 only; W warm-up GN iterations of
+    one registration, then K timed GN iterations of fresh registrations."""
     if rank != 0:
         return
-    st = default_stats(a)
-    steps = []
-    for _ in range(max(1, a.steps)):
-        tg, tf, cores = cpu_op_times(a.n)
-        steps.append(cpu_seconds_per_registration(st, a.nt, tg, tf))
-    sec = float(np.median(steps))
-    val = 1.0 / sec
+    mR, mT = cpu_problem(a)
+    warm = CpuRegistrations(a, mR, mT)
+    for _ in range(a.warmup):
+        warm.step()
+    warm.close()
+    reg = CpuRegistrations(a, mR, mT)
+    times = [reg.step() for _ in range(a.steps)]
+    elapsed = sum(times)
+    value, partial, info = reg.summary(elapsed, len(times))
+    cores = reg.cores
+    reg.close()
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": "registrations/s", "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"single registration {a.n}^3 {a.norm} beta={a.beta} nt={a.nt} maxit={a.maxit}",
-                   "n": a.n, "nt": a.nt, "regnorm": a.norm, "beta": a.beta},
-        "cpu_baseline": {"value": val, "unit": "registrations/s", "cores": cores, "kind": "port",
-                         "sample": f"oracle NumPy FP64 on {cores} host cores: one tricubic gather (points split "
-                                   f"over {cores} processes) + one r2c/c2r (pocketfft, {cores} threads) at {a.n}^3 "
-                                   "per step, composed with the reference's per-call operation counts of one "
-                                   "registration"},
-        "e2e": {"value": val, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed * 1e3 / max(1, a.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"single registrations {a.n}^3 {a.norm} beta={a.beta} nt={a.nt} maxit={a.maxit} "
+                               f"opttol={a.opttol}, one after another; a step is one GN iteration",
+                   "n": a.n, "nt": a.nt, "regnorm": a.norm, "beta": a.beta, **info},
+        "cpu_baseline": {"value": value, "unit": "registrations/s", "cores": cores, "kind": "port",
+                         "sample": f"C++/OpenMP FP32 restatement of the reference's CPU path (oracle/cpu_ref.cpp) "
+                                   f"on {cores} host threads ({cpu_model()}): {a.steps} GN iterations of "
+                                   "real registrations of the workload"},
+        "e2e": {"value": value, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -826,17 +869,7 @@ def main():
     s50 = float(np.percentile(ls, 50))
     s99 = float(np.percentile(ls, 99))
     st0 = r["stats"][0]
-    cpu = None
-    if not a.no_cpu:
-        t_gather, t_fft, cores = cpu_op_times(a.n)
-        mean_stats = {k: float(np.mean([s[k] for s in r["stats"]])) for k in
-                      ("obj_evals", "grad_evals", "hess_matvecs", "pc_matvecs")}
-        sec = cpu_seconds_per_registration(mean_stats, a.nt, t_gather, t_fft)
-        cpu = {"value": 1.0 / sec, "unit": "registrations/s", "cores": cores, "kind": "port",
-               "sample": f"oracle NumPy FP64 on {cores} host cores: one tricubic gather ({t_gather:.3f} s, "
-                         f"points split over {cores} processes) and one 3D real FFT ({t_fft:.4f} s, pocketfft "
-                         f"threads) at {a.n}^3, composed with this run's per-registration operation counts and "
-                         "the reference's per-call gather/FFT counts"}
+    cpu = None if a.no_cpu else cpu_baseline_sample(a)
     line = {
         "metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": r["total_ms"] / a.steps, "higher_is_better": True,

@@ -36,7 +36,9 @@ NORMS = {"l2": 0, "h1": 1, "h1s": 2, "h2": 3, "h2s": 4, "h3": 5, "h3s": 6}
 MODELS = {"compressible": 0, "stokes": 1, "relaxedstokes": 2}
 REG_KIND = {"gradient": 0, "inverse": 1, "sqrtinverse": 2}
 ERRORS = {-1: "invalid argument", -2: "allocation failed", -3: "CUDA error", -4: "numerical error (NaN)",
-          -5: "call out of order", -6: "unsupported grid size"}
+          -5: "call out of order", -6: "unsupported grid size",
+          -7: "too large (fixed workspace, free device memory or HBM budget)", -8: "request cancelled"}
+ERR_TOO_LARGE, ERR_CANCELLED = -7, -8
 
 
 class ClaireError(RuntimeError):
@@ -158,6 +160,7 @@ _signatures = {
     "claire_b200_server_wait": (_I, [_P, ctypes.c_longlong, _I, ctypes.POINTER(_I)]),
     "claire_b200_server_result": (_I, [_P, ctypes.c_longlong, _P, _P, ctypes.POINTER(ctypes.c_double)]),
     "claire_b200_server_info": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_I)]),
+    "claire_b200_server_cancel": (_I, [_P, ctypes.c_longlong]),
     "claire_b200_server_destroy": (_I, [_P]),
     "claire_b200_profile_read": (_I, [_P, _I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -747,7 +750,7 @@ def smooth(f, sigma=(1.0, 1.0, 1.0), out=None):
 # ---------------------------------------------------------------------------
 # serving: continuous batching of registrations (claire_b200_server_*)
 # ---------------------------------------------------------------------------
-REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 
 
 class Server:
@@ -806,6 +809,11 @@ class Server:
         _check(lib.claire_b200_server_result(self._srv, rid, v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st),
                                              ctypes.byref(lat)), "Server.result")
         return v, st.as_dict(), float(lat.value)
+
+    def cancel(self, rid: int) -> None:
+        """Cancel a queued request at once, or a running one at its pool's next
+        GN-iteration boundary (claire_b200_server_cancel)."""
+        _check(lib.claire_b200_server_cancel(self._srv, rid), "Server.cancel")
 
     def info(self) -> dict:
         pools, queued = ctypes.c_int(0), ctypes.c_int(0)

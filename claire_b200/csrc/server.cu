@@ -42,6 +42,7 @@ struct Request {
   claire_b200_stats stats{};
   int status = CB_REQ_QUEUED;
   int error = CB_OK;
+  bool cancel = false;        // cancellation asked for while running
   Clock::time_point t_submit{}, t_done{};
 };
 
@@ -77,12 +78,26 @@ namespace srv {
 
 struct Pool {
   claire_b200_opts key{};
-  Solver solver;
+  std::unique_ptr<Solver> solver;
   std::vector<long long> slot_req;  // request id per slot, 0 = free
   long long bytes = 0;
-  bool dead = false;  // worker has exited (memory released)
+  bool dead = false;    // worker is leaving: takes no more requests
+  bool exited = false;  // worker has released the memory and returns: the thread can be joined
   std::thread worker;
 };
+
+// Join and drop the pools whose workers have exited.  Called with s->mu held,
+// from client threads only (a worker never joins itself or another worker).
+static void reap_locked(claire_b200_server* s) {
+  for (auto it = s->pools.begin(); it != s->pools.end();) {
+    if ((*it)->exited) {
+      if ((*it)->worker.joinable()) (*it)->worker.join();
+      it = s->pools.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
 
 static long long pending_for(const claire_b200_server* s, const claire_b200_opts& key) {
   long long k = 0;
@@ -119,10 +134,11 @@ static void create_pools_locked(claire_b200_server* s) {
     auto pool = std::make_unique<Pool>();
     pool->key = r.opts;
     pool->key.verbosity = 0;
+    pool->solver = std::make_unique<Solver>();
     int caller_dev = 0;
     cudaGetDevice(&caller_dev);
     cudaSetDevice(s->opts.device);
-    const int e = pool->solver.init(pool->key, slots);
+    const int e = pool->solver->init(pool->key, slots);
     cudaSetDevice(caller_dev);
     if (e) {
       // this key cannot be served at all (unsupported grid, allocation failure)
@@ -134,7 +150,7 @@ static void create_pools_locked(claire_b200_server* s) {
       s->cv.notify_all();
       continue;
     }
-    pool->bytes = pool->solver.footprint();
+    pool->bytes = pool->solver->footprint();
     pool->slot_req.assign(slots, 0);
     s->used += pool->bytes;
     Pool* raw = pool.get();
@@ -218,7 +234,7 @@ static void fill_stats(const ProbState& ps, claire_b200_stats* st) {
 
 static void worker_main(claire_b200_server* s, Pool* p) {
   cudaSetDevice(s->opts.device);
-  Solver& sv = p->solver;
+  Solver& sv = *p->solver;
   const int S = sv.B;
   int err = CB_OK;
   while (true) {
@@ -226,6 +242,21 @@ static void worker_main(claire_b200_server* s, Pool* p) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (s->stop) break;
+      // cancelled requests leave their slots at this GN-iteration boundary
+      bool cancelled = false;
+      for (int b = 0; b < S; ++b) {
+        if (!p->slot_req[b]) continue;
+        Request& r = s->reqs.at(p->slot_req[b]);
+        if (!r.cancel) continue;
+        r.status = CB_REQ_CANCELLED;
+        r.error = CB_ERR_CANCELLED;
+        r.t_done = Clock::now();
+        p->slot_req[b] = 0;
+        sv.ps[b].running = false;
+        sv.ps[b].done = true;
+        cancelled = true;
+      }
+      if (cancelled) s->cv.notify_all();
       bool running = false;
       for (int b = 0; b < S; ++b) running |= p->slot_req[b] != 0;
       if (!running && s->opts.batch_window_us > 0) {
@@ -312,13 +343,13 @@ static void worker_main(claire_b200_server* s, Pool* p) {
       if (p->slot_req[b]) fail_request(s, p->slot_req[b], err ? err : CB_ERR_STATE);
     p->dead = true;
   }
-  sv.~Solver();
-  new (&sv) Solver();
+  p->solver.reset();
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->used -= p->bytes;
     p->bytes = 0;
     if (!s->stop) create_pools_locked(s);
+    p->exited = true;
     s->cv.notify_all();
   }
 }
@@ -381,6 +412,7 @@ int claire_b200_server_submit(claire_b200_server* s, const claire_b200_opts* o, 
   r.t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return CB_ERR_STATE;
+  cb::srv::reap_locked(s);
   if (cb::Solver::estimate_bytes(*o, std::max(1, s->opts.slots_per_pool)) > s->budget) return CB_ERR_TOO_LARGE;
   r.id = s->next_id++;
   *id = r.id;
@@ -405,7 +437,8 @@ int claire_b200_server_wait(claire_b200_server* s, long long id, int timeout_ms,
   std::unique_lock<std::mutex> lk(s->mu);
   auto finished = [&] {
     auto it = s->reqs.find(id);
-    return it == s->reqs.end() || it->second.status == CB_REQ_DONE || it->second.status == CB_REQ_FAILED;
+    return it == s->reqs.end() || it->second.status == CB_REQ_DONE || it->second.status == CB_REQ_FAILED ||
+           it->second.status == CB_REQ_CANCELLED;
   };
   if (timeout_ms < 0) s->cv.wait(lk, finished);
   else s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished);
@@ -422,7 +455,7 @@ int claire_b200_server_result(claire_b200_server* s, long long id, float* v, cla
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return CB_ERR_ARG;
   cb::srv::Request& r = it->second;
-  if (r.status == CB_REQ_FAILED) {
+  if (r.status == CB_REQ_FAILED || r.status == CB_REQ_CANCELLED) {
     const int e = r.error ? r.error : CB_ERR_STATE;
     s->reqs.erase(it);
     return e;
@@ -438,12 +471,36 @@ int claire_b200_server_result(claire_b200_server* s, long long id, float* v, cla
 int claire_b200_server_info(claire_b200_server* s, int* pools, long long* bytes_used, int* queued) {
   if (!s) return CB_ERR_ARG;
   std::lock_guard<std::mutex> lk(s->mu);
+  cb::srv::reap_locked(s);
   int live = 0;
   for (auto& p : s->pools) live += p->dead ? 0 : 1;
   if (pools) *pools = live;
   if (bytes_used) *bytes_used = s->used;
   if (queued) *queued = (int)s->queue.size();
   return CB_OK;
+}
+
+int claire_b200_server_cancel(claire_b200_server* s, long long id) {
+  if (!s) return CB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  cb::srv::reap_locked(s);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return CB_ERR_ARG;
+  cb::srv::Request& r = it->second;
+  if (r.status == CB_REQ_QUEUED) {
+    auto q = std::find(s->queue.begin(), s->queue.end(), id);
+    if (q != s->queue.end()) s->queue.erase(q);
+    r.status = CB_REQ_CANCELLED;
+    r.error = CB_ERR_CANCELLED;
+    r.t_done = Clock::now();
+    s->cv.notify_all();
+    return CB_OK;
+  }
+  if (r.status == CB_REQ_RUNNING) {
+    r.cancel = true;  // its pool retires it at the next GN-iteration boundary
+    return CB_OK;
+  }
+  return CB_ERR_STATE;  // already done, failed or cancelled
 }
 
 int claire_b200_server_destroy(claire_b200_server* s) {

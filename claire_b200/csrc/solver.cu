@@ -235,6 +235,20 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   }
   ht = (float)(1.0 / nt);
   hd = (float)((kTwoPi / d.n1) * (kTwoPi / d.n2) * (kTwoPi / d.n3));
+  {
+    // refuse before allocating anything when the footprint cannot fit
+    size_t freeb = 0, total = 0;
+    if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+      err = "cudaMemGetInfo failed";
+      return CB_ERR_CUDA;
+    }
+    const long long need = estimate_bytes(o, B);
+    if (need > (long long)freeb) {
+      err = "footprint " + std::to_string(need) + " bytes exceeds the free device memory (" +
+            std::to_string((long long)freeb) + " bytes)";
+      return CB_ERR_TOO_LARGE;
+    }
+  }
   if (cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "stream creation failed";
     return CB_ERR_CUDA;
@@ -378,9 +392,9 @@ int Solver::upload_mask(const std::vector<int>& sel, int* dmask) {
 }
 
 int Solver::fetch_scalars() {
-  cudaMemcpyAsync(hsc, dsc, sizeof(double) * NSLOT * B, cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(hint, dint, sizeof(int) * NISLOT * B, cudaMemcpyDeviceToHost, stream);
-  cudaError_t e = cudaStreamSynchronize(stream);
+  cudaError_t e = cudaMemcpyAsync(hsc, dsc, sizeof(double) * NSLOT * B, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hint, dint, sizeof(int) * NISLOT * B, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) {
     err = std::string("device error: ") + cudaGetErrorString(e);
     return CB_ERR_CUDA;
@@ -1099,24 +1113,26 @@ int Solver::def_grad(int b, float* F9) {
   sel[b] = 1;
   CB_TRY(upload_mask(sel, dact));
   CB_TRY(characteristic(v, 1.f, dact));
+  // scratch for problem b alone: the scratch arrays take problem stride 0
+  // (only b is active in the mask)
   float* w = nullptr;
-  if (cudaMalloc(&w, sizeof(float) * 36 * n * B) != cudaSuccess) {
+  if (cudaMalloc(&w, sizeof(float) * 36 * n) != cudaSuccess) {
     cudaGetLastError();
     err = "deformation gradient: allocation failed";
     return CB_ERR_ALLOC;
   }
-  float *F = w, *FX = w + 9 * n * B, *gv = w + 18 * n * B, *gvx = w + 27 * n * B;
+  float *F = w, *FX = w + 9 * n, *gv = w + 18 * n, *gvx = w + 27 * n;
   const long long P9 = 9 * n;
-  int e = grad_fields(v, 3 * n, n, gv, P9, 3 * n, 3, dact);  // gv[3k + a] = d_a v_k
-  if (!e) e = launch_interp(gv, P9, n, disp_st, 3 * n, tab_st, TP, gvx, P9, n, 9, B, d, dact, stream);
+  int e = grad_fields(v, 3 * n, n, gv, 0, 3 * n, 3, dact);  // gv[3k + a] = d_a v_k
+  if (!e) e = launch_interp(gv, 0, n, disp_st, 3 * n, tab_st, TP, gvx, 0, n, 9, B, d, dact, stream);
   for (int c = 0; c < 9 && !e; ++c)
-    e = launch_fill(F + c * n, P9, (c % 4 == 0) ? 1.f : 0.f, n, B, dact, stream);
+    e = launch_fill(F + c * n, 0, (c % 4 == 0) ? 1.f : 0.f, n, B, dact, stream);
   for (int j = 0; j < nt && !e; ++j) {
-    e = launch_interp(F, P9, n, disp_st, 3 * n, tab_st, TP, FX, P9, n, 9, B, d, dact, stream);
-    if (!e) e = launch_defgrad_step(FX, gvx, gv, F, P9, ht, B, n, dact, stream);
+    e = launch_interp(F, 0, n, disp_st, 3 * n, tab_st, TP, FX, 0, n, 9, B, d, dact, stream);
+    if (!e) e = launch_defgrad_step(FX, gvx, gv, F, 0, ht, B, n, dact, stream);
   }
   note_launches(2 + 9 + 2 * nt);
-  if (!e && (cudaMemcpyAsync(F9, F + b * P9, sizeof(float) * P9, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+  if (!e && (cudaMemcpyAsync(F9, F, sizeof(float) * P9, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
              cudaStreamSynchronize(stream) != cudaSuccess))
     e = CB_ERR_CUDA;
   cudaFree(w);
@@ -1133,13 +1149,13 @@ int Solver::disp_grad(int b, float* G9) {
   sel[b] = 1;
   CB_TRY(displacement_field(sel));
   float* w = nullptr;
-  if (cudaMalloc(&w, sizeof(float) * 9 * n * B) != cudaSuccess) {
+  if (cudaMalloc(&w, sizeof(float) * 9 * n) != cudaSuccess) {  // problem b alone (stride 0)
     cudaGetLastError();
     err = "displacement gradient: allocation failed";
     return CB_ERR_ALLOC;
   }
-  int e = grad_fields(x, 3 * n, n, w, 9 * n, 3 * n, 3, dact);
-  if (!e && (cudaMemcpyAsync(G9, w + b * 9 * n, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, stream) !=
+  int e = grad_fields(x, 3 * n, n, w, 0, 3 * n, 3, dact);
+  if (!e && (cudaMemcpyAsync(G9, w, sizeof(float) * 9 * n, cudaMemcpyDeviceToHost, stream) !=
                  cudaSuccess ||
              cudaStreamSynchronize(stream) != cudaSuccess))
     e = CB_ERR_CUDA;
@@ -1381,8 +1397,8 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   constexpr int kItersPerCheck = 2;
   int launched = 0;
   while (true) {
-    cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream);
-    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+    if (cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
       err = "device error in PCG";
       return CB_ERR_CUDA;
     }
@@ -1565,8 +1581,8 @@ int Solver::pcg_twolevel(const std::vector<int>& sel, double maxit_d) {
   std::vector<int> hact(B, 0);
   bool any = false;
   auto read_active = [&]() -> int {
-    cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream);
-    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+    if (cudaMemcpyAsync(hact.data(), act, sizeof(int) * B, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
       err = "device error in PCG";
       return CB_ERR_CUDA;
     }
@@ -1648,13 +1664,13 @@ int Solver::line_search(std::vector<int>& sel) {
     // vtrial = v + alpha x  (alpha per problem through S_ALPHA)
     std::vector<double> al(B, 0.0);
     for (int b = 0; b < B; ++b) al[b] = alpha[b];
-    cudaMemcpyAsync(slot(S_ALPHA), al.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+    // pageable source: the copy is staged before the call returns
+    if (cudaMemcpyAsync(slot(S_ALPHA), al.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+      return CB_ERR_CUDA;
     CB_TRY(upload_mask(trial, dact + 6 * B));
     CB_TRY(launch_lincomb(vtrial, 3 * n, v, 3 * n, nullptr, 1.0, x, 3 * n, slot(S_ALPHA), 1.0, 3 * n, B,
                           dact + 6 * B, stream));
     note_launches(1);
-    const double* Jold = nullptr;
-    (void)Jold;
     std::vector<double> J0(B);
     for (int b = 0; b < B; ++b) J0[b] = ps[b].J;
     std::vector<double> D0(B), R0(B);
@@ -1789,7 +1805,8 @@ int Solver::step(std::vector<int>& finished, double gttol, int miniter) {
       rtol[b] = rt;
     }
   }
-  cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream);
+  if (cudaMemcpyAsync(slot(S_RTOL), rtol.data(), sizeof(double) * B, cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    return CB_ERR_CUDA;
   outer_rtol = rtol;
   CB_TRY(upload_mask(act, dact));
   CB_TRY(hessian_prep(dact));

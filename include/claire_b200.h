@@ -26,7 +26,9 @@ extern "C" {
 #define CB_ERR_NUMERIC (-4)   /* NaN / Inf in objective or gradient */
 #define CB_ERR_STATE (-5)     /* call out of order (e.g. run before images) */
 #define CB_ERR_UNSUPPORTED (-6) /* grid size without an FFT plan */
-#define CB_ERR_TOO_LARGE (-7)   /* grid exceeds a fixed-size workspace */
+#define CB_ERR_TOO_LARGE (-7)   /* grid exceeds a fixed-size workspace, or the footprint exceeds the
+                                   free device memory / the server's HBM budget */
+#define CB_ERR_CANCELLED (-8)   /* the registration request was cancelled (claire_b200_server_cancel) */
 
 /* Regularisation norms (-regnorm): l2 h1 h1s h2 h2s h3 h3s. */
 enum {
@@ -113,7 +115,9 @@ int claire_b200_parse_args(claire_b200_opts* opts, int argc, const char* const* 
 
 /* ---- registration context (reg::CLAIREInterface) -------------------------- */
 /* Create a context holding `nbatch` independent problems of one grid size;
- * allocates all device state up front (include/CLAIREInterface.hpp:42-90). */
+ * allocates all device state up front (include/CLAIREInterface.hpp:42-90).
+ * CB_ERR_TOO_LARGE, with nothing allocated, when claire_b200_estimate_bytes
+ * exceeds the device's free memory; CB_ERR_ALLOC when an allocation fails. */
 int claire_b200_create(const claire_b200_opts* opts, int nbatch, claire_b200_ctx** ctx);
 int claire_b200_destroy(claire_b200_ctx* ctx);
 const char* claire_b200_last_error(const claire_b200_ctx* ctx);
@@ -318,6 +322,7 @@ typedef struct claire_b200_server_opts {
 #define CB_REQ_RUNNING 1
 #define CB_REQ_DONE 2
 #define CB_REQ_FAILED 3
+#define CB_REQ_CANCELLED 4
 void claire_b200_server_default_opts(claire_b200_server_opts* o);
 int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_server** srv);
 /* Queue a registration of host images mR, mT (nx[0]*nx[1]*nx[2] floats each,
@@ -326,7 +331,15 @@ int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_serv
 int claire_b200_server_submit(claire_b200_server* srv, const claire_b200_opts* o, const float* mR, const float* mT,
                               long long* request_id);
 int claire_b200_server_poll(claire_b200_server* srv, long long request_id, int* status);
-/* Block until the request is done or failed (timeout_ms < 0: no limit). */
+/* Cancel a request.  A queued request is removed at once; a running one
+ * leaves its slot at its pool's next GN-iteration boundary (no kernel of it is
+ * interrupted), after which its status is CB_REQ_CANCELLED and
+ * claire_b200_server_result returns CB_ERR_CANCELLED.  CB_ERR_STATE when the
+ * request has already finished.  The reference has no serving layer and so no
+ * counterpart (a CLAIREInterface::Run call, src/CLAIREInterface.cpp:709-885,
+ * runs to its stopping test). */
+int claire_b200_server_cancel(claire_b200_server* srv, long long request_id);
+/* Block until the request is done, failed or cancelled (timeout_ms < 0: no limit). */
 int claire_b200_server_wait(claire_b200_server* srv, long long request_id, int timeout_ms, int* status);
 /* Velocity (host, 3n floats, may be NULL), statistics and submit-to-done
  * latency of a finished request; releases it.  A failed request returns its

@@ -13,7 +13,9 @@ import struct
 import numpy as np
 import pytest
 
-REF_DATA = "/root/reference/doc/data"
+# directory of the reference's example images (doc/data/brain0{1,2}.nii.gz);
+# the test that reads them is skipped when it is not set or not present
+REF_DATA = os.environ.get("CLAIRE_EXAMPLE_DATA", "")
 
 DTYPES = {2: np.uint8, 256: np.int8, 4: np.int16, 512: np.uint16, 8: np.int32, 768: np.uint32, 16: np.float32,
           64: np.float64}
@@ -108,7 +110,8 @@ def test_unsupported_and_missing(cb, tmp_path):
         cb.read_nifti(str(tmp_path / "missing.nii"))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="the reference's example images are not present")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA),
+                    reason="CLAIRE_EXAMPLE_DATA does not name the reference's example images")
 @pytest.mark.parametrize("name", ["brain01.nii.gz", "brain02.nii.gz"])
 def test_reference_example_brains(cb, name):
     path = os.path.join(REF_DATA, name)
