@@ -61,6 +61,10 @@ def parse():
                     help="mixed batch instead: 12 x 64^3 + 12 x 96^3 + 8 x 128^3 (H1 beta=1e-2, nt=4) served "
                          "together against plain one-at-a-time runs")
     ap.add_argument("--mixed-slots", type=int, default=12, help="--mixed: slots per pool")
+    ap.add_argument("--conv-norm", default="h1s", help="norm of the converging leg (its Newton system carries hd)")
+    ap.add_argument("--conv-beta", type=float, default=1e-4, help="beta of the converging leg")
+    ap.add_argument("--conv-maxit", type=int, default=50, help="GN iteration cap of the converging leg")
+    ap.add_argument("--no-converge", action="store_true", help="skip the converging leg")
     ap.add_argument("--precision", action="store_true",
                     help="bf16-image study instead: 256^3 H2 beta=1e-4 nt=8 with bf16 and FP32 image storage")
     return ap.parse_args()
@@ -299,8 +303,49 @@ def run_ours(a, rank, world, local):
     roof = roofline(cb, a, ci, load_device, B) if rank == 0 else None
     ci.close()
     fixed = fixed_work(cb, a, probs, stream, zero_v) if rank == 0 else None
+    conv = converging_leg(cb, a, probs, stream, zero_v) if (rank == 0 and not a.no_converge) else None
     return dict(total_ms=total_ms, lat=lat_all, lat_srv=lat_srv, stats=stats, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
-                launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned, fixed=fixed)
+                launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned, fixed=fixed,
+                conv=conv)
+
+
+def converging_leg(cb, a, probs, stream, zero_v):
+    """The same 128^3 recipe problems registered with a norm whose Newton
+    system carries hd (the headline's H2 gradient lacks it, so those solves
+    never reach the metric's 1e-2 mismatch): one batch solved to the
+    gradient tolerance 1e-2, timed with CUDA events; the line states whether
+    every problem reached relative mismatch <= 1e-2 and |g| <= 1e-2 |g0|."""
+    import torch
+    B = len(probs)
+    opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", a.conv_norm, "-beta", repr(a.conv_beta),
+                     "-maxit", str(a.conv_maxit), "-opttol", "1e-2"])
+    ci = cb.CLAIREInterface(opt, nbatch=B)
+    ci.set_stream(stream)
+    out = None
+    for rep in range(2):  # warm-up, then timed
+        for b, (mR, mT, _) in enumerate(probs):
+            ci.set_images(mR, mT, b)
+            ci.SetInitialGuess(zero_v, b)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ci.Run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = [ci.stats(b) for b in range(B)]
+        out = {"workload": f"{B} registrations {a.n}^3 {a.conv_norm} beta={a.conv_beta} nt={a.nt} "
+                           f"maxit={a.conv_maxit} opttol=0.01, same recipe problems",
+               "value": B / (ms / 1e3), "unit": "registrations/s", "ms": ms,
+               "rel_mismatch": [s["rel_mismatch"] for s in st],
+               "grad_reduction": [s["gnorm"] / s["gnorm0"] for s in st],
+               "gn_iterations": [s["gn_iterations"] for s in st],
+               "pcg_iterations": [s["pcg_iterations"] for s in st]}
+    out["reaches_target"] = bool(all(m <= 1e-2 for m in out["rel_mismatch"]) and
+                                 all(g <= 1e-2 for g in out["grad_reduction"]))
+    ci.close()
+    return out
 
 
 def fixed_work(cb, a, probs, stream, zero_v, matvecs=10):
@@ -894,7 +939,8 @@ def main():
                    "hess_matvecs_per_s": float(sum(s["hess_matvecs"] for s in r["stats"]) * world * a.steps
                                                / (r["total_ms"] / 1e3)),
                    "fft_variants": r["tuned"] or "defaults (--no-autotune)",
-                   "fixed_work": r["fixed"]},
+                   "fixed_work": r["fixed"],
+                   "converging": r["conv"]},
         "e2e": {"value": regs / (r["e2e_ms"] / 1e3), "unit": "registrations/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "path": "claire_b200_server_submit / _wait / _result (host buffers)"},

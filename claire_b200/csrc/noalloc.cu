@@ -18,11 +18,15 @@
 // * every call shares the arrays: calls that may overlap on the GPU (different
 //   streams, other host threads) race and must be serialised by the caller.
 //   The spectrum is fully rewritten by each call, so nothing has to start at
-//   zero; the parameter block is rewritten by each call.
+//   zero; the parameter block is rewritten by each call (a one-thread kernel
+//   stores the block it receives as a launch argument, in stream order).
+// * v and out must be 16-byte aligned (CB_ERR_ARG otherwise, before anything
+//   is launched).
 // * the first call on a device sets that device up (looks up the arrays'
 //   device addresses with that device current and uploads the twiddle
 //   tables); make that first call before any stream capture.
 #include <cmath>
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/claire_b200.h"
@@ -43,6 +47,10 @@ constexpr int kTwOffset16 = 0, kTwOffset32 = 16, kTwOffset48 = 48, kTwOffset64 =
 static __device__ __align__(256) float2 g_spec[kSpecEntries];
 static __device__ __align__(256) cb::SpecParams g_params;
 static __device__ __align__(256) float2 g_twiddles[kTwEntries];
+
+// Writes the call's parameter block: the block travels as a kernel argument,
+// so no host buffer has to outlive the call.
+__global__ void k_set_params(cb::SpecParams p) { g_params = p; }
 
 struct DeviceArrays {
   bool ready = false;
@@ -97,6 +105,8 @@ extern "C" int claire_b200_reg_apply_noalloc(const float* v, float* out, const i
       kind < CB_REG_GRADIENT || kind > CB_REG_SQRTINVERSE)
     return CB_ERR_ARG;
   if (nx[0] <= 0 || nx[1] <= 0 || nx[2] <= 0) return CB_ERR_ARG;
+  // the transform kernels read and write 16-byte vectors
+  if ((reinterpret_cast<uintptr_t>(v) & 15) || (reinterpret_cast<uintptr_t>(out) & 15)) return CB_ERR_ARG;
   if (!(nx[0] == nx[1] && nx[1] == nx[2])) return CB_ERR_UNSUPPORTED;
   if (nx[0] > kMaxN) return CB_ERR_TOO_LARGE;
   const int toff = twiddle_offset(nx[0]);
@@ -126,11 +136,11 @@ extern "C" int claire_b200_reg_apply_noalloc(const float* v, float* out, const i
   p.beta2 = 0.f;
   p.hd = (float)((cb::kTwoPi / d.n1) * (cb::kTwoPi / d.n2) * (cb::kTwoPi / d.n3));
   p.sigma[0] = p.sigma[1] = p.sigma[2] = 1.f;
-  // pageable source: the copy is staged before cudaMemcpyAsync returns
-  if (cudaMemcpyAsync(a.params, &p, sizeof(p), cudaMemcpyHostToDevice, st) != cudaSuccess) return CB_ERR_CUDA;
+  k_set_params<<<1, 1, 0, st>>>(p);
+  if (cudaGetLastError() != cudaSuccess) return CB_ERR_CUDA;
   const int op = kind == CB_REG_GRADIENT ? cb::OP_REG_GRAD
                                          : (kind == CB_REG_INVERSE ? cb::OP_REG_INV : cb::OP_REG_SQRTINV);
-  cb::note_launches(5);
+  cb::note_launches(6);
   e = cb::launch_spectral3_explicit(v, out, a.spec, a.params, d, op, a.tw + toff, st);
   return e ? CB_ERR_CUDA : CB_OK;
 }

@@ -896,6 +896,11 @@ class Problem {
     finish();
   }
 
+  void last_adjoint(double* lam0, double* bf) const {
+    for (long long i = 0; i < nl; ++i) lam0[i] = (double)lam[i];
+    for (long long i = 0; i < 3 * nl; ++i) bf[i] = hd * (double)bfield[i];
+  }
+
   double seconds = 0;
   std::vector<R> m, mR, mT;
   std::vector<R> Xs, Xa;  // ghost coordinates of the state / adjoint foot points
@@ -1245,6 +1250,15 @@ int cref_stats(void* h, double* out) {
                           (double)P.cnt.hessmatvec, (double)P.cnt.pcmatvec, (double)P.cnt.pdesolve,
                           (double)P.cnt.gathers, (double)P.cnt.ffts, P.krylov_g0};
     std::memcpy(out, s, sizeof(s));
+    return 0;
+  });
+}
+
+// lambda at t = 0 and the body force hd b of the last gradient or Hessian
+// matvec (the incremental adjoint and body force after a matvec)
+int cref_last_adjoint(void* h, double* lam0, double* body_force) {
+  return dispatch(h, [&](auto& P) {
+    P.last_adjoint(lam0, body_force);
     return 0;
   });
 }

@@ -79,6 +79,7 @@ def lib():
             "cref_get_final_state": (I, [P, DP]),
             "cref_stats": (I, [P, DP]),
             "cref_reset_counters": (I, [P]),
+            "cref_last_adjoint": (I, [P, DP, DP]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -205,6 +206,13 @@ class CpuRef:
             d[k] = int(d[k])
         d["reason_name"] = REASONS.get(d["reason"], "?")
         return d
+
+    def last_adjoint(self):
+        """(lambda at t = 0, body force hd b) of the last gradient or Hessian matvec."""
+        lam = np.zeros(self.shape)
+        bf = np.zeros((3,) + self.shape)
+        self._chk(self.L.cref_last_adjoint(self.h, _ptr(lam), _ptr(bf)), "last_adjoint")
+        return lam, bf
 
     def reset_counters(self):
         self._chk(self.L.cref_reset_counters(self.h), "reset_counters")

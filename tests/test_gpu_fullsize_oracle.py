@@ -5,9 +5,18 @@ The NumPy oracle is too slow at 128^3 and 256^3; the C++/OpenMP restatement
 runs there in seconds.  On the recipe problems of the 128^3 configuration
 (H2, beta 1e-3, nt 8) and of the 256^3 one (H2, beta 1e-4, nt 8), at half the
 recipe velocity (displacements of ~1.3 cells per time step at 128^3, so the
-gathers see the recipe's box sizes), the device's transported image,
-objective, gradient, GN Hessian matvec and preconditioner agree with the FP64
-oracle on the same FP32 inputs within 1e-5 relative (L2 for fields).
+gathers see the recipe's box sizes), on the same FP32 inputs:
+
+* transported image, distance, regularisation functional, objective,
+  adjoint at t = 0 and body force (of the gradient and of the Hessian
+  matvec), preconditioner: within 1e-5 relative (L2 for fields);
+* gradient and GN Hessian matvec: within 1e-5, or within 1.5 times the error
+  of the reference's own single-precision arithmetic (the C++ restatement in
+  FP32) when that is larger.  For H2 it is: the operator's symbol
+  beta0 (kappa^2 + beta1) carries no hd and reaches 1.5e8 beta0 at 128^3, and
+  an FP32 field's roundoff at high wavenumbers, multiplied by it, is ~1% of
+  the result (the reference's FP32 build included); both outputs are
+  dominated by that term.
 """
 import numpy as np
 import pytest
@@ -22,6 +31,20 @@ def rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def cpu_side(n, nt, norm, beta, mR, mT, v, vt, fp64):
+    ref = CpuRef((n,) * 3, nt, norm, beta, fp64=fp64)
+    ref.set_images(mR, mT)
+    out = {"m1": ref.forward(v, mT)}
+    out["J"], out["D"], out["R"] = ref.objective(v)
+    out["g"] = ref.gradient(v)
+    out["lam"], out["bf"] = ref.last_adjoint()
+    out["H"] = ref.hessian_matvec(v, vt)
+    out["lamt"], out["bft"] = ref.last_adjoint()
+    out["P"] = ref.precond(vt)
+    ref.close()
+    return out
 
 
 @pytest.mark.parametrize("n,norm,beta,config", [(128, "h2", 1e-3, 1), (256, "h2", 1e-4, 3)])
@@ -43,30 +66,52 @@ def test_operators_at_full_size(cuda, n, norm, beta, config):
     rng = np.random.Generator(np.random.PCG64(7))
     vt = R.velocity_random((n, n, n), rng).astype(np.float32)
 
-    ref = CpuRef((n,) * 3, nt, norm, beta, fp64=True)
-    ref.set_images(mR, mT)
-    m1_ref = ref.forward(v, mT)
-    J_ref, D_ref, R_ref = ref.objective(v)
-    g_ref = ref.gradient(v)
-    H_ref = ref.hessian_matvec(v, vt)
-    P_ref = ref.precond(vt)
-    ref.close()
-
     opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", norm, "-beta", repr(beta)])
+    dev = {}
     with cb.CLAIREInterface(opt) as ci:
         ci.set_images(mR, mT)
         ci.SetInitialGuess(v)
-        m1 = ci.SolveForwardProblem(mT)
-        J, D, Rv = ci.EvaluateObjective(v)
-        g = ci.EvaluateGradient(v)
-        H = ci.HessianMatVec(v, vt)
-        P = ci.ApplyInvRegularizationOperator(vt)
+        dev["m1"] = ci.SolveForwardProblem(mT)
+        dev["J"], dev["D"], dev["R"] = ci.EvaluateObjective(v)
+        dev["g"] = ci.EvaluateGradient(v)
+        dev["lam"], dev["bf"] = ci.GetAdjoint()
+        dev["H"] = ci.HessianMatVec(v, vt)
+        dev["lamt"], dev["bft"] = ci.GetAdjoint()
+        dev["P"] = ci.ApplyInvRegularizationOperator(vt)
     torch.cuda.empty_cache()
 
-    assert rel(m1, m1_ref) < 1e-5
-    assert abs(D - D_ref) <= 1e-5 * abs(D_ref)
-    assert abs(Rv - R_ref) <= 1e-5 * abs(R_ref)
-    assert abs(J - J_ref) <= 1e-5 * abs(J_ref)
-    assert rel(g, g_ref) < 1e-5
-    assert rel(H, H_ref) < 1e-5
-    assert rel(P, P_ref) < 1e-5
+    ref = cpu_side(n, nt, norm, beta, mR, mT, v, vt, fp64=True)
+    for k in ("m1", "lam", "bf", "lamt", "bft", "P"):
+        assert rel(dev[k], ref[k]) < 1e-5, k
+    for k in ("D", "R", "J"):
+        assert abs(dev[k] - ref[k]) <= 1e-5 * abs(ref[k]), k
+    single = cpu_side(n, nt, norm, beta, mR, mT, v, vt, fp64=False)
+    for k in ("g", "H"):
+        tol = max(1e-5, 1.5 * rel(single[k], ref[k]))
+        assert rel(dev[k], ref[k]) < tol, (k, rel(dev[k], ref[k]), rel(single[k], ref[k]))
+
+
+def test_gathers_against_the_reference_kernel(cuda):
+    """The device's tricubic gather at the 128^3 recipe's state and adjoint
+    characteristics against the reference's own optimized_interp3_ghost_xyz_p
+    (oracle/_ref, its double and single builds) on the same FP32 inputs."""
+    from oracle import ref_interp3
+    if not (ref_interp3.available("f64") and ref_interp3.available("f32")):
+        pytest.skip("oracle/_ref not built (needs the reference tree at build time)")
+    import torch
+
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+
+    n, nt = 128, 8
+    mR, mT, v = synthetic.ellipsoid_problem(n, nt, 1, 0, cuda)
+    sl = cb.SemiLagrangian(nt)
+    for flag in ("state", "adjoint"):
+        disp = sl.ComputeTrajectory(v, flag)
+        got = sl.Interpolate(mR, disp)
+        torch.cuda.synchronize()
+        f = mR.cpu().numpy()
+        dh = disp.cpu().numpy().astype(np.float64)
+        g = got.cpu().numpy()
+        assert rel(g, ref_interp3.interp3(f, dh, "f64")) < 1e-6
+        assert rel(g, ref_interp3.interp3(f, dh, "f32")) < 2e-6

@@ -19,8 +19,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-5
-NORMS = {"h1s": 2, "h1": 1, "h2": 3, "l2": 0}
-KINDS = {"gradient": 0, "inverse": 1}
+NORMS = {"l2": 0, "h1": 1, "h1s": 2, "h2": 3, "h2s": 4, "h3": 5, "h3s": 6}
+KINDS = {"gradient": 0, "inverse": 1, "sqrtinverse": 2}
 
 
 def _call(lib, fn, v, out, n, norm, kind, beta, stream):
@@ -36,8 +36,10 @@ def _rel(a, b):
     return float((a - b).norm() / b.norm())
 
 
-@pytest.mark.parametrize("n", [32, 64])
-@pytest.mark.parametrize("norm,kind", [("h1s", "inverse"), ("h2", "gradient"), ("h1", "inverse"), ("l2", "gradient")])
+@pytest.mark.parametrize("n", [16, 32, 48, 64])
+@pytest.mark.parametrize("norm,kind", [("h1s", "inverse"), ("h2", "gradient"), ("h1", "inverse"), ("l2", "gradient"),
+                                       ("h2s", "sqrtinverse"), ("h3", "inverse"), ("h3s", "gradient"),
+                                       ("h2", "sqrtinverse")])
 def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(cuda, n, norm, kind):
     import torch
     import claire_b200 as cb
@@ -54,6 +56,44 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(cuda, n, no
         torch.cuda.synchronize()
         assert torch.isfinite(got).all(), f"call {call}: output not fully written"
         assert _rel(got, ref) <= TOL, f"call {call}"
+
+
+def test_noalloc_allocates_nothing(cuda):
+    """After the first call on the device (its set-up, and the lazy loading of
+    its kernels), further calls leave the device's free memory and the torch
+    allocator's counters unchanged."""
+    import torch
+    import claire_b200 as cb
+    n = 64
+    stream = torch.cuda.current_stream().cuda_stream
+    v = torch.randn((3, n, n, n), device=cuda)
+    out = torch.empty_like(v)
+    for kind in ("inverse", "gradient", "sqrtinverse"):
+        assert _call(cb.lib, "claire_b200_reg_apply_noalloc", v, out, n, "h2", kind, (1e-3, 1e-4), stream) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0, reserved0 = torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
+    for _ in range(3):
+        for kind in ("inverse", "gradient", "sqrtinverse"):
+            assert _call(cb.lib, "claire_b200_reg_apply_noalloc", v, out, n, "h2", kind, (1e-3, 1e-4), stream) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0 and torch.cuda.memory_reserved() == reserved0
+
+
+def test_noalloc_rejects_misaligned_buffers(cuda):
+    import torch
+    import claire_b200 as cb
+    n = 32
+    buf = torch.zeros(3 * n ** 3 + 4, device=cuda)
+    v = buf[1:1 + 3 * n ** 3]            # 4-byte offset: not 16-byte aligned
+    out = torch.zeros(3 * n ** 3, device=cuda)
+    rc = _call(cb.lib, "claire_b200_reg_apply_noalloc", v, out, n, "h1s", "inverse", (1e-2, 1e-4),
+               torch.cuda.current_stream().cuda_stream)
+    assert rc == -1   # CB_ERR_ARG, before anything is launched
+    torch.cuda.synchronize()
+    assert float(out.abs().max()) == 0.0
 
 
 def test_noalloc_rejects_grids_above_its_workspace(cuda):
