@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--conv-beta", type=float, default=1e-4, help="beta of the converging leg")
     ap.add_argument("--conv-maxit", type=int, default=50, help="GN iteration cap of the converging leg")
     ap.add_argument("--no-converge", action="store_true", help="skip the converging leg")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small fixed workload for ncu captures: one 128^3 recipe problem, objective, gradient, "
+                         "Hessian matvec and preconditioner with FP32 and bf16 images, and a Stokes-model gradient")
     ap.add_argument("--precision", action="store_true",
                     help="bf16-image study instead: 256^3 H2 beta=1e-4 nt=8 with bf16 and FP32 image storage")
     return ap.parse_args()
@@ -886,6 +889,37 @@ def run_precision(a, rank, world, local):
 
 
 # ---------------------------------------------------------------------------
+def run_profile_case(a, local):
+    """Every kernel of the path once or twice on one 128^3 problem (a few GB on
+    the device): the workload the committed ncu summaries capture."""
+    import torch
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if a.fft_variant >= 0:
+        cb.set_fft_variant(a.n, a.fft_variant)
+    mR, mT, v = synthetic.ellipsoid_problem(a.n, a.nt, 1, 0, dev)
+    vh = (0.5 * v).cpu().numpy()
+    vt = (0.1 * v).cpu().numpy()
+    for extra in ([], ["-bf16images"]):
+        opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", a.norm, "-beta", repr(a.beta)] + extra)
+        with cb.CLAIREInterface(opt) as ci:
+            ci.set_images(mR, mT)
+            for _ in range(2):
+                ci.EvaluateObjective(vh)
+                ci.EvaluateGradient(vh)
+                ci.HessianMatVec(vh, vt)
+                ci.ApplyInvRegularizationOperator(vt)
+    opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", "h1s", "-beta", "1e-2"]).set("model", "stokes")
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        ci.EvaluateObjective(vh)
+        ci.EvaluateGradient(vh)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": "done", "n": a.n, "nt": a.nt}), flush=True)
+
+
 def main():
     a = parse()
     rank, world, local = dist_init(a)
@@ -900,6 +934,9 @@ def main():
         return
     if a.precision:
         run_precision(a, rank, world, local)
+        return
+    if a.profile_case:
+        run_profile_case(a, local)
         return
     r = run_ours(a, rank, world, local)
     if rank != 0:

@@ -133,3 +133,27 @@ def test_unsupported_grid_fails_cleanly(cb):
         assert srv.wait(rid, 60000) == cb.REQ_FAILED
         with pytest.raises(cb.ClaireError):
             srv.result(rid, (40, 40, 40))
+
+
+def test_scheduler_places_whole_requests(cb):
+    """The multi-GPU scheduler over the devices this run has (one here): a
+    request placed by it computes what the device's own server computes."""
+    import torch
+    from claire_b200.scheduler import Scheduler
+    n, nt = 32, 4
+    mR, mT = sin2(n, nt)
+    o = opt_for(cb, n, nt, "h1s", 1e-2)
+    with cb.Server(slots_per_pool=2) as srv:
+        rid = srv.submit(o, mR, mT)
+        assert srv.wait(rid, 120000) == cb.REQ_DONE
+        v_ref, st_ref, _ = srv.result(rid, (n, n, n))
+    devices = list(range(torch.cuda.device_count()))
+    with Scheduler(devices, slots_per_pool=2) as sch:
+        gids = [sch.submit(o, mR, mT) for _ in range(2 * len(devices))]
+        assert sorted(sch.device_of(g) for g in gids) == sorted(devices * 2)
+        for g in gids:
+            assert sch.wait(g, 120000) == cb.REQ_DONE
+            v, st, _ = sch.result(g, (n, n, n))
+            assert st["gn_iterations"] == st_ref["gn_iterations"]
+            assert np.array_equal(v, v_ref)
+        assert all(x == 0 for x in sch.outstanding.values())
