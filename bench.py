@@ -401,6 +401,10 @@ def tune(cb, sizes, nbatch):
 # one 128^3 problem of the workload (42,410,240 bytes; ncu --set full, the
 # command in profiles/k_gather_scale_128.md), per point
 GATHER_SCALE_DRAM_BYTES_PER_POINT = 42410240 / 128 ** 3
+# l1tex__data_pipe_lsu_wavefronts_mem_shared.sum of the same capture (4.44 M
+# shared-memory wavefronts for 128^3 points: the 64 taps per point plus the box
+# copies), per point; a B200 SM serves one 128-byte wavefront per clock
+GATHER_SCALE_SMEM_WAVEFRONTS_PER_POINT = 4.44e6 / 128 ** 3
 
 
 def roofline(cb, a, ci, load_device, B):
@@ -434,10 +438,19 @@ def roofline(cb, a, ci, load_device, B):
     bytes_ = 24 * n * B
     achieved = bytes_ / (avg_ms / 1e3) / 1e9
     traffic = GATHER_SCALE_DRAM_BYTES_PER_POINT * n * B
+    # the bound that binds: shared-memory wavefronts against one per SM per clock
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    wf = GATHER_SCALE_SMEM_WAVEFRONTS_PER_POINT * n * B
+    wf_peak = 148 * sm_mhz * 1e6
+    smem = {"what": "shared-memory wavefronts per second against one 128-byte wavefront per SM per clock "
+                    f"(148 SMs at {sm_mhz:.0f} MHz)", "wavefronts_per_launch": wf,
+            "achieved_per_s": wf / (avg_ms / 1e3), "peak_per_s": wf_peak,
+            "frac": round(wf / (avg_ms / 1e3) / wf_peak, 4)}
     return {"kernel": "k_gather_scale (adjoint time step: tricubic tile gather x per-point factor)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "algorithmic_bytes": bytes_,
-            "avg_launch_us": round(avg_ms * 1e3, 2), "launches_timed": cnt, "peak_source": peak_src}
+            "avg_launch_us": round(avg_ms * 1e3, 2), "launches_timed": cnt, "peak_source": peak_src,
+            "shared_memory_roofline": smem}
 
 
 # ---------------------------------------------------------------------------

@@ -352,21 +352,22 @@ __global__ void __launch_bounds__(kThreads) k_cols(float2* __restrict__ data, lo
                                                     long long es, const float2* __restrict__ twg,
                                                     const int* __restrict__ active) {
   constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
+  using PL = Plan<N, V>;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
-  float* re = smem + 2 * N;
-  float* im = re + N * PITCH;
-  float* sre = im + N * PITCH;
+  float* sre = smem + 2 * N;
   float* sim = sre + N * PITCH;
   float2* base = data + blockIdx.z * pstr + blockIdx.y * fstr;
   const int g = blockIdx.x * C + threadIdx.x % C;
   float2* colp = (g < ncols) ? base + (long long)(g / cpg) * gs + (g % cpg) : nullptr;
   load_twiddles<N>(tw, twg);
-  load_col_tile<N, C, PITCH>(re, im, colp, es);
+  // first stage straight from the columns, last stage straight back: every
+  // column element passes through shared memory once (in place: all reads of
+  // the CTA's columns finish before the barrier, all writes follow it)
+  fft_stage_load<N, PL::R0, INV, C, PITCH>(colp, es, sre, sim);
   __syncthreads();
-  fft_lines<N, INV, C, PITCH, V>(re, im, sre, sim, tw);
-  store_col_tile<N, C, PITCH>(re, im, colp, es);
+  fft_stage_store<N, PL::R1, PL::R0, INV, C, PITCH>(sre, sim, tw, colp, es);
 }
 
 // ---------------------------------------------------------------------------
@@ -504,6 +505,7 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
                                                        const int* __restrict__ active) {
   constexpr int C = ColCfg<N, V>::C, PITCH = ColCfg<N, V>::PITCH;
   constexpr int RSTEP = kThreads / C, K = (N + RSTEP - 1) / RSTEP;
+  using PL = Plan<N, V>;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -520,9 +522,11 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
   const ColumnK ck = column_k(g / n3h, g % n3h, d);
   const float s = 1.f / (float)((double)d.n1 * d.n2 * d.n3);
   load_twiddles<N>(tw, twg);
-  load_col_tile<N, C, PITCH>(re, im, colp, ncols);
+  // forward transform: first stage straight from the column, second into (re, im)
+  fft_stage_load<N, PL::R0, false, C, PITCH>(colp, ncols, sre, sim);
   __syncthreads();
-  fft_lines<N, false, C, PITCH, V>(re, im, sre, sim, tw);
+  fft_stage<N, PL::R1, PL::R0, false, C, PITCH>(sre, sim, re, im, tw);
+  __syncthreads();
   // one copy of the symbol code (a rolled loop keeps the kernel small enough
   // for the instruction cache)
 #pragma unroll 1
@@ -535,8 +539,10 @@ __global__ void __launch_bounds__(kThreads) k_pencil1(float2* __restrict__ spec,
     im[a] = y.y;
   }
   __syncthreads();
-  fft_lines<N, true, C, PITCH, V>(re, im, sre, sim, tw);
-  store_col_tile<N, C, PITCH>(re, im, colp, ncols);
+  // inverse transform: first stage in shared memory, last straight to the column
+  fft_stage<N, PL::R0, 1, true, C, PITCH>(re, im, sre, sim, tw);
+  __syncthreads();
+  fft_stage_store<N, PL::R1, PL::R0, true, C, PITCH>(sre, sim, tw, colp, ncols);
 }
 
 // x1 pencil with the three fields in one CTA (coupled projections).
@@ -567,12 +573,17 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
   const SpecParams q = params[blockIdx.z];
   const ColumnK ck = column_k(g / n3h, g % n3h, d);
   const float s = 1.f / (float)((double)d.n1 * d.n2 * d.n3);
+  using PL = Plan<N, V>;
   load_twiddles<N>(tw, twg);
-#pragma unroll
-  for (int f = 0; f < 3; ++f) load_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
-  __syncthreads();
+  // forward transforms: first stage straight from each field's column into
+  // the scratch, second stage into the field's lines
 #pragma unroll 1
-  for (int f = 0; f < 3; ++f) fft_lines<N, false, C, PITCH, V>(fre[f], fim[f], sre, sim, tw);
+  for (int f = 0; f < 3; ++f) {
+    fft_stage_load<N, PL::R0, false, C, PITCH>(colp ? colp + f * fstr : nullptr, ncols, sre, sim);
+    __syncthreads();
+    fft_stage<N, PL::R1, PL::R0, false, C, PITCH>(sre, sim, fre[f], fim[f], tw);
+    __syncthreads();
+  }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int e = e0 + k * RSTEP;
@@ -589,10 +600,14 @@ __global__ void __launch_bounds__(kThreads) k_pencil3(float2* __restrict__ spec,
     }
   }
   __syncthreads();
+  // inverse transforms: first stage into the scratch, last straight to the column
 #pragma unroll 1
-  for (int f = 0; f < 3; ++f) fft_lines<N, true, C, PITCH, V>(fre[f], fim[f], sre, sim, tw);
-#pragma unroll
-  for (int f = 0; f < 3; ++f) store_col_tile<N, C, PITCH>(fre[f], fim[f], colp ? colp + f * fstr : nullptr, ncols);
+  for (int f = 0; f < 3; ++f) {
+    fft_stage<N, PL::R0, 1, true, C, PITCH>(fre[f], fim[f], sre, sim, tw);
+    __syncthreads();
+    fft_stage_store<N, PL::R1, PL::R0, true, C, PITCH>(sre, sim, tw, colp ? colp + f * fstr : nullptr, ncols);
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -644,6 +659,50 @@ __global__ void __launch_bounds__(kThreads) k_deriv_rows(const float* __restrict
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
 }
 
+// Column derivative: the thread's packed line p holds real columns 2p (real
+// part) and 2p + 1 (imaginary part); the forward transform's first stage reads
+// them from global memory, its last stage multiplies by i k / N on the way to
+// shared memory, and the inverse transform's last stage hands both columns to
+// the epilogue (store, add, or sum of squares) straight from registers.
+template <int N>
+struct DerivColLoad {
+  const float* src;
+  long long ca, cb, es;
+  bool oka, okb;
+  CB_DEVICE float2 operator()(int, int e) const {
+    return make_float2(oka ? __ldg(src + ca + (long long)e * es) : 0.f, okb ? __ldg(src + cb + (long long)e * es) : 0.f);
+  }
+};
+
+template <int N, int PITCH>
+struct MulIkStore {
+  float* re;
+  float* im;
+  CB_DEVICE void operator()(int p, int e, float2 v) const {
+    const float k = (float)wavenumber(e, N) * (1.f / (float)N);
+    re[e * PITCH + p] = -k * v.y;
+    im[e * PITCH + p] = k * v.x;
+  }
+};
+
+struct DerivColEpi {
+  float* dst;
+  long long ca, cb, es;
+  bool oka, okb;
+  int epi;
+  double* acc;
+  CB_DEVICE void put(long long c, float val) const {
+    if (epi == EPI_SUMSQ) *acc += (double)val * (double)val;  // no output array needed
+    else if (!dst) return;
+    else if (epi == EPI_STORE) dst[c] = val;
+    else if (epi == EPI_ADD) dst[c] = dst[c] + val;
+  }
+  CB_DEVICE void operator()(int, int e, float2 v) const {
+    if (oka) put(ca + (long long)e * es, v.x);
+    if (okb) put(cb + (long long)e * es, v.y);
+  }
+};
+
 template <int N, int V>
 __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict__ in, long long ip,
                                                           long long ifs, float* __restrict__ out,
@@ -653,9 +712,8 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
                                                           double* __restrict__ partials, int nparts,
                                                           const int* __restrict__ active) {
   constexpr int L = ColCfg<N, V>::C;       // packed complex lines per CTA
-  constexpr int C = 2 * L;              // real columns per CTA
   constexpr int PITCH = ColCfg<N, V>::PITCH;
-  constexpr int RSTEP = kThreads / C, K = (N + RSTEP - 1) / RSTEP;
+  using PL = Plan<N, V>;
   if (active && !active[blockIdx.z]) return;
   extern __shared__ float smem[];
   float2* tw = reinterpret_cast<float2*>(smem);
@@ -665,49 +723,21 @@ __global__ void __launch_bounds__(kThreads) k_deriv_cols(const float* __restrict
   float* sim = sre + N * PITCH;
   const float* src = in + blockIdx.z * ip + blockIdx.y * ifs;
   float* dst = out ? out + blockIdx.z * op + blockIdx.y * ofs : nullptr;
-  const int c = threadIdx.x % C, e0 = threadIdx.x / C;
-  const int g = blockIdx.x * C + c;
-  const bool ok = g < ncols;
-  const long long cbase = ok ? (long long)(g / cpg) * gs + (g % cpg) : 0;
-  float* lane = ((c & 1) ? im : re) + (c >> 1);
+  const int p = threadIdx.x % L;
+  const int ga = blockIdx.x * 2 * L + 2 * p, gb = ga + 1;
+  const bool oka = ga < ncols, okb = gb < ncols;
+  const long long ca = oka ? (long long)(ga / cpg) * gs + (ga % cpg) : 0;
+  const long long cb = okb ? (long long)(gb / cpg) * gs + (gb % cpg) : 0;
   load_twiddles<N>(tw, twg);
-  {
-    float v[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = e0 + k * RSTEP;
-      v[k] = (ok && in_line<N, RSTEP>(e)) ? __ldg(src + cbase + (long long)e * es) : 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = e0 + k * RSTEP;
-      if (in_line<N, RSTEP>(e)) lane[e * PITCH] = v[k];
-    }
-  }
+  fft_stage_in<N, PL::R0, false, L, PITCH>(DerivColLoad<N>{src, ca, cb, es, oka, okb}, sre, sim);
   __syncthreads();
-  fft_lines<N, false, L, PITCH, V>(re, im, sre, sim, tw);
-  mul_ik<N, L, PITCH>(re, im, 1.f / (float)N);
+  fft_stage_out<N, PL::R1, PL::R0, false, L, PITCH>(sre, sim, tw, MulIkStore<N, PITCH>{re, im});
   __syncthreads();
-  fft_lines<N, true, L, PITCH, V>(re, im, sre, sim, tw);
+  fft_stage<N, PL::R0, 1, true, L, PITCH>(re, im, sre, sim, tw);
+  __syncthreads();
   double acc = 0.0;
-  if (ok) {
-    float old[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = e0 + k * RSTEP;
-      old[k] = (epi == EPI_ADD && in_line<N, RSTEP>(e)) ? dst[cbase + (long long)e * es] : 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const int e = e0 + k * RSTEP;
-      if (!in_line<N, RSTEP>(e)) continue;
-      const float val = lane[e * PITCH];
-      const long long gi = cbase + (long long)e * es;
-      if (epi == EPI_STORE) dst[gi] = val;
-      else if (epi == EPI_ADD) dst[gi] = old[k] + val;
-      else acc += (double)val * (double)val;
-    }
-  }
+  fft_stage_out<N, PL::R1, PL::R0, true, L, PITCH>(
+      sre, sim, tw, DerivColEpi{dst, ca, cb, es, oka, okb, epi, &acc});
   if (epi == EPI_SUMSQ)
     block_reduce_store(acc, partials + (long long)blockIdx.z * nparts, blockIdx.x + gridDim.x * blockIdx.y);
 }
@@ -890,7 +920,7 @@ static int cols_impl(float2* data, long long pstr, long long fstr, int ncols, in
                      long long es, int nf, int nprob, const int* active, cudaStream_t s) {
   const float2* tw = twiddles(N);
   if (!tw) return (int)cudaErrorMemoryAllocation;
-  size_t sm = col_smem<N, V>(2);
+  size_t sm = col_smem<N, V>(1);  // one line buffer: the first stage reads global memory
   int e = set_smem(k_cols<N, INV, V>, sm);
   if (e) return e;
   dim3 grid((ncols + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, nf, nprob);
@@ -1088,8 +1118,8 @@ static int spectral3_explicit_impl(const float* in, float* out, float2* spec, co
   const int n3h = N / 2 + 1;
   const int nrows = d.n1 * d.n2;
   int e = set_smem(k_r2c_rows<N, V>, row_smem<N, V>(false));
-  if (!e) e = set_smem(k_cols<N, false, V>, col_smem<N, V>(2));
-  if (!e) e = set_smem(k_cols<N, true, V>, col_smem<N, V>(2));
+  if (!e) e = set_smem(k_cols<N, false, V>, col_smem<N, V>(1));
+  if (!e) e = set_smem(k_cols<N, true, V>, col_smem<N, V>(1));
   if (!e) e = set_smem(k_pencil1<N, V>, col_smem<N, V>(2));
   if (!e) e = set_smem(k_c2r_rows<N, V>, row_smem<N, V>(true));
   if (e) return e;
@@ -1099,10 +1129,10 @@ static int spectral3_explicit_impl(const float* in, float* out, float2* spec, co
   const int ncx1 = d.n2 * n3h;
   const dim3 pen((ncx1 + ColCfg<N, V>::C - 1) / ColCfg<N, V>::C, 3, 1);
   k_r2c_rows<N, V><<<rows, kThreads, row_smem<N, V>(false), s>>>(in, 0, n, spec, 0, nc, nrows, tw, nullptr);
-  k_cols<N, false, V><<<cols, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+  k_cols<N, false, V><<<cols, kThreads, col_smem<N, V>(1), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                           nullptr);
   k_pencil1<N, V><<<pen, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, d, op, params, tw, nullptr);
-  k_cols<N, true, V><<<cols, kThreads, col_smem<N, V>(2), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
+  k_cols<N, true, V><<<cols, kThreads, col_smem<N, V>(1), s>>>(spec, 0, nc, ncx2, n3h, (long long)d.n2 * n3h, n3h, tw,
                                                          nullptr);
   k_c2r_rows<N, V><<<rows, kThreads, row_smem<N, V>(true), s>>>(spec, 0, nc, out, 0, n, nrows, tw, EPI_STORE, nullptr,
                                                            nullptr, 0, nullptr, nullptr);

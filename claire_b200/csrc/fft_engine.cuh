@@ -293,6 +293,111 @@ CB_DEVICE void fft_lines(float* re, float* im, float* sre, float* sim, const flo
   __syncthreads();
 }
 
+// Column layout (lines are columns of a strided array; the thread's line p is
+// threadIdx.x % NL in every stage because kFftThreads % NL == 0): the first
+// stage can read its inputs straight from global memory and the last one
+// write its outputs straight back, the warp's lanes covering NL adjacent
+// columns at one element (coalesced).  The arithmetic is fft_stage's, so
+// results are bit-identical to staging the lines in shared memory first.
+
+// First stage (span 1: no twiddles) reading element e of the thread's line p
+// through ld(p, e) (a float2), into (dre, dim).
+template <int N, int R, bool INV, int NL, int PITCH, class Load>
+CB_DEVICE void fft_stage_in(const Load& ld, float* __restrict__ dre, float* __restrict__ dim) {
+  constexpr int J = N / R;
+  constexpr int total = NL * J;
+  static_assert(kFftThreads % NL == 0, "a thread keeps its line across stages");
+#pragma unroll 2
+  for (int u = threadIdx.x; u < total; u += kFftThreads) {
+    const int p = u % NL;
+    const int j = u / NL;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = ld(p, j + r * J);
+    Dft<R, INV>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int idx = (j * R + r) * PITCH + p;
+      dre[idx] = v[r].x;
+      dim[idx] = v[r].y;
+    }
+  }
+}
+
+// Last stage (span NS) from (sre, sim), handing element e of line p to
+// st(p, e, value).
+template <int N, int R, int NS, bool INV, int NL, int PITCH, class Store>
+CB_DEVICE void fft_stage_out(const float* __restrict__ sre, const float* __restrict__ sim,
+                             const float2* __restrict__ tw, const Store& st) {
+  constexpr int J = N / R;
+  constexpr int total = NL * J;
+  static_assert(kFftThreads % NL == 0, "a thread keeps its line across stages");
+#pragma unroll 2
+  for (int u = threadIdx.x; u < total; u += kFftThreads) {
+    const int p = u % NL;
+    const int j = u / NL;
+    const int k = j % NS;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int idx = (j + r * J) * PITCH + p;
+      v[r] = make_float2(sre[idx], sim[idx]);
+    }
+    if (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = tw[r * k * (N / (NS * R))];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    Dft<R, INV>::run(v);
+    const int o = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) st(p, o + r * NS, v[r]);
+  }
+}
+
+// The two for a column of complex elements colp[e * es] (colp null: zeros in,
+// nothing out).
+struct ColumnLoad {
+  const float2* colp;
+  long long es;
+  CB_DEVICE float2 operator()(int, int e) const {
+    return colp ? __ldg(colp + (long long)e * es) : make_float2(0.f, 0.f);
+  }
+};
+struct ColumnStore {
+  float2* colp;
+  long long es;
+  CB_DEVICE void operator()(int, int e, float2 v) const {
+    if (colp) colp[(long long)e * es] = v;
+  }
+};
+
+// Shared-memory lines (re, im) as a stage's destination.
+template <int PITCH>
+struct SmemStore {
+  float* re;
+  float* im;
+  CB_DEVICE void operator()(int p, int e, float2 v) const {
+    re[e * PITCH + p] = v.x;
+    im[e * PITCH + p] = v.y;
+  }
+};
+
+template <int N, int R, bool INV, int NL, int PITCH>
+CB_DEVICE void fft_stage_load(const float2* __restrict__ colp, long long es, float* __restrict__ dre,
+                              float* __restrict__ dim) {
+  fft_stage_in<N, R, INV, NL, PITCH>(ColumnLoad{colp, es}, dre, dim);
+}
+
+template <int N, int R, int NS, bool INV, int NL, int PITCH>
+CB_DEVICE void fft_stage_store(const float* __restrict__ sre, const float* __restrict__ sim,
+                               const float2* __restrict__ tw, float2* __restrict__ colp, long long es) {
+  fft_stage_out<N, R, NS, INV, NL, PITCH>(sre, sim, tw, ColumnStore{colp, es});
+}
+
 // Stage the N-entry twiddle table into shared memory.
 template <int N>
 CB_DEVICE void load_twiddles(float2* dst, const float2* __restrict__ src) {

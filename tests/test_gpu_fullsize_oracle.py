@@ -9,14 +9,15 @@ gathers see the recipe's box sizes), on the same FP32 inputs:
 
 * transported image, distance, regularisation functional, objective,
   adjoint at t = 0 and body force (of the gradient and of the Hessian
-  matvec), preconditioner: within 1e-5 relative (L2 for fields);
-* gradient and GN Hessian matvec: within 1e-5, or within 1.5 times the error
-  of the reference's own single-precision arithmetic (the C++ restatement in
-  FP32) when that is larger.  For H2 it is: the operator's symbol
-  beta0 (kappa^2 + beta1) carries no hd and reaches 1.5e8 beta0 at 128^3, and
-  an FP32 field's roundoff at high wavenumbers, multiplied by it, is ~1% of
-  the result (the reference's FP32 build included); both outputs are
-  dominated by that term.
+  matvec): within 1e-5 relative (L2 for fields);
+* gradient, GN Hessian matvec and preconditioner: within 1e-5, or within 1.5
+  times the error of the reference's own single-precision arithmetic (the C++
+  restatement in FP32) when that is larger.  For H2 it is: the operator's
+  symbol beta0 (kappa^2 + beta1) carries no hd and reaches 1.5e8 beta0 at
+  128^3, so an FP32 field's roundoff at high wavenumbers comes out at ~1% of
+  the gradient and the Hessian matvec (the reference's FP32 build included),
+  and the inverse symbol reaches 1 / (beta0 beta1) = 1e7 at k = 0, so the
+  preconditioner's FP32 error is 2.1e-5 at 128^3 and 2.4e-5 at 256^3.
 """
 import numpy as np
 import pytest
@@ -81,12 +82,12 @@ def test_operators_at_full_size(cuda, n, norm, beta, config):
     torch.cuda.empty_cache()
 
     ref = cpu_side(n, nt, norm, beta, mR, mT, v, vt, fp64=True)
-    for k in ("m1", "lam", "bf", "lamt", "bft", "P"):
-        assert rel(dev[k], ref[k]) < 1e-5, k
+    for k in ("m1", "lam", "bf", "lamt", "bft"):
+        assert rel(dev[k], ref[k]) < 1e-5, (k, rel(dev[k], ref[k]))
     for k in ("D", "R", "J"):
         assert abs(dev[k] - ref[k]) <= 1e-5 * abs(ref[k]), k
     single = cpu_side(n, nt, norm, beta, mR, mT, v, vt, fp64=False)
-    for k in ("g", "H"):
+    for k in ("g", "H", "P"):
         tol = max(1e-5, 1.5 * rel(single[k], ref[k]))
         assert rel(dev[k], ref[k]) < tol, (k, rel(dev[k], ref[k]), rel(single[k], ref[k]))
 
