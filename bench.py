@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--beta", type=float, default=1e-3)
     ap.add_argument("--maxit", type=int, default=10)
     ap.add_argument("--opttol", type=float, default=1e-2)
-    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--batch", type=int, default=8, help="registrations per GPU per step")
     ap.add_argument("--no-plain", action="store_true", help="skip the single-problem comparison leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--serve", action="store_true",
@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--conv-norm", default="h1s", help="norm of the converging leg (its Newton system carries hd)")
     ap.add_argument("--conv-beta", type=float, default=1e-4, help="beta of the converging leg")
     ap.add_argument("--conv-maxit", type=int, default=50, help="GN iteration cap of the converging leg")
+    ap.add_argument("--conv-nt", type=int, default=16, help="time steps of the converging leg")
     ap.add_argument("--no-converge", action="store_true", help="skip the converging leg")
     ap.add_argument("--profile-case", action="store_true",
                     help="small fixed workload for ncu captures: one 128^3 recipe problem, objective, gradient, "
@@ -320,7 +321,7 @@ def converging_leg(cb, a, probs, stream, zero_v):
     every problem reached relative mismatch <= 1e-2 and |g| <= 1e-2 |g0|."""
     import torch
     B = len(probs)
-    opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.nt), "-regnorm", a.conv_norm, "-beta", repr(a.conv_beta),
+    opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.conv_nt), "-regnorm", a.conv_norm, "-beta", repr(a.conv_beta),
                      "-maxit", str(a.conv_maxit), "-opttol", "1e-2"])
     ci = cb.CLAIREInterface(opt, nbatch=B)
     ci.set_stream(stream)
@@ -338,7 +339,7 @@ def converging_leg(cb, a, probs, stream, zero_v):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st = [ci.stats(b) for b in range(B)]
-        out = {"workload": f"{B} registrations {a.n}^3 {a.conv_norm} beta={a.conv_beta} nt={a.nt} "
+        out = {"workload": f"{B} registrations {a.n}^3 {a.conv_norm} beta={a.conv_beta} nt={a.conv_nt} "
                            f"maxit={a.conv_maxit} opttol=0.01, same recipe problems",
                "value": B / (ms / 1e3), "unit": "registrations/s", "ms": ms,
                "rel_mismatch": [s["rel_mismatch"] for s in st],
