@@ -61,10 +61,11 @@ def parse():
                     help="mixed batch instead: 12 x 64^3 + 12 x 96^3 + 8 x 128^3 (H1 beta=1e-2, nt=4) served "
                          "together against plain one-at-a-time runs")
     ap.add_argument("--mixed-slots", type=int, default=12, help="--mixed: slots per pool")
-    ap.add_argument("--conv-norm", default="h1s", help="norm of the converging leg (its Newton system carries hd)")
+    ap.add_argument("--conv-norm", default="h1s",
+                    help="norm of the converging leg (the reference's synthetic problem; its Newton system carries hd)")
     ap.add_argument("--conv-beta", type=float, default=1e-4, help="beta of the converging leg")
     ap.add_argument("--conv-maxit", type=int, default=50, help="GN iteration cap of the converging leg")
-    ap.add_argument("--conv-nt", type=int, default=16, help="time steps of the converging leg")
+    ap.add_argument("--conv-nt", type=int, default=8, help="time steps of the converging leg")
     ap.add_argument("--no-converge", action="store_true", help="skip the converging leg")
     ap.add_argument("--profile-case", action="store_true",
                     help="small fixed workload for ncu captures: one 128^3 recipe problem, objective, gradient, "
@@ -307,29 +308,35 @@ def run_ours(a, rank, world, local):
     roof = roofline(cb, a, ci, load_device, B) if rank == 0 else None
     ci.close()
     fixed = fixed_work(cb, a, probs, stream, zero_v) if rank == 0 else None
-    conv = converging_leg(cb, a, probs, stream, zero_v) if (rank == 0 and not a.no_converge) else None
+    conv = converging_leg(cb, a, stream, B) if (rank == 0 and not a.no_converge) else None
     return dict(total_ms=total_ms, lat=lat_all, lat_srv=lat_srv, stats=stats, e2e_ms=e2e_ms, h2d=h2d, d2h=d2h,
                 launches=launches, clocks=clk.summary(), plain=plain, roof=roof, tuned=tuned, fixed=fixed,
                 conv=conv)
 
 
-def converging_leg(cb, a, probs, stream, zero_v):
-    """The same 128^3 recipe problems registered with a norm whose Newton
-    system carries hd (the headline's H2 gradient lacks it, so those solves
-    never reach the metric's 1e-2 mismatch): one batch solved to the
-    gradient tolerance 1e-2, timed with CUDA events; the line states whether
-    every problem reached relative mismatch <= 1e-2 and |g| <= 1e-2 |g0|."""
+def converging_leg(cb, a, stream, B):
+    """Registrations/s to the metric's target: the headline H2 solves never
+    reach a relative mismatch of 1e-2 (the H2 gradient lacks the hd of its
+    objective), so this leg registers the reference's own synthetic problem
+    (-synthetic 0: sin^2 template transported by the trig velocity,
+    src/CLAIREBase.cpp:1026-1250) at the same grid with the H1 seminorm, whose
+    Newton system carries hd: a batch of B copies solved to the gradient
+    tolerance 1e-2, timed with CUDA events; the line states whether every
+    problem reached relative mismatch <= 1e-2 and |g| <= 1e-2 |g0|."""
     import torch
-    B = len(probs)
+    from claire_b200 import synthetic
+    dev = torch.device("cuda", torch.cuda.current_device())
+    mR, mT, _ = synthetic.sin2_problem(a.n, a.conv_nt, reference_case=True, device=dev)
+    zero = torch.zeros((3, a.n, a.n, a.n), device=dev)
     opt = cb.RegOpt(["-nx", str(a.n), "-nt", str(a.conv_nt), "-regnorm", a.conv_norm, "-beta", repr(a.conv_beta),
                      "-maxit", str(a.conv_maxit), "-opttol", "1e-2"])
     ci = cb.CLAIREInterface(opt, nbatch=B)
     ci.set_stream(stream)
     out = None
     for rep in range(2):  # warm-up, then timed
-        for b, (mR, mT, _) in enumerate(probs):
+        for b in range(B):
             ci.set_images(mR, mT, b)
-            ci.SetInitialGuess(zero_v, b)
+            ci.SetInitialGuess(zero, b)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -339,15 +346,13 @@ def converging_leg(cb, a, probs, stream, zero_v):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st = [ci.stats(b) for b in range(B)]
-        out = {"workload": f"{B} registrations {a.n}^3 {a.conv_norm} beta={a.conv_beta} nt={a.conv_nt} "
-                           f"maxit={a.conv_maxit} opttol=0.01, same recipe problems",
+        out = {"workload": f"{B} registrations of the reference's synthetic problem (-synthetic 0) at {a.n}^3, "
+                           f"{a.conv_norm} beta={a.conv_beta} nt={a.conv_nt} maxit={a.conv_maxit} opttol=0.01",
                "value": B / (ms / 1e3), "unit": "registrations/s", "ms": ms,
-               "rel_mismatch": [s["rel_mismatch"] for s in st],
-               "grad_reduction": [s["gnorm"] / s["gnorm0"] for s in st],
-               "gn_iterations": [s["gn_iterations"] for s in st],
-               "pcg_iterations": [s["pcg_iterations"] for s in st]}
-    out["reaches_target"] = bool(all(m <= 1e-2 for m in out["rel_mismatch"]) and
-                                 all(g <= 1e-2 for g in out["grad_reduction"]))
+               "rel_mismatch": max(s["rel_mismatch"] for s in st),
+               "grad_reduction": max(s["gnorm"] / s["gnorm0"] for s in st),
+               "gn_iterations": st[0]["gn_iterations"], "pcg_iterations": st[0]["pcg_iterations"]}
+    out["reaches_target"] = bool(out["rel_mismatch"] <= 1e-2 and out["grad_reduction"] <= 1e-2)
     ci.close()
     return out
 

@@ -451,10 +451,12 @@ CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ 
     cp_async_wait_all();
     __syncthreads();
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
+    // two points per instruction (packed f32x2 pairs), as the table-driven gathers
 #pragma unroll
-    for (int a = 0; a < kTilePts; ++a) {
-      const BoxPoint bp = box_point(dd[a], tt.x1(a), tt, tt.valid_idx(a), bx);
-      epi(tt, a, gather_staged(sbase, bp, bx));
+    for (int a = 0; a < kTilePts; a += 2) {
+      const float2 r = gather_staged_pair(sbase, dd[a], dd[a + 1], a, tt, bx);
+      epi(tt, a, r.x);
+      epi(tt, a + 1, r.y);
     }
   } else {
 #pragma unroll

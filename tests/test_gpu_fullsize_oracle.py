@@ -116,3 +116,43 @@ def test_gathers_against_the_reference_kernel(cuda):
         g = got.cpu().numpy()
         assert rel(g, ref_interp3.interp3(f, dh, "f64")) < 1e-6
         assert rel(g, ref_interp3.interp3(f, dh, "f32")) < 2e-6
+
+
+def test_registration_to_the_metric_target_at_128(cuda):
+    """A whole 128^3 registration against the FP64 restatement run to the
+    end: the reference's own synthetic problem (-synthetic 0) with the H1
+    seminorm (no kappa = 0 amplification: counts are reproducible), beta 1e-4,
+    nt 8, gradient tolerance 1e-2.  Both reach relative mismatch <= 1e-2 with
+    |g| <= 1e-2 |g0|; GN and PCG counts agree within one, the mismatch within
+    1e-4 relative and the velocity within 1e-3 relative L2."""
+    import torch
+
+    import claire_b200 as cb
+    from claire_b200 import synthetic
+
+    n, nt, norm, beta = 128, 8, "h1s", 1e-4
+    mR_d, mT_d, _ = synthetic.sin2_problem(n, nt, reference_case=True, device=cuda)
+    torch.cuda.synchronize()
+    mR = mR_d.cpu().numpy()
+    mT = mT_d.cpu().numpy()
+    opt = cb.RegOpt(["-nx", str(n), "-nt", str(nt), "-regnorm", norm, "-beta", repr(beta), "-maxit", "50",
+                     "-opttol", "1e-2"])
+    with cb.CLAIREInterface(opt) as ci:
+        ci.set_images(mR, mT)
+        ci.Run()
+        st = ci.stats()
+        v = ci.GetSolution()
+    ref = CpuRef((n,) * 3, nt, norm, beta, fp64=True)
+    ref.set_images(mR, mT)
+    ref.set_gn(maxit=50, gttol=1e-2)
+    rs = ref.run()
+    vr = ref.velocity()
+    ref.close()
+    facts = (st["gn_iterations"], st["pcg_iterations"], st["rel_mismatch"], rs["iters"], rs["pcg_iters"],
+             rs["rel_mismatch"], rel(v, vr))
+    assert st["rel_mismatch"] <= 1e-2 and st["gnorm"] <= 1e-2 * st["gnorm0"], facts
+    assert rs["rel_mismatch"] <= 1e-2, facts
+    assert abs(st["gn_iterations"] - rs["iters"]) <= 1, facts
+    assert abs(st["pcg_iterations"] - rs["pcg_iters"]) <= 1, facts
+    assert abs(st["rel_mismatch"] - rs["rel_mismatch"]) <= 1e-4 * rs["rel_mismatch"], facts
+    assert rel(v, vr) < 1e-3, facts
