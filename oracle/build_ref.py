@@ -15,8 +15,10 @@ as it lies in the reference tree (nothing is copied) into
   switch to the Intel-compiler AVX kernels, include/interp3.hpp:37-39).
 
 The reference builds with -O3 -fopenmp -march=native (config/setup.mk:12-22);
-here -O3 -fopenmp -mavx2 -mfma (a portable x86-64 instruction set).  The built libraries travel with the repository's other built files;
-/root/reference itself is read only when it is present (this build host).
+here -O3 -fopenmp -mavx2 -mfma (a portable x86-64 instruction set).  The
+built libraries travel with the repository's other built files; the
+reference tree itself is read only where it is present (the host that builds
+the libraries).
 
   python oracle/build_ref.py
 """

@@ -142,7 +142,7 @@ def test_newton_step_sensitivity(norm, beta, amplified):
     1/(beta0 beta1) at k = 0, and H2's gradient lacks the hd of its objective,
     src/RegularizationH2.cpp:164, 239), while the seminorms stay near
     roundoff.  Measured on the oracle itself at the second GN iterate of the
-    16^3 configuration-1 problem."""
+    16^3 problem with the sin^2 template and the trig velocity."""
     n, nt = 16, 4
     mR, mT, _ = R.synthetic_c1(n, np.float64, nt)
     prob = R.Problem(mR, mT, nt, R.Regularization(norm, beta))

@@ -53,7 +53,7 @@ def cpu_solve(fp64, n, nt, norm, beta, mR, mT, maxit):
 
 
 CASES = [
-    # the benchmark norm on the benchmark recipe (configuration-1 seeds), 64^3
+    # the benchmark norm on the ellipsoid recipe (seed set 1), 64^3
     ("h2", 1e-3, 64, 8, "ellipsoids", 0),
     ("h2", 1e-3, 64, 8, "ellipsoids", 1),
 ]
@@ -87,7 +87,7 @@ def test_counts_against_both_reference_precisions(cb, monkeypatch, norm, beta, n
 
 
 def test_h1_counts_follow_fp32_arithmetic(cb, monkeypatch):
-    """H1 (beta 1e-2) on the 32^3 configuration-1 problem: the reference's
+    """H1 (beta 1e-2) on the 32^3 sin^2 / trig-velocity problem: the reference's
     FP64 build takes 1 + 1 + 4 PCG iterations, its FP32 build 1 + 6 + 14 (the
     third Newton system amplifies roundoff by 1 / (beta0 beta1) = 1e6 at
     k = 0, so the FP32 count is not reproducible to +-1 across two FFT
