@@ -6,7 +6,12 @@
 // into free slots at every GN-iteration boundary (Solver::begin), advances all
 // running slots by one GN iteration per Solver::step, and retires the slots
 // whose stopping test fired (Solver::finish), copying the velocity out and
-// freeing the slot for the next request.  Pools of different keys run
+// freeing the slot for the next request.  Host copies go through page-locked
+// blocks that each pool allocates when it starts and that are recycled:
+// submit puts the images into a free one, so the worker's upload is a DMA,
+// and the worker writes each velocity into one that result() copies out, so
+// the worker never copies a velocity on the CPU; without a free block the
+// pageable path is used.  Pools of different keys run
 // concurrently on their own streams, so the work of requests of different
 // sizes overlaps on the device.  Pools are created while their footprint
 // (Solver::estimate_bytes) fits the HBM budget and release their memory after
@@ -37,8 +42,10 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   long long id = 0;
   claire_b200_opts opts{};
-  std::vector<float> mR, mT;  // host copies of the inputs
-  std::vector<float> v;       // result velocity (host)
+  std::vector<float> mR, mT;  // host copies of the inputs (pageable path)
+  float* in_pin = nullptr;    // or page-locked: mR then mT
+  std::vector<float> v;       // result velocity (pageable path)
+  float* v_pin = nullptr;     // or page-locked
   claire_b200_stats stats{};
   int status = CB_REQ_QUEUED;
   int error = CB_OK;
@@ -71,6 +78,10 @@ struct claire_b200_server {
   long long budget = 0, used = 0;
   long long next_id = 1;
   bool stop = false;
+  // page-locked host blocks per direction (0 inputs, 1 results): free lists
+  // and blocks allocated, by float count
+  std::map<long long, std::vector<float*>> pinned_free[2];
+  std::map<long long, int> pinned_count[2];
 };
 
 namespace cb {
@@ -96,6 +107,51 @@ static void reap_locked(claire_b200_server* s) {
     } else {
       ++it;
     }
+  }
+}
+
+// Page-locked blocks of `count` floats for direction dir (0: request inputs,
+// 1: results).  A pool's worker allocates them when it starts (the pool's
+// slot count twice over, at most kPinnedPerSize bytes of one size and
+// direction); take_pinned only recycles, so no request waits on a
+// page-locked allocation, and returns nullptr when none is free (the caller
+// uses pageable memory).
+constexpr long long kPinnedPerSize = 512LL << 20;
+
+static float* take_pinned(claire_b200_server* s, int dir, long long count) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto& fl = s->pinned_free[dir][count];
+  if (fl.empty()) return nullptr;
+  float* p = fl.back();
+  fl.pop_back();
+  return p;
+}
+
+// Return a block to its free list (caller holds s->mu).
+static void give_pinned_locked(claire_b200_server* s, int dir, long long count, float* p) {
+  if (p) s->pinned_free[dir][count].push_back(p);
+}
+
+// Bring the blocks of one size and direction up to `want` (bounded by
+// kPinnedPerSize); called by a worker without s->mu held.
+static void prealloc_pinned(claire_b200_server* s, int dir, long long count, int want) {
+  const long long bytes = count * (long long)sizeof(float);
+  want = (int)std::max(1LL, std::min<long long>(want, kPinnedPerSize / std::max(1LL, bytes)));
+  while (true) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->pinned_count[dir][count] >= want) return;
+      ++s->pinned_count[dir][count];
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, (size_t)bytes, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      std::lock_guard<std::mutex> lk(s->mu);
+      --s->pinned_count[dir][count];
+      return;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->pinned_free[dir][count].push_back(static_cast<float*>(p));
   }
 }
 
@@ -189,19 +245,24 @@ static std::vector<std::pair<int, long long>> admit_locked(claire_b200_server* s
   return out;
 }
 
+// Inputs of request r into slot b.  The copies are complete when this returns
+// (set_problem synchronises the stream), so the request's input block can be
+// recycled.
 static int load_slot(Solver& sv, int b, const Request& r) {
   const long long n = sv.n;
+  const float* hR = r.in_pin ? r.in_pin : r.mR.data();
+  const float* hT = r.in_pin ? r.in_pin + n : r.mT.data();
   if (sv.img16) {
     // stage through the free slot's PCG work vector, then round to bf16
     float* st = sv.x + b * 3 * n;
-    if (cudaMemcpyAsync(st, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess ||
-        cudaMemcpyAsync(st + n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess)
+    if (cudaMemcpyAsync(st, hR, sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess ||
+        cudaMemcpyAsync(st + n, hT, sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) != cudaSuccess)
       return CB_ERR_CUDA;
     if (int e = sv.load_images(b, st, st + n)) return e;
     if (cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess) return CB_ERR_CUDA;
-  } else if (cudaMemcpyAsync(sv.mR + b * n, r.mR.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+  } else if (cudaMemcpyAsync(sv.mR + b * n, hR, sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
                  cudaSuccess ||
-             cudaMemcpyAsync(sv.mT + b * n, r.mT.data(), sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
+             cudaMemcpyAsync(sv.mT + b * n, hT, sizeof(float) * n, cudaMemcpyHostToDevice, sv.stream) !=
                  cudaSuccess ||
              cudaMemsetAsync(sv.v + b * 3 * n, 0, sizeof(float) * 3 * n, sv.stream) != cudaSuccess) {
     return CB_ERR_CUDA;
@@ -236,6 +297,8 @@ static void worker_main(claire_b200_server* s, Pool* p) {
   cudaSetDevice(s->opts.device);
   Solver& sv = *p->solver;
   const int S = sv.B;
+  prealloc_pinned(s, 0, 2 * sv.n, 2 * S);
+  prealloc_pinned(s, 1, 3 * sv.n, 2 * S);
   int err = CB_OK;
   while (true) {
     std::vector<std::pair<int, long long>> admits;
@@ -291,6 +354,11 @@ static void worker_main(claire_b200_server* s, Pool* p) {
         r = &s->reqs.at(a.second);
       }
       err = load_slot(sv, a.first, *r);
+      if (r->in_pin) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        give_pinned_locked(s, 0, 2 * sv.n, r->in_pin);
+        r->in_pin = nullptr;
+      }
       if (err) break;
       sel_new[a.first] = 1;
     }
@@ -309,24 +377,38 @@ static void worker_main(claire_b200_server* s, Pool* p) {
     if (!err && anydone) err = sv.finish(done);
     if (err) break;
     if (anydone) {
-      std::vector<std::pair<int, std::vector<float>>> outv;
-      for (int b = 0; b < S; ++b) {
+      // velocities into page-locked blocks (one synchronisation for all), or
+      // into pageable vectors past the cap
+      struct Out {
+        int b;
+        float* pin;
+        std::vector<float> vh;
+      };
+      std::vector<Out> outv;
+      const long long nv = 3 * sv.n;
+      for (int b = 0; b < S && !err; ++b) {
         if (!done[b]) continue;
-        std::vector<float> vh((size_t)(3 * sv.n));
-        if (cudaMemcpyAsync(vh.data(), sv.v + b * 3 * sv.n, sizeof(float) * 3 * sv.n, cudaMemcpyDeviceToHost,
-                            sv.stream) != cudaSuccess ||
-            cudaStreamSynchronize(sv.stream) != cudaSuccess) {
+        Out o{b, take_pinned(s, 1, nv), {}};
+        if (!o.pin) o.vh.resize((size_t)nv);
+        float* dst = o.pin ? o.pin : o.vh.data();
+        if (cudaMemcpyAsync(dst, sv.v + b * nv, sizeof(float) * nv, cudaMemcpyDeviceToHost, sv.stream) !=
+                cudaSuccess ||
+            (!o.pin && cudaStreamSynchronize(sv.stream) != cudaSuccess))
           err = CB_ERR_CUDA;
-          break;
-        }
-        outv.push_back({b, std::move(vh)});
+        outv.push_back(std::move(o));
       }
-      if (err) break;
+      if (!err && cudaStreamSynchronize(sv.stream) != cudaSuccess) err = CB_ERR_CUDA;
+      if (err) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (auto& o : outv) give_pinned_locked(s, 1, nv, o.pin);
+        break;
+      }
       std::lock_guard<std::mutex> lk(s->mu);
       for (auto& o : outv) {
-        const int b = o.first;
+        const int b = o.b;
         Request& r = s->reqs.at(p->slot_req[b]);
-        r.v = std::move(o.second);
+        r.v = std::move(o.vh);
+        r.v_pin = o.pin;
         fill_stats(sv.ps[b], &r.stats);
         r.status = CB_REQ_DONE;
         r.t_done = Clock::now();
@@ -403,17 +485,26 @@ int claire_b200_server_submit(claire_b200_server* s, const claire_b200_opts* o, 
   const long long n = (long long)o->nx[0] * o->nx[1] * o->nx[2];
   cb::srv::Request r;
   r.opts = *o;
-  try {
-    r.mR.assign(mR, mR + n);
-    r.mT.assign(mT, mT + n);
-  } catch (...) {
-    return CB_ERR_ALLOC;
+  r.in_pin = cb::srv::take_pinned(s, 0, 2 * n);
+  if (r.in_pin) {
+    std::memcpy(r.in_pin, mR, sizeof(float) * n);
+    std::memcpy(r.in_pin + n, mT, sizeof(float) * n);
+  } else {
+    try {
+      r.mR.assign(mR, mR + n);
+      r.mT.assign(mT, mT + n);
+    } catch (...) {
+      return CB_ERR_ALLOC;
+    }
   }
   r.t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(s->mu);
-  if (s->stop) return CB_ERR_STATE;
+  const bool too_large = cb::Solver::estimate_bytes(*o, std::max(1, s->opts.slots_per_pool)) > s->budget;
+  if (s->stop || too_large) {
+    cb::srv::give_pinned_locked(s, 0, 2 * n, r.in_pin);
+    return s->stop ? CB_ERR_STATE : CB_ERR_TOO_LARGE;
+  }
   cb::srv::reap_locked(s);
-  if (cb::Solver::estimate_bytes(*o, std::max(1, s->opts.slots_per_pool)) > s->budget) return CB_ERR_TOO_LARGE;
   r.id = s->next_id++;
   *id = r.id;
   s->reqs.emplace(r.id, std::move(r));
@@ -455,13 +546,19 @@ int claire_b200_server_result(claire_b200_server* s, long long id, float* v, cla
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return CB_ERR_ARG;
   cb::srv::Request& r = it->second;
+  const long long n = (long long)r.opts.nx[0] * r.opts.nx[1] * r.opts.nx[2];
   if (r.status == CB_REQ_FAILED || r.status == CB_REQ_CANCELLED) {
     const int e = r.error ? r.error : CB_ERR_STATE;
+    cb::srv::give_pinned_locked(s, 0, 2 * n, r.in_pin);
     s->reqs.erase(it);
     return e;
   }
   if (r.status != CB_REQ_DONE) return CB_ERR_STATE;
-  if (v) std::memcpy(v, r.v.data(), sizeof(float) * r.v.size());
+  if (v) {
+    if (r.v_pin) std::memcpy(v, r.v_pin, sizeof(float) * 3 * n);
+    else std::memcpy(v, r.v.data(), sizeof(float) * r.v.size());
+  }
+  cb::srv::give_pinned_locked(s, 1, 3 * n, r.v_pin);
   if (st) *st = r.stats;
   if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
   s->reqs.erase(it);
@@ -514,6 +611,13 @@ int claire_b200_server_destroy(claire_b200_server* s) {
   }
   for (auto& p : s->pools)
     if (p->worker.joinable()) p->worker.join();
+  for (auto& kv : s->reqs) {
+    if (kv.second.in_pin) cudaFreeHost(kv.second.in_pin);
+    if (kv.second.v_pin) cudaFreeHost(kv.second.v_pin);
+  }
+  for (auto& fl : s->pinned_free)
+    for (auto& kv : fl)
+      for (float* p : kv.second) cudaFreeHost(p);
   delete s;
   return CB_OK;
 }
