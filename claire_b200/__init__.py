@@ -151,6 +151,8 @@ _signatures = {
     "claire_b200_smooth": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_distance": (_I, [_P, _P, _IA, _DA, _P]),
     "claire_b200_kernel_launches": (ctypes.c_longlong, []),
+    "claire_b200_stage_timeouts": (_I, [ctypes.POINTER(ctypes.c_longlong)]),
+    "claire_b200_stage_wait_selftest": (_I, [ctypes.c_longlong, _P]),
     "claire_b200_profile": (_I, [_P, _I]),
     "claire_b200_det_def_grad": (_I, [_P, _I, _I, _P, ctypes.POINTER(ctypes.c_double)]),
     "claire_b200_server_default_opts": (None, [_P]),
@@ -294,6 +296,19 @@ def set_fft_variant(n: int, variant: int) -> None:
 def kernel_launches() -> int:
     """CUDA kernel launches issued by the library since it was loaded."""
     return int(lib.claire_b200_kernel_launches())
+
+
+def stage_timeouts() -> int:
+    """Tile gathers on the current device whose shared-memory box copy ran out
+    of its bounded wait (claire_b200_stage_timeouts)."""
+    c = ctypes.c_longlong(0)
+    _check(lib.claire_b200_stage_timeouts(ctypes.byref(c)), "stage_timeouts")
+    return int(c.value)
+
+
+def stage_wait_selftest(wait_ns: int = 1_000_000) -> None:
+    """Make one bounded box-copy wait run out (claire_b200_stage_wait_selftest)."""
+    _check(lib.claire_b200_stage_wait_selftest(int(wait_ns), _stream()), "stage_wait_selftest")
 
 
 # ---------------------------------------------------------------------------

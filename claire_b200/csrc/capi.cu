@@ -803,6 +803,20 @@ int claire_b200_interp3(const float* f, const float* disp, float* out, const int
   return cuda_status(e);
 }
 
+int claire_b200_stage_timeouts(long long* count) {
+  if (!count) return CB_ERR_ARG;
+  unsigned long long t = 0;
+  if (stage_timeouts(&t)) return CB_ERR_CUDA;
+  *count = (long long)t;
+  return CB_OK;
+}
+
+int claire_b200_stage_wait_selftest(long long wait_ns, void* stream) {
+  if (wait_ns < 0 || wait_ns > 10000000000LL) return CB_ERR_ARG;
+  note_launches(1);
+  return cuda_status(launch_stage_wait_selftest((unsigned long long)wait_ns, (cudaStream_t)stream));
+}
+
 int claire_b200_interp3_bf16(const unsigned short* f, const float* disp, unsigned short* out, const int nx[3],
                              void* stream) {
   if (!f || !disp || !out || !dims_ok(nx)) return CB_ERR_ARG;

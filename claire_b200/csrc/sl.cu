@@ -457,4 +457,32 @@ int launch_field_stats(const float* f, long long fp, long long n, int nprob, dou
   return (int)cudaGetLastError();
 }
 
+// Health of the box copies' bounded waits: tile gathers on this device whose
+// box copy did not complete within the wait limit (each skipped its tile).
+int stage_timeouts(unsigned long long* count) {
+  unsigned v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_stage_timeouts, sizeof(unsigned)) != cudaSuccess) return (int)cudaGetLastError();
+  *count = v;
+  return 0;
+}
+
+// Self-test of the bounded wait: one CTA arms its barrier for 16 bytes that no
+// copy delivers and waits wait_ns, so the wait runs out, is counted, and the
+// kernel returns; the context stays usable.
+__global__ void __launch_bounds__(kTileThreads) k_stage_wait_selftest(unsigned long long wait_ns) {
+  __shared__ alignas(8) unsigned long long mbar;
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&mbar);
+  if (threadIdx.x == 0) {
+    mbar_init(bar);
+    mbar_arrive_expect(bar, 16u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) stage_box_wait(bar, wait_ns);  // nothing delivers the 16 bytes
+}
+
+int launch_stage_wait_selftest(unsigned long long wait_ns, cudaStream_t s) {
+  k_stage_wait_selftest<<<1, kTileThreads, 0, s>>>(wait_ns);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace cb

@@ -8,7 +8,10 @@
 // The CTA reads its points' displacements, reduces the bounding box of every
 // stencil tap over the tile (min / max of i + floor(d), widened by the
 // stencil's -1 .. +2) and, when the box fits, copies it into shared memory
-// with 16-byte cp.async (periodic wrap applied while copying).  The 64 taps
+// with bulk asynchronous copies (the TMA engine's untiled form), one per x3
+// row of the box (two where the row crosses the periodic x3 seam; the x1 / x2
+// wrap is applied per row), which complete on an mbarrier that every thread
+// waits on (bounded).  The 64 taps
 // per point are then served from shared memory; tiles whose box is too large
 // (large, rough displacements) gather from global memory instead.
 //
@@ -26,6 +29,7 @@
 #pragma once
 
 #include <climits>
+#include <type_traits>
 
 #include "sl.cuh"
 
@@ -208,6 +212,98 @@ CB_DEVICE void cp_async16(float* smem_dst, const float* gmem_src) {
 }
 CB_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 CB_DEVICE void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// ---- bulk box copies completing on an mbarrier ------------------------------
+// Count of tile gathers whose box copy did not complete within the wait limit
+// (the gather then skips its points); read by stage_timeouts().
+__device__ unsigned g_stage_timeouts = 0;
+
+// Wait limit of a box copy (ns of %globaltimer); the copies of one box take
+// microseconds.
+constexpr unsigned long long kStageWaitNs = 200000000ull;
+
+CB_DEVICE unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+CB_DEVICE void mbar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n\tfence.mbarrier_init.release.cluster;" ::"r"(bar)
+               : "memory");
+}
+// the barrier's one arrival, announcing the bytes its copies will deliver
+CB_DEVICE void mbar_arrive_expect(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+CB_DEVICE bool mbar_test(unsigned bar) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase 0 of the barrier for at most limit_ns; false on timeout.
+CB_DEVICE bool mbar_wait(unsigned bar, unsigned long long limit_ns) {
+  if (mbar_test(bar)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_test(bar))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+CB_DEVICE void bulk_copy(unsigned dst, const float* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// Bytes of a staged box (every copy of it lands on the barrier).
+CB_DEVICE unsigned box_bytes(const TileBox& bx) { return 4u * (unsigned)(bx.e1 * bx.e2 * bx.e3); }
+
+// Bulk copies of field f's box into the box at shared address sbase: row r of
+// the box (x1 plane r / e2, x2 row r % e2) by thread r (mod the CTA size).
+// Every source and destination is 16-byte aligned and every size a multiple
+// of 16 bytes: x3 starts on a multiple of 4 floats, N3 % 4 == 0, and P, Q are
+// multiples of 4.  (Issuing all rows from one warp instead ran 1.6 times
+// slower: the copies of a box must start from many threads at once.)
+CB_DEVICE void issue_box_bulk(unsigned sbase, const float* __restrict__ f, const TileBox& bx, const Dims& d,
+                              unsigned bar) {
+  const int rows = bx.e1 * bx.e2;
+  const int g3 = wrap_near(bx.lo[2], d.n3);
+  const int first = min(bx.e3, d.n3 - g3);  // floats before the x3 seam
+  const unsigned row = (unsigned)d.n3, plane = (unsigned)d.n2 * (unsigned)d.n3;
+  for (int r = threadIdx.x; r < rows; r += kTileThreads) {
+    const int l1 = small_div(r, bx.e2), l2 = r - l1 * bx.e2;
+    const int g1 = wrap_near(bx.lo[0] + l1, d.n1), g2 = wrap_near(bx.lo[1] + l2, d.n2);
+    const float* src = f + ((unsigned)g1 * plane + (unsigned)g2 * row);
+    const unsigned dst = sbase + 4u * (unsigned)(l1 * bx.Q + l2 * bx.P);
+    bulk_copy(dst, src + g3, 4u * (unsigned)first, bar);
+    if (first < bx.e3) bulk_copy(dst + 4u * (unsigned)first, src, 4u * (unsigned)(bx.e3 - first), bar);
+  }
+}
+
+// Start the bulk copy of a staged box: barrier set up and armed with the box's
+// bytes by thread 0, published to the CTA, then the row copies.  Contains
+// __syncthreads: call from uniform control flow.
+CB_DEVICE void stage_box_start(unsigned sbase, const float* __restrict__ f, const TileBox& bx, const Dims& d,
+                               unsigned bar) {
+  if (threadIdx.x == 0) {
+    mbar_init(bar);
+    mbar_arrive_expect(bar, box_bytes(bx));
+  }
+  __syncthreads();
+  issue_box_bulk(sbase, f, bx, d, bar);
+}
+
+// Wait for the box; on timeout count it, wait once more for the copies still
+// in flight (bounded as well) and report false: the caller skips its points.
+CB_DEVICE bool stage_box_wait(unsigned bar, unsigned long long limit_ns) {
+  if (mbar_wait(bar, limit_ns)) return true;
+  if (threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1u);
+  mbar_wait(bar, limit_ns);
+  return false;
+}
 
 // Issue the 16-byte asynchronous copies of field f's box into sb.  A warp
 // copies whole x3 rows (lanes over the row's chunks, coalesced); rows advance
@@ -446,11 +542,11 @@ CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ 
   src.load(dd, tt, d);
   const TileBox bx = tile_box(dd, tt, d);
   if (bx.within && bx.vol <= kGatherBudget) {
-    issue_box(sb, f, bx, d);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
+    __shared__ alignas(8) unsigned long long mbar;
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&mbar);
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
+    stage_box_start(sbase, f, bx, d, bar);
+    if (!stage_box_wait(bar, kStageWaitNs)) return;
     // two points per instruction (packed f32x2 pairs), as the table-driven gathers
 #pragma unroll
     for (int a = 0; a < kTilePts; a += 2) {
@@ -479,9 +575,15 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
                                const T* __restrict__ f, const Dims& d, const Epi& epi) {
   const TileBox bx = box_from_table(tab, d);
   const bool staged = bx.within && bx.vol <= kGatherBudget;
+  __shared__ alignas(8) unsigned long long mbar;
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&mbar);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
   if (staged) {
-    issue_box(sb, f, bx, d);
-    cp_async_commit();
+    if constexpr (std::is_same<T, float>::value) {
+      stage_box_start(sbase, f, bx, d, bar);
+    } else {
+      issue_box(sb, f, bx, d);  // bf16: widened to FP32 while staged (synchronous)
+    }
   }
   const TileThread tt = tile_thread(d);
   float dd[kTilePts][3], aux[kTilePts];
@@ -497,9 +599,11 @@ CB_DEVICE void tile_gather_tab(float* sb, const float* __restrict__ disp, const 
     aux[a] = (ok && epi.aux) ? __ldg(epi.aux + i) : 0.f;
   }
   if (staged) {
-    cp_async_wait_all();
-    __syncthreads();
-    const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
+    if constexpr (std::is_same<T, float>::value) {
+      if (!stage_box_wait(bar, kStageWaitNs)) return;
+    } else {
+      __syncthreads();
+    }
 #pragma unroll
     for (int a = 0; a < kTilePts; a += 2) {
       const float2 r = gather_staged_pair(sbase, dd[a], dd[a + 1], a, tt, bx);

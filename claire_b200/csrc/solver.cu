@@ -209,9 +209,21 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
   return bytes;
 }
 
+// A tile gather whose box copy ran out of its bounded wait skipped its tile
+// (sl_tile.cuh); report it once, at the next GN-iteration boundary.
+int Solver::check_stage() {
+  unsigned long long t = 0;
+  if (stage_timeouts(&t)) return CB_ERR_CUDA;
+  if (t <= stage_seen) return 0;
+  stage_seen = t;
+  err = "a tile gather's shared-memory box copy did not complete within its wait limit";
+  return CB_ERR_CUDA;
+}
+
 int Solver::init(const claire_b200_opts& o, int Bn) {
   opts = o;
   B = Bn;
+  stage_timeouts(&stage_seen);
   d = Dims{o.nx[0], o.nx[1], o.nx[2]};
   nt = o.nt;
   if (B < 1 || B > 1024 || nt < 1) {
@@ -1819,6 +1831,7 @@ int Solver::step(std::vector<int>& finished, double gttol, int miniter) {
   if (anyacc) CB_TRY(gradient_at_current(acc));
   for (int b = 0; b < B; ++b)
     if (acc[b]) ps[b].iter++;
+  CB_TRY(check_stage());
   if (opts.verbosity > 0) {
     // OptimizationMonitor line (src/TaoInterface.cpp:529-606)
     for (int b = 0; b < B; ++b)
@@ -1849,6 +1862,7 @@ int Solver::finish(const std::vector<int>& sel) {
   CB_TRY(launch_finalize(partials, maxparts, np, slot(S_RR), B, 1.0, false, stream, dact));
   note_launches(2);
   CB_TRY(fetch_scalars());
+  CB_TRY(check_stage());
   const auto t1 = std::chrono::steady_clock::now();
   for (int b = 0; b < B; ++b) {
     if (!sel[b]) continue;

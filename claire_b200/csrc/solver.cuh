@@ -94,6 +94,8 @@ class Solver {
   cudaStream_t own_stream = nullptr;  // the context's own stream
   std::vector<ProbState> ps;
   std::string err;
+  unsigned long long stage_seen = 0;  // box-copy timeouts of the device already reported
+  int check_stage();                  // CB_ERR_CUDA when a gather's box copy ran out of its wait
 
   // device state: one allocation per array, problem p at base + p * stride
   float *mR = nullptr, *mT = nullptr, *v = nullptr, *vtrial = nullptr, *m = nullptr;

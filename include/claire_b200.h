@@ -297,6 +297,19 @@ int claire_b200_distance(const float* mR, const float* m1, const int nx[3], doub
 /* Number of CUDA kernel launches issued by this library since load (all threads). */
 long long claire_b200_kernel_launches(void);
 
+/* Health of the tricubic gathers' bounded waits.  Each tile gather stages its
+ * box of the field in shared memory with bulk asynchronous copies that
+ * complete on a barrier; every wait for them is bounded (200 ms), and a wait
+ * that runs out is counted, its tile skipped and the kernel returns.
+ * claire_b200_stage_timeouts returns the count on the current device (a
+ * context's next GN step reports CB_ERR_CUDA when it grew).
+ * claire_b200_stage_wait_selftest launches one block that waits wait_ns for a
+ * copy that is never issued, so the count grows by one and the context stays
+ * usable.  The reference's interpolation has no device waits
+ * (src/interp3.cpp:2492-2719 runs on the host). */
+int claire_b200_stage_timeouts(long long* count);
+int claire_b200_stage_wait_selftest(long long wait_ns, void* stream);
+
 /* ---- Serving: continuous batching of independent registrations ----------
  * The reference runs one registration per CLAIREInterface::Run call
  * (src/CLAIREInterface.cpp:709-885) and has no serving layer; a server runs

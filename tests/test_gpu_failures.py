@@ -5,9 +5,10 @@ TAO_DIVERGED_NAN when the objective or the gradient norm is not finite
 (src/TaoInterface.cpp:425-436).  Here every entry point returns a status
 code; these tests make the failure on the host (a NaN written into a host
 image, a batch too large for the device, a budget smaller than a pool, a
-cancelled request) and check that it is reported cleanly, that the other
-problems of a batch or of a server are unaffected, and that the context or
-server stays usable.  No test faults, traps or hangs the GPU.
+cancelled request) or let a bounded device wait run out on a flag nothing
+sets, and check that it is reported cleanly, that the other problems of a
+batch or of a server are unaffected, and that the context or server stays
+usable.  No test faults, traps or hangs the GPU.
 """
 import os
 import time
@@ -149,3 +150,23 @@ def test_idle_pools_are_reaped(cb):
         assert info["pools"] == 0
         assert info["bytes_used"] == 0
         assert tasks() <= base
+
+
+def test_box_copy_wait_runs_out_cleanly(cb):
+    """The tile gathers wait for their shared-memory box copies with a bounded
+    wait.  The self-test arms a barrier for a copy that is never issued, so the
+    wait (1 ms here) runs out: the count of timeouts grows by one, the kernel
+    returns, and the device keeps computing correct gathers afterwards."""
+    import torch
+    before = cb.stage_timeouts()
+    cb.stage_wait_selftest(1_000_000)
+    torch.cuda.synchronize()
+    assert cb.stage_timeouts() == before + 1
+    n = 32
+    rng = np.random.default_rng(9)
+    f = rng.standard_normal((n, n, n)).astype(np.float32)
+    disp = rng.uniform(-2.5, 2.5, size=(3, n, n, n)).astype(np.float32)
+    out = cb.SemiLagrangian.Interpolate(torch.from_numpy(f).cuda(), torch.from_numpy(disp).cuda()).cpu().numpy()
+    ref = R.interp3(f.astype(np.float64), R.index_grid((n, n, n)) + disp.astype(np.float64))
+    assert np.linalg.norm((out - ref).ravel()) <= 1e-5 * np.linalg.norm(ref.ravel())
+    assert cb.stage_timeouts() == before + 1  # real copies complete within the limit
