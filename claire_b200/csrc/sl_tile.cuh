@@ -206,13 +206,6 @@ CB_DEVICE TileBox box_from_table(const int4* __restrict__ tab, const Dims&) {
   return bx;
 }
 
-CB_DEVICE void cp_async16(float* smem_dst, const float* gmem_src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
-CB_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-CB_DEVICE void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // ---- bulk box copies completing on an mbarrier ------------------------------
 // Count of tile gathers whose box copy did not complete within the wait limit
 // (the gather then skips its points); read by stage_timeouts().
@@ -305,45 +298,13 @@ CB_DEVICE bool stage_box_wait(unsigned bar, unsigned long long limit_ns) {
   return false;
 }
 
-// Issue the 16-byte asynchronous copies of field f's box into sb.  A warp
-// copies whole x3 rows (lanes over the row's chunks, coalesced); rows advance
-// incrementally, without divisions.  The box never exceeds the grid along an
-// axis, so one conditional subtraction wraps each coordinate.
-CB_DEVICE void issue_box(float* __restrict__ sb, const float* __restrict__ f, const TileBox& bx, const Dims& d) {
-  // warp w copies x1 planes w, w + 8, ...; its lanes cover rpi rows of nck
-  // 16-byte chunks at a time; pointers advance by whole rows, with one
-  // conditional wrap per row along x2 and per plane along x1
-  const int nck = bx.e3 >> 2;           // 16-byte chunks per row, 1 .. 16
-  const int rpi = small_div(32, nck);   // rows a warp copies per step
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int lr = small_div(lane, nck), lc = lane - lr * nck;
-  if (lr >= rpi || lr >= bx.e2) return;
-  int g1 = wrap_near(bx.lo[0] + warp, d.n1);
-  const int w2 = wrap_near(bx.lo[1] + lr, d.n2);
-  int g3 = wrap_near(bx.lo[2], d.n3) + 4 * lc;
-  g3 -= (g3 >= d.n3) ? d.n3 : 0;
-  const float* fb = f + g3;
-  const unsigned row = (unsigned)d.n3, plane = (unsigned)d.n2 * (unsigned)d.n3;
-  constexpr int kWarps = kTileThreads / 32;
-  for (int l1 = warp; l1 < bx.e1; l1 += kWarps) {
-    const float* fp = fb + (unsigned)g1 * plane;
-    float* sp = sb + l1 * bx.Q + lr * bx.P + 4 * lc;
-    int g2 = w2;
-    for (int l2 = lr; l2 < bx.e2; l2 += rpi) {
-      cp_async16(sp, fp + (unsigned)g2 * row);
-      sp += rpi * bx.P;
-      g2 += rpi;
-      while (g2 >= d.n2) g2 -= d.n2;
-    }
-    g1 += kWarps;
-    g1 -= (g1 >= d.n1) ? d.n1 : 0;
-  }
-}
-
-// bf16 image field: the same box, widened to FP32 while it is staged.  Each
-// 4-element chunk is one 8-byte load (x3 offsets are multiples of 4 and N3 %
-// 4 == 0, so every chunk is 8-byte aligned) and one 16-byte shared store; the
-// shared-memory layout, and so the gather that reads it, is the FP32 one.
+// bf16 image field: the box is widened to FP32 while it is staged, with plain
+// loads and stores.  Warp w copies x1 planes w, w + 8, ...; its lanes cover
+// whole x3 rows of 4-element chunks, rows advancing without divisions (one
+// conditional wrap per row along x2 and per plane along x1).  Each chunk is
+// one 8-byte load (x3 offsets are multiples of 4 and N3 % 4 == 0, so every
+// chunk is 8-byte aligned) and one 16-byte shared store; the shared-memory
+// layout, and so the gather that reads it, is the FP32 one.
 CB_DEVICE void issue_box(float* __restrict__ sb, const bf16* __restrict__ f, const TileBox& bx, const Dims& d) {
   const int nck = bx.e3 >> 2;
   const int rpi = small_div(32, nck);
