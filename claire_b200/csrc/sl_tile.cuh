@@ -228,20 +228,23 @@ CB_DEVICE void mbar_init(unsigned bar) {
 CB_DEVICE void mbar_arrive_expect(unsigned bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-CB_DEVICE bool mbar_test(unsigned bar) {
+// One try_wait on phase 0; a thread whose phase is not complete is suspended
+// by the hardware for up to hint_ns (or until the phase completes).
+CB_DEVICE bool mbar_test(unsigned bar, unsigned hint_ns) {
   unsigned ok;
   asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(bar)
+      : "r"(bar), "r"(hint_ns)
       : "memory");
   return ok != 0;
 }
 // Wait for phase 0 of the barrier for at most limit_ns; false on timeout.
+// Waiting threads sleep in try_wait (1 us at a time) instead of spinning.
 CB_DEVICE bool mbar_wait(unsigned bar, unsigned long long limit_ns) {
-  if (mbar_test(bar)) return true;
+  if (mbar_test(bar, 1000u)) return true;
   const unsigned long long t0 = global_ns();
-  while (!mbar_test(bar))
+  while (!mbar_test(bar, 1000u))
     if (global_ns() - t0 > limit_ns) return false;
   return true;
 }
