@@ -425,13 +425,14 @@ def tune(cb, sizes, nbatch):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_gather_scale launch over
-# one 128^3 problem of the workload (42,410,240 bytes; ncu --set full, the
+# one 128^3 problem of the workload (42,417,664 bytes; ncu --set full, the
 # command in profiles/k_gather_scale_128.md), per point
-GATHER_SCALE_DRAM_BYTES_PER_POINT = 42410240 / 128 ** 3
-# l1tex__data_pipe_lsu_wavefronts_mem_shared.sum of the same capture (4.44 M
-# shared-memory wavefronts for 128^3 points: the 64 taps per point plus the box
-# copies), per point; a B200 SM serves one 128-byte wavefront per clock
-GATHER_SCALE_SMEM_WAVEFRONTS_PER_POINT = 4.44e6 / 128 ** 3
+GATHER_SCALE_DRAM_BYTES_PER_POINT = 42417664 / 128 ** 3
+# l1tex__data_pipe_lsu_wavefronts_mem_shared.sum of the same capture (4.29 M
+# shared-memory wavefronts for 128^3 points: the 64 taps per point; the box
+# arrives by bulk copies, which this counter does not see), per point; a B200
+# SM serves one 128-byte wavefront per clock
+GATHER_SCALE_SMEM_WAVEFRONTS_PER_POINT = 4.286e6 / 128 ** 3
 
 
 def roofline(cb, a, ci, load_device, B):
