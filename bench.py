@@ -460,6 +460,7 @@ def roofline(cb, a, ci, load_device, B):
     ci.profile(True)
     ci.Run()
     ms, cnt = ci.profile_read(cb.PROF_ADJOINT_STEP)
+    pc_ms, pc_cnt = ci.profile_read(cb.PROF_PRECOND)
     ci.profile(False)
     torch.cuda.synchronize()
     avg_ms = ms / max(cnt, 1)
@@ -474,11 +475,24 @@ def roofline(cb, a, ci, load_device, B):
                     f"(148 SMs at {sm_mhz:.0f} MHz)", "wavefronts_per_launch": wf,
             "achieved_per_s": wf / (avg_ms / 1e3), "peak_per_s": wf_peak,
             "frac": round(wf / (avg_ms / 1e3) / wf_peak, 4)}
+    # the PCG preconditioner z = P r: one 3-field r2c -> inverse symbol -> c2r
+    # over the B problems (5 passes: rows, x2 columns, x1 pencil with the
+    # symbol, x2 columns, rows with the r.z epilogue); algorithmic bytes 24n
+    # per problem (3 fields in, 3 out)
+    pc_avg = pc_ms / max(pc_cnt, 1)
+    pc_bytes = 24 * n * B
+    spectral = {"what": "z = P r (3-field forward + inverse FFT with the inverse regularisation symbol), "
+                        "B problems per launch sequence",
+                "avg_us": round(pc_avg * 1e3, 2), "us_per_problem": round(pc_avg * 1e3 / B, 2),
+                "algorithmic_bytes": pc_bytes,
+                "achieved": round(pc_bytes / (pc_avg / 1e3) / 1e9, 1) if pc_cnt else None,
+                "frac": round(pc_bytes / (pc_avg / 1e3) / 1e9 / peak, 4) if pc_cnt else None,
+                "applications_timed": pc_cnt}
     return {"kernel": "k_gather_scale (adjoint time step: tricubic tile gather x per-point factor)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "algorithmic_bytes": bytes_,
             "avg_launch_us": round(avg_ms * 1e3, 2), "launches_timed": cnt, "peak_source": peak_src,
-            "shared_memory_roofline": smem}
+            "shared_memory_roofline": smem, "spectral_operator": spectral}
 
 
 # ---------------------------------------------------------------------------

@@ -1330,7 +1330,11 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
   note_launches(1);
   // z = P r and r.z into slot s (the inverse transform's epilogue sums it)
   auto apply_pc = [&](int s) -> int {
-    if (opts.precond) return reg_op(r, z, OP_REG_INV, EPI_STORE, act, r, s);
+    if (opts.precond) {
+      CB_TRY(prof_mark(CB_PROF_PRECOND));
+      CB_TRY(reg_op(r, z, OP_REG_INV, EPI_STORE, act, r, s));
+      return prof_mark(CB_PROF_PRECOND);
+    }
     note_launches(1);
     CB_TRY(launch_lincomb(z, 3 * n, r, 3 * n, nullptr, 1.0, nullptr, 0, nullptr, 0.0, 3 * n, B, act, stream));
     return dot(r, 3 * n, z, 3 * n, 3 * n, s, act);

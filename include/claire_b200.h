@@ -372,7 +372,10 @@ int claire_b200_server_destroy(claire_b200_server* srv);
 #define CB_PROF_ADJOINT_STEP 0  /* lambda^{l-1} = c * lambda^l(X): one per adjoint step */
 #define CB_PROF_INCSTATE_STEP 1 /* m~^{j+1} = m~^j(X) + s_j: one per incremental step */
 #define CB_PROF_STATE_STEP 2    /* m^{j+1} = m^j(X): one per state step */
-#define CB_PROF_NCAT 3
+#define CB_PROF_PRECOND 3       /* z = P r in the PCG: one 3-field forward + inverse transform with the
+                                   inverse symbol, per Krylov iteration (Preconditioner::MatVec,
+                                   src/Preconditioner.cpp:507-580) */
+#define CB_PROF_NCAT 4
 int claire_b200_profile(claire_b200_ctx* ctx, int enable);
 int claire_b200_profile_read(claire_b200_ctx* ctx, int category, double* total_ms, long long* launches);
 
