@@ -46,6 +46,7 @@ struct Request {
   float* in_pin = nullptr;    // or page-locked: mR then mT
   std::vector<float> v;       // result velocity (pageable path)
   float* v_pin = nullptr;     // or page-locked
+  bool staging = false;       // the stager is copying the inputs into a page-locked block
   claire_b200_stats stats{};
   int status = CB_REQ_QUEUED;
   int error = CB_OK;
@@ -82,6 +83,7 @@ struct claire_b200_server {
   // and blocks allocated, by float count
   std::map<long long, std::vector<float*>> pinned_free[2];
   std::map<long long, int> pinned_count[2];
+  std::thread stager;  // copies queued pageable inputs into free page-locked blocks
 };
 
 namespace cb {
@@ -95,6 +97,27 @@ struct Pool {
   bool dead = false;    // worker is leaving: takes no more requests
   bool exited = false;  // worker has released the memory and returns: the thread can be joined
   std::thread worker;
+  // Result copies run on their own stream: the worker queues a finished
+  // slot's velocity copy and goes on; the publisher thread waits for the copy
+  // and publishes the request.  The slot's next request waits (on the device)
+  // for the copy out of the slot before its velocity is reset.
+  cudaStream_t copy = nullptr;
+  float* stage_out = nullptr;            // device, 3n floats per slot: finished velocities being copied out
+  std::vector<cudaEvent_t> slot_ready;   // per slot: its velocity is in stage_out
+  std::vector<cudaEvent_t> slot_copied;  // per slot: its last copy to the host is done
+  std::vector<bool> slot_copy_issued;
+  struct Pending {
+    long long rid;
+    float* pin;
+    long long count;
+    cudaEvent_t ev;
+  };
+  std::mutex pmu;  // guards pending, ev_free, pstop
+  std::condition_variable pcv;
+  std::deque<Pending> pending;
+  std::vector<cudaEvent_t> ev_free;
+  bool pstop = false;
+  std::thread publisher;
 };
 
 // Join and drop the pools whose workers have exited.  Called with s->mu held,
@@ -185,7 +208,8 @@ static void create_pools_locked(claire_b200_server* s) {
     Request& r = s->reqs.at(id);
     if (find_pool(s, r.opts)) continue;
     const int slots = std::max(1, s->opts.slots_per_pool);
-    const long long need = Solver::estimate_bytes(r.opts, slots);
+    const long long nv = 3LL * r.opts.nx[0] * r.opts.nx[1] * r.opts.nx[2];
+    const long long need = Solver::estimate_bytes(r.opts, slots) + slots * nv * (long long)sizeof(float);
     if (s->used + need > s->budget) continue;  // stays queued until memory frees up
     auto pool = std::make_unique<Pool>();
     pool->key = r.opts;
@@ -206,7 +230,7 @@ static void create_pools_locked(claire_b200_server* s) {
       s->cv.notify_all();
       continue;
     }
-    pool->bytes = pool->solver->footprint();
+    pool->bytes = pool->solver->footprint() + slots * nv * (long long)sizeof(float);  // + stage_out
     pool->slot_req.assign(slots, 0);
     s->used += pool->bytes;
     Pool* raw = pool.get();
@@ -220,7 +244,7 @@ static std::vector<std::pair<int, long long>> admit_locked(claire_b200_server* s
   std::vector<std::pair<int, long long>> out;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     const Request& r = s->reqs.at(*it);
-    if (!same_pool(r.opts, p->key)) {
+    if (!same_pool(r.opts, p->key) || r.staging) {
       ++it;
       continue;
     }
@@ -245,9 +269,9 @@ static std::vector<std::pair<int, long long>> admit_locked(claire_b200_server* s
   return out;
 }
 
-// Inputs of request r into slot b.  The copies are complete when this returns
-// (set_problem synchronises the stream), so the request's input block can be
-// recycled.
+// Inputs of request r into slot b, queued on the pool's stream; the caller
+// synchronises (Solver::upload_problems, once for all admitted requests) before
+// the request's input block is recycled.
 static int load_slot(Solver& sv, int b, const Request& r) {
   const long long n = sv.n;
   const float* hR = r.in_pin ? r.in_pin : r.mR.data();
@@ -268,7 +292,130 @@ static int load_slot(Solver& sv, int b, const Request& r) {
     return CB_ERR_CUDA;
   }
   sv.images_changed(b);
-  return sv.set_problem(b, r.opts);  // per-slot norm and weights (synchronises the stream)
+  return sv.set_problem(b, r.opts, false);  // per-slot norm and weights, uploaded by the caller
+}
+
+// Publisher thread of a pool: waits (without holding the server's lock) for
+// each queued velocity copy and then publishes its request.  It leaves when
+// the pool's worker asks it to and the queue is empty.
+static void publisher_main(claire_b200_server* s, Pool* p) {
+  cudaSetDevice(s->opts.device);
+  while (true) {
+    Pool::Pending x{};
+    {
+      std::unique_lock<std::mutex> lk(p->pmu);
+      p->pcv.wait(lk, [&] { return p->pstop || !p->pending.empty(); });
+      if (p->pending.empty()) break;
+      x = p->pending.front();
+      p->pending.pop_front();
+    }
+    const bool ok = cudaEventSynchronize(x.ev) == cudaSuccess;
+    {
+      std::lock_guard<std::mutex> lk(p->pmu);
+      p->ev_free.push_back(x.ev);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(x.rid);
+    if (it != s->reqs.end() && ok) {
+      it->second.v_pin = x.pin;
+      it->second.status = CB_REQ_DONE;
+      it->second.t_done = Clock::now();
+    } else {
+      give_pinned_locked(s, 1, x.count, x.pin);
+      if (it != s->reqs.end()) {
+        it->second.status = CB_REQ_FAILED;
+        it->second.error = CB_ERR_CUDA;
+        it->second.t_done = Clock::now();
+      }
+    }
+    s->cv.notify_all();
+  }
+}
+
+// Queue the copy of slot b's velocity into the page-locked block pin on the
+// pool's copy stream (after the slot's last kernel) and hand it to the
+// publisher.  Called by the worker.
+static int queue_result_copy(Pool* p, Solver& sv, int b, long long rid, float* pin) {
+  const long long nv = 3 * sv.n;
+  cudaEvent_t ev = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(p->pmu);
+    if (!p->ev_free.empty()) {
+      ev = p->ev_free.back();
+      p->ev_free.pop_back();
+    }
+  }
+  if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return CB_ERR_CUDA;
+  // with stage_out the slot's velocity is first copied on the device (the slot
+  // is then free at once); the host copy runs beside the next requests' work
+  const float* src = sv.v + b * nv;
+  bool ok = true;
+  if (p->stage_out) {
+    float* st = p->stage_out + b * nv;
+    ok = (!p->slot_copy_issued[b] || cudaStreamWaitEvent(sv.stream, p->slot_copied[b], 0) == cudaSuccess) &&
+         cudaMemcpyAsync(st, src, sizeof(float) * nv, cudaMemcpyDeviceToDevice, sv.stream) == cudaSuccess;
+    src = st;
+  }
+  ok = ok && cudaEventRecord(p->slot_ready[b], sv.stream) == cudaSuccess &&
+       cudaStreamWaitEvent(p->copy, p->slot_ready[b], 0) == cudaSuccess &&
+       cudaMemcpyAsync(pin, src, sizeof(float) * nv, cudaMemcpyDeviceToHost, p->copy) == cudaSuccess &&
+       cudaEventRecord(p->slot_copied[b], p->copy) == cudaSuccess && cudaEventRecord(ev, p->copy) == cudaSuccess;
+  if (!ok) {
+    cudaEventDestroy(ev);
+    return CB_ERR_CUDA;
+  }
+  p->slot_copy_issued[b] = true;
+  {
+    std::lock_guard<std::mutex> lk(p->pmu);
+    p->pending.push_back(Pool::Pending{rid, pin, nv, ev});
+  }
+  p->pcv.notify_all();
+  return CB_OK;
+}
+
+// Stager thread: while a queued request still holds pageable inputs and a
+// page-locked input block of its size is free, move the inputs into the block
+// (the CPU copy runs here, beside the pools' GPU work, so the worker's upload
+// of that request is a DMA).  A request is not admitted while it is staged.
+static void stager_main(claire_b200_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    long long pick = 0, n = 0;
+    float* blk = nullptr;
+    for (long long id : s->queue) {
+      Request& r = s->reqs.at(id);
+      if (r.in_pin || r.staging || r.mR.empty()) continue;
+      const long long nn = (long long)r.opts.nx[0] * r.opts.nx[1] * r.opts.nx[2];
+      auto fl = s->pinned_free[0].find(2 * nn);
+      if (fl == s->pinned_free[0].end() || fl->second.empty()) continue;
+      blk = fl->second.back();
+      fl->second.pop_back();
+      pick = id;
+      n = nn;
+      break;
+    }
+    if (!pick) {
+      s->cv.wait(lk);
+      continue;
+    }
+    Request& r = s->reqs.at(pick);
+    r.staging = true;
+    std::vector<float> a = std::move(r.mR), b = std::move(r.mT);
+    lk.unlock();
+    std::memcpy(blk, a.data(), sizeof(float) * n);
+    std::memcpy(blk + n, b.data(), sizeof(float) * n);
+    lk.lock();
+    auto it = s->reqs.find(pick);
+    if (it != s->reqs.end() && it->second.status == CB_REQ_QUEUED) {
+      it->second.in_pin = blk;
+      it->second.staging = false;
+    } else {
+      // cancelled or failed meanwhile: its inputs are no longer needed
+      if (it != s->reqs.end()) it->second.staging = false;
+      give_pinned_locked(s, 0, 2 * n, blk);
+    }
+    s->cv.notify_all();
+  }
 }
 
 static void fill_stats(const ProbState& ps, claire_b200_stats* st) {
@@ -300,7 +447,20 @@ static void worker_main(claire_b200_server* s, Pool* p) {
   prealloc_pinned(s, 0, 2 * sv.n, 2 * S);
   prealloc_pinned(s, 1, 3 * sv.n, 2 * S);
   int err = CB_OK;
-  while (true) {
+  p->slot_ready.assign(S, nullptr);
+  p->slot_copied.assign(S, nullptr);
+  p->slot_copy_issued.assign(S, false);
+  if (cudaStreamCreateWithFlags(&p->copy, cudaStreamNonBlocking) != cudaSuccess) err = CB_ERR_CUDA;
+  for (int b = 0; b < S && !err; ++b)
+    if (cudaEventCreateWithFlags(&p->slot_ready[b], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->slot_copied[b], cudaEventDisableTiming) != cudaSuccess)
+      err = CB_ERR_CUDA;
+  if (!err && cudaMalloc((void**)&p->stage_out, sizeof(float) * 3 * sv.n * S) != cudaSuccess) {
+    cudaGetLastError();
+    p->stage_out = nullptr;  // copies go straight from the slots' velocities
+  }
+  p->publisher = std::thread(publisher_main, s, p);
+  while (!err) {
     std::vector<std::pair<int, long long>> admits;
     {
       std::unique_lock<std::mutex> lk(s->mu);
@@ -345,22 +505,37 @@ static void worker_main(claire_b200_server* s, Pool* p) {
         continue;
       }
     }
-    // admission: inputs into the slots, then InitializeOptimization for them
+    // admission: inputs into the slots (one synchronisation for all), then
+    // InitializeOptimization for them
     std::vector<int> sel_new(S, 0);
+    std::vector<Request*> loaded;
     for (auto& a : admits) {
       Request* r;
       {
         std::lock_guard<std::mutex> lk(s->mu);
         r = &s->reqs.at(a.second);
       }
-      err = load_slot(sv, a.first, *r);
-      if (r->in_pin) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        give_pinned_locked(s, 0, 2 * sv.n, r->in_pin);
-        r->in_pin = nullptr;
-      }
+      loaded.push_back(r);
+      // without stage_out the slot's previous velocity is copied straight
+      // from the slot, and must be out before the slot is reset
+      if (!p->stage_out && p->slot_copy_issued[a.first] &&
+          cudaStreamWaitEvent(sv.stream, p->slot_copied[a.first], 0) != cudaSuccess)
+        err = CB_ERR_CUDA;
+      if (!err) err = load_slot(sv, a.first, *r);
       if (err) break;
       sel_new[a.first] = 1;
+    }
+    if (!admits.empty()) {
+      const int e = sv.upload_problems();  // synchronises: the uploads are done
+      if (!err) err = e;
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (Request* r : loaded)
+        if (r->in_pin) {
+          if (e) continue;  // an upload may still be in flight: keep the block with the request
+          give_pinned_locked(s, 0, 2 * sv.n, r->in_pin);
+          r->in_pin = nullptr;
+        }
+      s->cv.notify_all();  // the stager may fill the returned blocks for queued requests
     }
     if (!err && !admits.empty()) err = sv.begin(sel_new);
     std::vector<int> fin(S, 0);
@@ -377,48 +552,76 @@ static void worker_main(claire_b200_server* s, Pool* p) {
     if (!err && anydone) err = sv.finish(done);
     if (err) break;
     if (anydone) {
-      // velocities into page-locked blocks (one synchronisation for all), or
-      // into pageable vectors past the cap
-      struct Out {
-        int b;
-        float* pin;
-        std::vector<float> vh;
-      };
-      std::vector<Out> outv;
+      // velocities into page-locked blocks on the copy stream (published by the
+      // publisher thread when they land), or, past the blocks, synchronously
+      // into pageable vectors
       const long long nv = 3 * sv.n;
+      std::vector<std::pair<int, std::vector<float>>> outv;
+      std::vector<int> queued;
       for (int b = 0; b < S && !err; ++b) {
         if (!done[b]) continue;
-        Out o{b, take_pinned(s, 1, nv), {}};
-        if (!o.pin) o.vh.resize((size_t)nv);
-        float* dst = o.pin ? o.pin : o.vh.data();
-        if (cudaMemcpyAsync(dst, sv.v + b * nv, sizeof(float) * nv, cudaMemcpyDeviceToHost, sv.stream) !=
+        float* pin = take_pinned(s, 1, nv);
+        long long rid;
+        {
+          // statistics first: the publisher may publish the request as soon as
+          // its copy is queued
+          std::lock_guard<std::mutex> lk(s->mu);
+          rid = p->slot_req[b];
+          fill_stats(sv.ps[b], &s->reqs.at(rid).stats);
+        }
+        if (pin) {
+          err = queue_result_copy(p, sv, b, rid, pin);
+          if (err) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            give_pinned_locked(s, 1, nv, pin);
+          } else {
+            queued.push_back(b);
+          }
+          continue;
+        }
+        std::vector<float> vh((size_t)nv);
+        if (cudaMemcpyAsync(vh.data(), sv.v + b * nv, sizeof(float) * nv, cudaMemcpyDeviceToHost, sv.stream) !=
                 cudaSuccess ||
-            (!o.pin && cudaStreamSynchronize(sv.stream) != cudaSuccess))
+            cudaStreamSynchronize(sv.stream) != cudaSuccess)
           err = CB_ERR_CUDA;
-        outv.push_back(std::move(o));
-      }
-      if (!err && cudaStreamSynchronize(sv.stream) != cudaSuccess) err = CB_ERR_CUDA;
-      if (err) {
-        std::lock_guard<std::mutex> lk(s->mu);
-        for (auto& o : outv) give_pinned_locked(s, 1, nv, o.pin);
-        break;
+        else
+          outv.push_back({b, std::move(vh)});
       }
       std::lock_guard<std::mutex> lk(s->mu);
+      for (int b : queued) p->slot_req[b] = 0;  // published when their copies land
       for (auto& o : outv) {
-        const int b = o.b;
+        const int b = o.first;
         Request& r = s->reqs.at(p->slot_req[b]);
-        r.v = std::move(o.vh);
-        r.v_pin = o.pin;
-        fill_stats(sv.ps[b], &r.stats);
+        r.v = std::move(o.second);
         r.status = CB_REQ_DONE;
         r.t_done = Clock::now();
         p->slot_req[b] = 0;
       }
       s->cv.notify_all();
+      if (err) break;
     }
   }
-  // exit: fail what this pool still holds, release the memory, let queued
-  // requests of other keys get a pool
+  // exit: let the publisher finish the queued copies (it takes the server's
+  // lock, so it is joined before this thread takes it), fail what this pool
+  // still holds, release the memory, let queued requests of other keys get a
+  // pool
+  {
+    std::lock_guard<std::mutex> lk(p->pmu);
+    p->pstop = true;
+  }
+  p->pcv.notify_all();
+  if (p->publisher.joinable()) p->publisher.join();
+  if (p->copy) cudaStreamSynchronize(p->copy);
+  for (cudaEvent_t e : p->ev_free) cudaEventDestroy(e);
+  p->ev_free.clear();
+  for (cudaEvent_t e : p->slot_ready)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->slot_copied)
+    if (e) cudaEventDestroy(e);
+  if (p->copy) cudaStreamDestroy(p->copy);
+  p->copy = nullptr;
+  if (p->stage_out) cudaFree(p->stage_out);
+  p->stage_out = nullptr;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     for (int b = 0; b < S; ++b)
@@ -468,6 +671,12 @@ int claire_b200_server_create(const claire_b200_server_opts* o, claire_b200_serv
     return CB_ERR_CUDA;
   }
   s->budget = o->hbm_budget_bytes > 0 ? o->hbm_budget_bytes : (long long)(0.9 * (double)freeb);
+  try {
+    s->stager = std::thread(cb::srv::stager_main, s);
+  } catch (...) {
+    delete s;
+    return CB_ERR_ALLOC;
+  }
   *out = s;
   return CB_OK;
 }
@@ -609,6 +818,7 @@ int claire_b200_server_destroy(claire_b200_server* s) {
     s->queue.clear();
     s->cv.notify_all();
   }
+  if (s->stager.joinable()) s->stager.join();
   for (auto& p : s->pools)
     if (p->worker.joinable()) p->worker.join();
   for (auto& kv : s->reqs) {

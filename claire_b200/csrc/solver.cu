@@ -369,7 +369,7 @@ int Solver::init(const claire_b200_opts& o, int Bn) {
   return 0;
 }
 
-int Solver::set_problem(int b, const claire_b200_opts& o) {
+int Solver::set_problem(int b, const claire_b200_opts& o, bool upload) {
   if (b < 0 || b >= B) return CB_ERR_ARG;
   if (o.nx[0] != d.n1 || o.nx[1] != d.n2 || o.nx[2] != d.n3 || o.nt != nt) {
     err = "per-problem options must keep nx and nt";
@@ -379,7 +379,7 @@ int Solver::set_problem(int b, const claire_b200_opts& o) {
   ps[b].beta0 = o.beta[0];
   ps[b].beta1 = o.beta[1];
   ps[b].beta2 = o.beta[2];
-  return upload_params();
+  return upload ? upload_params() : 0;
 }
 
 int Solver::upload_params() {

@@ -81,7 +81,10 @@ class Solver {
   // SetMask (src/CLAIREInterface.cpp:277-286): weights w (device, n floats) of
   // problem b's distance, or none (w = null: weight 1)
   int set_mask(int b, const float* w);
-  int set_problem(int b, const claire_b200_opts& o);
+  // per-problem norm and weights; upload = false leaves the upload (and its
+  // synchronisation) to a later upload_problems()
+  int set_problem(int b, const claire_b200_opts& o, bool upload = true);
+  int upload_problems() { return upload_params(); }
   long long footprint() const { return bytes_; }
 
   // grid and sizes
