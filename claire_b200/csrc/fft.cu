@@ -90,7 +90,9 @@ template <int N, int V = 0> struct RowCfg {
 };
 template <int N, int V = 0> struct ColCfg {
   static constexpr int C = (V & 2) ? ColLines<N>::alt : ColLines<N>::base;
-  static constexpr int PITCH = C + 1;
+  // 16 lines: pitch 16 with rotated first-stage writes (RotateFirst); 32
+  // lines: odd pitch (a warp's lanes are the 32 lines at one element)
+  static constexpr int PITCH = C == 16 ? 16 : C + 1;
 };
 
 constexpr int kThreads = kFftThreads;

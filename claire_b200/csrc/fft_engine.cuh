@@ -2,8 +2,9 @@
 //
 // A CTA transforms `nlines` complex lines of length N that live in shared
 // memory as split real/imaginary arrays: element e of line p sits at
-// re[e*PITCH + p], im[e*PITCH + p] (line index fastest, PITCH odd so that
-// consecutive lines hit distinct banks).  Line count and pitch are
+// re[e*PITCH + p], im[e*PITCH + p] (line index fastest; PITCH odd for 32 or
+// more lines, so that consecutive lines hit distinct banks, and 16 for 16
+// lines, see RotateFirst).  Line count and pitch are
 // compile-time so every loop has a known trip count.  Every plan has exactly two radix
 // stages (N = R0*R1, R0, R1 in {4, 8, 10, 12, 15, 16}), each an in-register DFT
 // followed by one shared-memory exchange, so the result lands back in the
@@ -246,6 +247,19 @@ template <int N, int V = 0> struct Plan {
 
 constexpr int kFftThreads = 256;  // threads per CTA of every FFT kernel
 
+// Bank spread of a 16-line layout.  Lanes 0-15 and 16-31 of a warp hold one
+// element index apart (j and j + 1).  A pitch of 16 (mod 32) puts the two
+// half-warps in opposite halves of the bank space for every read and every
+// write of a later stage (element offsets 1 or odd).  A first-stage (span 1)
+// write puts the two half-warps R elements apart: for even R that is the same
+// half.  So there the upper half-warp writes its R outputs rotated by one,
+// which makes the offset R + 1 (or 1), odd again.  Every output is still
+// written once, with the same value.
+template <int NL, int PITCH, int R>
+struct RotateFirst {
+  static constexpr bool value = NL == 16 && PITCH % 32 == 16 && R % 2 == 0;
+};
+
 template <int N, int R, int NS, bool INV, int NL, int PITCH>
 CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict__ sim,
                          float* __restrict__ dre, float* __restrict__ dim, const float2* __restrict__ tw) {
@@ -272,11 +286,23 @@ CB_DEVICE void fft_stage(const float* __restrict__ sre, const float* __restrict_
     }
     Dft<R, INV>::run(v);
     const int o = (j - k) * R + k;
+    if constexpr (NS == 1 && RotateFirst<NL, PITCH, R>::value) {
+      const int h = j & 1;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int idx = (o + r * NS) * PITCH + p;
-      dre[idx] = v[r].x;
-      dim[idx] = v[r].y;
+      for (int r = 0; r < R; ++r) {
+        const int rr = (r + h == R) ? 0 : r + h;
+        const float2 x = h ? v[(r + 1) % R] : v[r];
+        const int idx = (o + rr) * PITCH + p;
+        dre[idx] = x.x;
+        dim[idx] = x.y;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int idx = (o + r * NS) * PITCH + p;
+        dre[idx] = v[r].x;
+        dim[idx] = v[r].y;
+      }
     }
   }
 }
@@ -315,11 +341,23 @@ CB_DEVICE void fft_stage_in(const Load& ld, float* __restrict__ dre, float* __re
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = ld(p, j + r * J);
     Dft<R, INV>::run(v);
+    if constexpr (RotateFirst<NL, PITCH, R>::value) {
+      const int h = j & 1;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int idx = (j * R + r) * PITCH + p;
-      dre[idx] = v[r].x;
-      dim[idx] = v[r].y;
+      for (int r = 0; r < R; ++r) {
+        const int rr = (r + h == R) ? 0 : r + h;
+        const float2 x = h ? v[(r + 1) % R] : v[r];
+        const int idx = (j * R + rr) * PITCH + p;
+        dre[idx] = x.x;
+        dim[idx] = x.y;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int idx = (j * R + r) * PITCH + p;
+        dre[idx] = v[r].x;
+        dim[idx] = v[r].y;
+      }
     }
   }
 }
