@@ -157,3 +157,31 @@ def test_scheduler_places_whole_requests(cb):
             assert st["gn_iterations"] == st_ref["gn_iterations"]
             assert np.array_equal(v, v_ref)
         assert all(x == 0 for x in sch.outstanding.values())
+
+
+def test_burst_beyond_page_locked_blocks(cb):
+    """A burst of requests larger than the pool's page-locked blocks (slots
+    per pool 1: 2 input and 2 result blocks): the later requests arrive with
+    pageable inputs that the stager moves into recycled blocks, every
+    velocity comes back on the pool's copy stream, and one queued request is
+    cancelled in the middle.  Each result equals the plain run of its inputs."""
+    n, nt = 32, 4
+    probs = [ellipsoids(n, nt, 20 + i) for i in range(6)]
+    opt = opt_for(cb, n, nt, "h1s", 1e-2, maxit=2)
+    refs = [plain_run(cb, opt, mR, mT) for mR, mT in probs]
+    with cb.Server(slots_per_pool=1, idle_ms=200) as srv:
+        ids = [srv.submit(opt, mR, mT) for mR, mT in probs]
+        srv.cancel(ids[3])  # still queued behind the single slot
+        for i, rid in enumerate(ids):
+            st = srv.wait(rid, 300000)
+            if i == 3:
+                assert st == cb.REQ_CANCELLED
+                with pytest.raises(cb.ClaireError):
+                    srv.result(rid, (n, n, n))
+                continue
+            assert st == cb.REQ_DONE
+            v, stats, _ = srv.result(rid, (n, n, n))
+            v_ref, st_ref = refs[i]
+            assert stats["gn_iterations"] == st_ref["gn_iterations"]
+            assert stats["pcg_iterations"] == st_ref["pcg_iterations"]
+            assert np.array_equal(v, v_ref)
