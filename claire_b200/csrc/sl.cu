@@ -459,9 +459,12 @@ int launch_field_stats(const float* f, long long fp, long long n, int nprob, dou
 
 // Health of the box copies' bounded waits: tile gathers on this device whose
 // box copy did not complete within the wait limit (each skipped its tile).
-int stage_timeouts(unsigned long long* count) {
+int stage_timeouts(unsigned long long* count, cudaStream_t s) {
   unsigned v = 0;
-  if (cudaMemcpyFromSymbol(&v, g_stage_timeouts, sizeof(unsigned)) != cudaSuccess) return (int)cudaGetLastError();
+  if (cudaMemcpyFromSymbolAsync(&v, g_stage_timeouts, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return (int)cudaGetLastError();
   *count = v;
   return 0;
 }

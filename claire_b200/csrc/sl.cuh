@@ -90,8 +90,9 @@ int launch_trajectory(const float* v, long long vp, float* disp, long long dp, i
 // Box table of displacement field disp[p] for the tile gathers below:
 // 2 int4 per 8x8x16 tile (tile_table_int4s(d) int4 per problem, tp apart).
 // Box copies of the tile gathers that ran out of their bounded wait (count on
-// the current device), and a self-test that makes one wait run out.
-int stage_timeouts(unsigned long long* count);
+// the current device; read on stream s after its work), and a self-test that
+// makes one wait run out.
+int stage_timeouts(unsigned long long* count, cudaStream_t s = nullptr);
 int launch_stage_wait_selftest(unsigned long long wait_ns, cudaStream_t s);
 int launch_tile_table(const float* disp, long long dp, int4* tab, long long tp, int nprob, const Dims& d,
                       const int* active, cudaStream_t s);

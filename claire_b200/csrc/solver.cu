@@ -213,7 +213,7 @@ long long Solver::estimate_bytes(const claire_b200_opts& o, int B) {
 // (sl_tile.cuh); report it once, at the next GN-iteration boundary.
 int Solver::check_stage() {
   unsigned long long t = 0;
-  if (stage_timeouts(&t)) return CB_ERR_CUDA;
+  if (stage_timeouts(&t, stream)) return CB_ERR_CUDA;
   if (t <= stage_seen) return 0;
   stage_seen = t;
   err = "a tile gather's shared-memory box copy did not complete within its wait limit";
