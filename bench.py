@@ -461,6 +461,13 @@ def roofline(cb, a, ci, load_device, B):
     ci.Run()
     ms, cnt = ci.profile_read(cb.PROF_ADJOINT_STEP)
     pc_ms, pc_cnt = ci.profile_read(cb.PROF_PRECOND)
+    # the operations apps/benchmark.cpp of the reference times one by one
+    # (src/apps/benchmark.cpp:116-295), here in situ over the batch
+    per_op = {}
+    for name, cat in (("objective", cb.PROF_OBJECTIVE), ("gradient", cb.PROF_GRADIENT),
+                      ("hessian_matvec", cb.PROF_HESSIAN)):
+        op_ms, op_cnt = ci.profile_read(cat)
+        per_op[name] = {"ms_per_call": round(op_ms / max(op_cnt, 1), 3), "calls": op_cnt}
     ci.profile(False)
     torch.cuda.synchronize()
     avg_ms = ms / max(cnt, 1)
@@ -492,7 +499,7 @@ def roofline(cb, a, ci, load_device, B):
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "algorithmic_bytes": bytes_,
             "avg_launch_us": round(avg_ms * 1e3, 2), "launches_timed": cnt, "peak_source": peak_src,
-            "shared_memory_roofline": smem, "spectral_operator": spectral}
+            "shared_memory_roofline": smem, "spectral_operator": spectral, "per_op": per_op}
 
 
 # ---------------------------------------------------------------------------
@@ -514,6 +521,36 @@ def cpu_model():
     except OSError:
         pass
     return "unknown"
+
+
+def cpu_per_op(a, reps=3):
+    """Per-operation times of the C++ restatement (FP32, all host cores) on
+    the workload's first problem, as apps/benchmark.cpp of the reference
+    times them: objective (state solve + distance + regularisation),
+    gradient, GN Hessian matvec, at half the problem's true velocity."""
+    from oracle import claire_ref as R
+    from oracle.cpu_ref import CpuRef
+    shape = (a.n,) * 3
+    rng = np.random.Generator(np.random.PCG64(R.problem_seed(1, 0)))
+    mT = R.template_ellipsoids(shape, rng)
+    v = R.velocity_random(shape, rng)
+    c = CpuRef(shape, a.nt, a.norm, a.beta, fp64=False, threads=cpu_cores())
+    mR = c.forward(v, mT)
+    c.set_images(mR, mT)
+    vh = 0.5 * v
+    vt = 0.1 * v
+    out = {}
+    # the matvec reuses the state and adjoint of the gradient at vh, as the
+    # reference's HessianMatVec does after EvaluateGradient
+    for name, fn in (("objective", lambda: c.objective(vh)), ("gradient", lambda: c.gradient(vh)),
+                     ("hessian_matvec", lambda: c.hessian_matvec_current(vt))):
+        fn()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        out[name] = round((time.perf_counter() - t) / reps * 1e3, 1)
+    c.close()
+    return out
 
 
 def cpu_problem(a, problem_index=0):
@@ -1007,6 +1044,22 @@ def main():
     s99 = float(np.percentile(ls, 99))
     st0 = r["stats"][0]
     cpu = None if a.no_cpu else cpu_baseline_sample(a)
+    # per-operation table (the reference's apps/benchmark.cpp operations): the
+    # device's in-situ calls over the batch beside the CPU restatement's
+    per_op = None
+    if r["roof"] is not None:
+        dev = r["roof"].pop("per_op", None)
+        per_op = {"device_ms_per_call": dev, "problems_per_device_call": B,
+                  "what": "device: mean CUDA-event time per call in the timed registration of the roofline leg "
+                          "(line-search objectives cover the problems still searching); cpu: the C++ FP32 "
+                          "restatement on one problem"}
+        if not a.no_cpu:
+            cpu_ops = cpu_per_op(a)
+            per_op["cpu_ms_per_problem"] = cpu_ops
+            if dev:
+                per_op["cpu_over_device_per_problem"] = {
+                    k: round(cpu_ops[k] / (dev[k]["ms_per_call"] / B), 1) for k in cpu_ops
+                    if dev.get(k) and dev[k]["ms_per_call"] > 0}
     line = {
         "metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": r["total_ms"] / a.steps, "higher_is_better": True,
@@ -1034,6 +1087,7 @@ def main():
                                                / (r["total_ms"] / 1e3)),
                    "fft_variants": r["tuned"] or "defaults (--no-autotune)",
                    "fixed_work": r["fixed"],
+                   "per_op": per_op,
                    "converging": r["conv"]},
         "e2e": {"value": regs / (r["e2e_ms"] / 1e3), "unit": "registrations/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],

@@ -169,6 +169,7 @@ _signatures = {
 
 # device timer categories (claire_b200_profile_read)
 PROF_ADJOINT_STEP, PROF_INCSTATE_STEP, PROF_STATE_STEP, PROF_PRECOND = 0, 1, 2, 3
+PROF_OBJECTIVE, PROF_GRADIENT, PROF_HESSIAN = 4, 5, 6
 for _name, (_res, _args) in _signatures.items():
     _fn = getattr(lib, _name)
     _fn.restype = _res

@@ -762,6 +762,7 @@ static double reg_factor(const ProbState& s, double hd, double sumsq, double vv)
 }
 
 int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
+  CB_TRY(prof_mark(CB_PROF_OBJECTIVE));
   CB_TRY(upload_mask(sel, dact));
   CB_TRY(state_solve(vel, dact));
   CB_TRY(distance(sel, dact));
@@ -799,7 +800,7 @@ int Solver::objective_at(const float* vel, const std::vector<int>& sel) {
     ps[b].pde_solves++;
     state_of[b] = (vel == v) ? 1 : 2;
   }
-  return 0;
+  return prof_mark(CB_PROF_OBJECTIVE);
 }
 
 // ---------------------------------------------------------------------------
@@ -926,6 +927,7 @@ int Solver::finish_with_reg(const float* vin, float* out, const int* act, const 
 // EvaluateGradient at v (src/CLAIRE.cpp:871-1042); the state must be valid for v.
 int Solver::gradient(const int* act) {
   const long long PM = (nt + 1) * n, PGM = (nt + 1) * 3 * n, PL = (nt + 1) * n;
+  CB_TRY(prof_mark(CB_PROF_GRADIENT));
   CB_TRY(characteristic(v, -1.f, act));
   CB_TRY(image_grad(act));
   CB_TRY(divergence(v, divv, act));
@@ -936,7 +938,7 @@ int Solver::gradient(const int* act) {
   note_launches(2);
   CB_TRY(finish_with_reg(v, g, act));
   CB_TRY(dot(g, 3 * n, g, 3 * n, 3 * n, S_GG, act));
-  return 0;
+  return prof_mark(CB_PROF_GRADIENT);
 }
 
 // caches for the Hessian: (grad m^j)(X_state), j < nt
@@ -1360,7 +1362,9 @@ int Solver::pcg(const std::vector<int>& sel, double maxit_d) {
       rec_act = act_rec;
       norec_act = any_norec ? act_norec : nullptr;
     }
+    CB_TRY(prof_mark(CB_PROF_HESSIAN));
     const int he = apply_op(pv, q, act, S_PQ);  // q = H p and p.q
+    if (!he) CB_TRY(prof_mark(CB_PROF_HESSIAN));
     reg_in = nullptr;
     rec_act = norec_act = nullptr;
     CB_TRY(he);

@@ -375,7 +375,11 @@ int claire_b200_server_destroy(claire_b200_server* srv);
 #define CB_PROF_PRECOND 3       /* z = P r in the PCG: one 3-field forward + inverse transform with the
                                    inverse symbol, per Krylov iteration (Preconditioner::MatVec,
                                    src/Preconditioner.cpp:507-580) */
-#define CB_PROF_NCAT 4
+#define CB_PROF_OBJECTIVE 4     /* one objective evaluation: state solve, distance, regularisation functional
+                                   (OptimizationProblem::EvaluateObjective) */
+#define CB_PROF_GRADIENT 5      /* one gradient: adjoint solve, body force, regularisation (EvaluateGradient) */
+#define CB_PROF_HESSIAN 6       /* one GN Hessian matvec in the PCG (HessianMatVec) */
+#define CB_PROF_NCAT 7
 int claire_b200_profile(claire_b200_ctx* ctx, int enable);
 int claire_b200_profile_read(claire_b200_ctx* ctx, int category, double* total_ms, long long* launches);
 

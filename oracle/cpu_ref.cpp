@@ -1108,6 +1108,20 @@ int cref_hessian_matvec(void* h, const double* v, const double* vt, double* out)
   });
 }
 
+// GN Hessian matvec at the velocity of the last cref_gradient call (its state,
+// adjoint and characteristics are reused, as HessianMatVec reuses them after
+// EvaluateGradient in the reference, src/CLAIRE.cpp:1218-1303).
+int cref_hessian_matvec_current(void* h, const double* vt, double* out) {
+  return dispatch(h, [&](auto& P) {
+    using R = typename std::remove_reference<decltype(P.v[0])>::type;
+    auto tt = conv<R>(vt, 3 * P.nl);
+    std::vector<R> o(3 * P.nl);
+    P.hessian_matvec(tt.data(), o.data());
+    back(o.data(), out, 3 * P.nl);
+    return 0;
+  });
+}
+
 int cref_precond(void* h, const double* x, double* out) {
   return dispatch(h, [&](auto& P) {
     using R = typename std::remove_reference<decltype(P.v[0])>::type;

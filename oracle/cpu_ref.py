@@ -63,6 +63,7 @@ def lib():
             "cref_objective": (I, [P, DP, DP]),
             "cref_gradient": (I, [P, DP, DP]),
             "cref_hessian_matvec": (I, [P, DP, DP, DP]),
+            "cref_hessian_matvec_current": (I, [P, DP, DP]),
             "cref_precond": (I, [P, DP, DP]),
             "cref_reg_apply": (I, [P, I, DP, DP]),
             "cref_reg_functional": (I, [P, DP, DP]),
@@ -146,6 +147,11 @@ class CpuRef:
 
     def hessian_matvec(self, v, vt):
         return self._vec_op(self.L.cref_hessian_matvec, [_ptr(_in(v)), _ptr(_in(vt))], (3,) + self.shape)
+
+    def hessian_matvec_current(self, vt):
+        """Hessian matvec at the velocity of the last gradient() call (its
+        state and adjoint reused)."""
+        return self._vec_op(self.L.cref_hessian_matvec_current, [_ptr(_in(vt))], (3,) + self.shape)
 
     def precond(self, x):
         return self._vec_op(self.L.cref_precond, [_ptr(_in(x))], (3,) + self.shape)

@@ -70,6 +70,8 @@ def test_objective_gradient_hessian(norm, beta):
     assert abs(J - prob.objective(v)) <= 1e-13 * abs(J)
     assert rel(c.gradient(v), prob.gradient(v)) < 1e-12
     assert rel(c.hessian_matvec(v, vt), prob.hessian_matvec(vt)) < 1e-12
+    c.gradient(v)  # the matvec at the current iterate reuses this gradient's state and adjoint
+    assert rel(c.hessian_matvec_current(vt), prob.hessian_matvec(vt)) < 1e-12
     assert rel(c.precond(vt), prob.precond(vt)) < 1e-12
     m1 = c.forward(v, mT)
     assert rel(m1, R.forward_transport(mT, v, nt)) < 1e-13
