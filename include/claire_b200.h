@@ -363,12 +363,15 @@ int claire_b200_server_info(claire_b200_server* srv, int* pools, long long* byte
 /* Fails queued requests, waits for running ones' pools to stop, frees everything. */
 int claire_b200_server_destroy(claire_b200_server* srv);
 
-/* Device timers of the solver's time-step kernels, the counterpart of the
- * reference's per-phase timers and counters (include/RegOpt.hpp:183-202).
- * While enabled, every launch of a category is bracketed by CUDA events on
- * the context's stream (host overhead per launch: use for instrumented runs).
+/* Device timers of the solver's time steps and operations, the counterpart
+ * of the reference's per-phase timers and counters (include/RegOpt.hpp:183-202).
+ * While enabled, every launch or call of a category is bracketed by CUDA
+ * events on the context's stream (host overhead per launch: use for
+ * instrumented runs; PCG iterations then run without graph replay).  An
+ * operation category (objective, gradient, Hessian) covers every launch of
+ * one call, including the waits for its host-side decisions.
  * claire_b200_profile_read synchronizes the stream, returns the summed device
- * time and the launch count of a category since the last read, and resets it. */
+ * time and the count of a category since the last read, and resets it. */
 #define CB_PROF_ADJOINT_STEP 0  /* lambda^{l-1} = c * lambda^l(X): one per adjoint step */
 #define CB_PROF_INCSTATE_STEP 1 /* m~^{j+1} = m~^j(X) + s_j: one per incremental step */
 #define CB_PROF_STATE_STEP 2    /* m^{j+1} = m^j(X): one per state step */
