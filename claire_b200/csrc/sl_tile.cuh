@@ -502,14 +502,20 @@ CB_DEVICE float2 gather_staged_pair(unsigned sb, const float (&da)[3], const flo
 template <class Src, class Epi>
 CB_DEVICE void tile_gather(float* sb, const Src& src, const float* __restrict__ f, const Dims& d, const Epi& epi) {
   const TileThread tt = tile_thread(d);
+  // the box barrier is set up first: tile_box's own barriers publish it
+  __shared__ alignas(8) unsigned long long mbar;
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&mbar);
+  if (threadIdx.x == 0) mbar_init(bar);
   float dd[kTilePts][3];
   src.load(dd, tt, d);
   const TileBox bx = tile_box(dd, tt, d);
   if (bx.within && bx.vol <= kGatherBudget) {
-    __shared__ alignas(8) unsigned long long mbar;
-    const unsigned bar = (unsigned)__cvta_generic_to_shared(&mbar);
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sb);
-    stage_box_start(sbase, f, bx, d, bar);
+    // thread 0 arms the barrier while the copies start: bytes that land
+    // before the arrival take its transaction count below zero, and the
+    // phase cannot complete before the arrival
+    if (threadIdx.x == 0) mbar_arrive_expect(bar, box_bytes(bx));
+    issue_box_bulk(sbase, f, bx, d, bar);
     if (!stage_box_wait(bar, kStageWaitNs)) return;
     // two points per instruction (packed f32x2 pairs), as the table-driven gathers
 #pragma unroll
