@@ -84,6 +84,27 @@ def test_interp3_reproduces_cubics_and_nodes(cb):
     assert np.max(np.abs(out[inner] - exact[inner])) < 2e-5
 
 
+@pytest.mark.parametrize("n", [32, 48, 64])
+def test_interp3_staged_boxes_across_the_seams(cb, n):
+    """Displacements of under a cell keep every tile's footprint box small
+    enough to be staged in shared memory, so these gathers take the staged
+    path (bulk row copies), not the global fallback of the rougher
+    displacements above.  Boxes of border tiles start before the domain and
+    rows cross the periodic x3 seam (two copies per row); a uniform
+    displacement makes every tile's box the same shape."""
+    rng = np.random.default_rng(300 + n)
+    shape = (n, n, n)
+    f = smooth_field(shape, rng, 6) + 0.1 * rng.standard_normal(shape).astype(np.float32)
+    f = f.astype(np.float32)
+    idx = R.index_grid(shape)
+    for disp in (np.stack([np.full(shape, c, np.float32) for c in (0.37, -0.81, 0.55)]),
+                 np.stack([(0.45 * smooth_field(shape, rng, 3) / 6).astype(np.float32) for _ in range(3)])):
+        assert np.abs(disp).max() < 1.0
+        ref = R.interp3(f.astype(np.float64), idx + disp.astype(np.float64))
+        out = cb.SemiLagrangian.Interpolate(to_dev(f), to_dev(disp)).cpu().numpy()
+        assert rel(out, ref) < TOL
+
+
 @pytest.mark.parametrize("n,nt,flag", [(32, 4, "state"), (32, 8, "adjoint"), (48, 4, "state"), (64, 4, "adjoint")])
 def test_trajectory(cb, n, nt, flag):
     rng = np.random.default_rng(n + nt)
